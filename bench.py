@@ -1,0 +1,385 @@
+#!/usr/bin/env python
+"""Benchmark: MG-PCG solves/s (and p50/p99 latency) to 1e-8 relative residual,
+mixed precision vs FP64, for the multiresolution cantilever.
+
+One step = SetupGMG(densities) + SolveMG (zero start, ||f-Ku||/||f|| <= 1e-8)
++ Grad (sensitivities and transposed filter), i.e. one "solve plus Grad" of
+the reference's per-iteration hot path, on one GPU per rank.  Ranks are
+independent replicas (the path does not shard here); the printed value is
+the whole-job rate, timed with CUDA events and maximised over ranks.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tosp|reference]
+
+`--impl reference` times the reference algorithm on the host cores (the C/OpenMP
+restatement of the matrix-free SolveMGWOK path in oracle/) on a bounded sample.
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "topopt-slp-3d_b200")
+for _p in (ROOT, PKG):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+import numpy as np  # noqa: E402
+
+METRIC = "MG-PCG solves/s and p50/p99 latency at 1e-8 rel. residual, mixed vs FP64 GPU"
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as fh:
+            return json.load(fh), "measured"
+    return PEAKS_FALLBACK, "fallback"
+
+
+class Clocks:
+    """nvidia-smi samples during the timed region (SM clock, throttle reasons)."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [v.strip() for v in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = max(mx, float(f[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def run_reference(args, world, rank):
+    """Reference algorithm on the host cores (oracle C/OpenMP port)."""
+    if rank != 0:
+        return 0
+    from oracle.cpu_wok import CpuWok
+    from tosp.workloads import WORKLOADS, build_workload
+    spec = WORKLOADS[args.workload]
+    pb, n, xfil, spec = build_workload(args.workload, filter_fn=_cpu_filter(args.workload))
+    cores = os.cpu_count()
+    cw = CpuWok(pb, n, spec["ngrids"], 0.6, nthreads=cores)
+    f = pb.f_full()
+    its = spec.get("pcg_iterations_fp64")
+    samples = []
+
+    def one_step():
+        t0 = time.perf_counter()
+        cw.setup(xfil)
+        t1 = time.perf_counter()
+        u, it, per_it = cw.solve(np.zeros(f.size), f, 1e-8, 1000, max_iterations=1)
+        t2 = time.perf_counter()
+        cw.grad0(u)
+        t3 = time.perf_counter()
+        return (t1 - t0) + (its or 1) * float(np.mean(per_it)) + (t3 - t2), per_it
+
+    for _ in range(args.warmup):
+        one_step()
+    for _ in range(args.steps):
+        t, _ = one_step()
+        samples.append(t)
+    t_mean = float(np.mean(samples))
+    value = 1.0 / t_mean
+    sample = (f"per step: SetupGMG (Galerkin hierarchy + coarsest Cholesky) + 1 of {its} PCG iterations "
+              f"of the full {args.workload} solve + Grad, timed; solve time projected as setup + {its} x "
+              f"iteration + Grad")
+    line = {"impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * t_mean, 3),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": args.workload},
+            "cpu_baseline": {"value": round(value, 6), "unit": "solves/s", "cores": cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": round(value, 6), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+def _cpu_filter(workload):
+    """Host filter for building the uniform-filtered workload without a GPU."""
+    from oracle import filt
+    from tosp.workloads import WORKLOADS
+    spec = WORKLOADS[workload]
+    if spec["density"] != "uniform_filtered":
+        return None
+    nelx, nely, nelz = spec["dims"]
+    n = spec["n"]
+
+    def f(x):
+        W, w = filt.elem_neighborhood(nelx * n, nely * n, nelz * n, 1.0 / n, 1.0 / n, 1.0 / n, spec["rmin"], 1)
+        return filt.apply_filter(x, W, w, 1, False)
+    return f
+
+
+def cpu_baseline(args, pb, n, xfil, spec, it_fp64):
+    """Bounded CPU sample of the same workload (oracle port, all host cores)."""
+    from oracle.cpu_wok import CpuWok
+    cores = os.cpu_count()
+    cw = CpuWok(pb, n, spec["ngrids"], 0.6, nthreads=cores)
+    f = pb.f_full()
+    t0 = time.perf_counter()
+    cw.setup(xfil)
+    t1 = time.perf_counter()
+    u, it, per_it = cw.solve(np.zeros(f.size), f, 1e-8, 1000, max_iterations=args.cpu_iters)
+    t2 = time.perf_counter()
+    cw.grad0(u)
+    t3 = time.perf_counter()
+    t_solve = (t1 - t0) + it_fp64 * float(np.mean(per_it)) + (t3 - t2)
+    return {"value": round(1.0 / t_solve, 6), "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": (f"SetupGMG + {len(per_it)} of {it_fp64} PCG iterations (reference WOK algorithm: "
+                       f"AciProd coarse products) + Grad on the full workload, "
+                       f"{t3 - t0:.1f} s timed; full solve projected as setup + {it_fp64} x iteration + Grad")}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="tosp", choices=["tosp", "reference"])
+    ap.add_argument("--workload", default="cantilever192x96x96_mr2")
+    ap.add_argument("--fp64-steps", type=int, default=2)
+    ap.add_argument("--cpu-iters", type=int, default=2)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    if args.impl == "reference":
+        return run_reference(args, world, rank)
+
+    import torch
+    import torch.distributed as dist
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    import tosp
+    from tosp.workloads import build_workload
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- workload -------------------------------------------------------------
+    holder = {}
+
+    def gpu_filter(x):
+        return holder["s64"].ApplyFilter(x)
+
+    from tosp.workloads import WORKLOADS
+    spec0 = WORKLOADS[args.workload]
+    nelx, nely, nelz = spec0["dims"]
+    pb0 = tosp.problems.cantilever(nelx, nely, nelz)
+    mg = tosp.default_mg(ngrids=spec0["ngrids"], cycle=0, omega=0.6, smoothiter1=1, smoothiter2=1, tolMG=1e-8,
+                         maxiterMG=1000)
+    n = spec0["n"]
+    kw = dict(mr_n=n, p=3.0, emin=1e-9, opfilter=1, rmin=spec0["rmin"])
+    holder["s64"] = tosp.Solver(pb0, mg, precision=tosp.PREC_FP64, **kw)
+    pb, n, xfil, spec = build_workload(args.workload, filter_fn=gpu_filter)
+    s64 = holder["s64"]
+    smx = tosp.Solver(pb, mg, precision=tosp.PREC_MIXED, **kw)
+    dev = torch.device("cuda", local)
+    xfil_d = torch.tensor(xfil, dtype=torch.float64, device=dev)
+    f_d = torch.tensor(pb.f, dtype=torch.float64, device=dev)
+    u_d = torch.zeros(pb.freedofs.size, dtype=torch.float64, device=dev)
+    ufull_d = torch.zeros(3 * pb.nnodes, dtype=torch.float64, device=dev)
+    g_d = torch.zeros(xfil.size, dtype=torch.float64, device=dev)
+    fidx_d = torch.tensor(pb.freedofs, dtype=torch.int64, device=dev)
+    lib = tosp._lib
+    import ctypes as C
+
+    def step_dev(s):
+        s.SetupGMG(xfil_d)
+        u_d.zero_()
+        it, rr = C.c_int32(), C.c_double()
+        rc = lib.tosp_solve_mg(s.h, u_d.data_ptr(), f_d.data_ptr(), u_d.numel(), C.byref(it), C.byref(rr))
+        if rc != 0:
+            raise tosp.TospError(rc, lib.tosp_last_error(s.h).decode())
+        ufull_d.zero_()
+        ufull_d[fidx_d] = u_d
+        rc = lib.tosp_grad(s.h, ufull_d.data_ptr(), ufull_d.numel(), g_d.data_ptr(), None, g_d.numel())
+        if rc != 0:
+            raise tosp.TospError(rc, lib.tosp_last_error(s.h).decode())
+        return it.value, rr.value
+
+    def timed(s, steps, warmup):
+        for _ in range(warmup):
+            step_dev(s)
+        torch.cuda.synchronize()
+        barrier()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        its = []
+        l0 = tosp.kernel_launches()
+        ev[0].record()
+        for k in range(steps):
+            its.append(step_dev(s))
+            ev[k + 1].record()
+        torch.cuda.synchronize()
+        launches = tosp.kernel_launches() - l0
+        barrier()
+        per = [ev[k].elapsed_time(ev[k + 1]) for k in range(steps)]
+        return per, its, launches
+
+    clocks = Clocks(local)
+    clocks.start()
+    per_mx, its_mx, launches = timed(smx, args.steps, args.warmup)
+    clk = clocks.stop()
+    total_ms = max_over_ranks(sum(per_mx))
+    per_64, its_64, _ = timed(s64, args.fp64_steps, 1)
+    total64 = max_over_ranks(sum(per_64))
+    stats_mx = smx.stats()
+
+    # ---- end to end through the C ABI with pinned host buffers ------------------
+    xfil_h = torch.tensor(xfil, dtype=torch.float64).pin_memory()
+    f_h = torch.tensor(pb.f, dtype=torch.float64).pin_memory()
+    u_h = torch.zeros(pb.freedofs.size, dtype=torch.float64).pin_memory()
+    uf_h = torch.zeros(3 * pb.nnodes, dtype=torch.float64).pin_memory()
+    g_h = torch.zeros(xfil.size, dtype=torch.float64).pin_memory()
+    fidx_h = torch.tensor(pb.freedofs, dtype=torch.int64)
+
+    def step_host(s):
+        lib.tosp_setup_gmg(s.h, xfil_h.data_ptr(), xfil_h.numel())
+        u_h.zero_()
+        it, rr = C.c_int32(), C.c_double()
+        lib.tosp_solve_mg(s.h, u_h.data_ptr(), f_h.data_ptr(), u_h.numel(), C.byref(it), C.byref(rr))
+        uf_h.zero_()
+        uf_h[fidx_h] = u_h
+        lib.tosp_grad(s.h, uf_h.data_ptr(), uf_h.numel(), g_h.data_ptr(), None, g_h.numel())
+        return it.value
+
+    e2e_steps = max(1, min(args.steps, 3))
+    step_host(smx)
+    torch.cuda.synchronize()
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        step_host(smx)
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    h2d = 8 * (xfil.size + 2 * pb.freedofs.size + 3 * pb.nnodes)
+    d2h = 8 * (pb.freedofs.size + xfil.size)
+    # parity guard: the host path gives the same gradient as the device path
+    assert torch.allclose(g_h, g_d.cpu(), rtol=1e-6, atol=1e-12 * float(g_h.abs().max()))
+
+    # ---- kernel roofline (finest-level operators) ---------------------------------
+    peaks, peak_kind = load_peaks()
+    ms_op32 = smx.time_operator(tosp.PREC_MIXED, reps=10)
+    ms_op64 = smx.time_operator(tosp.PREC_FP64, reps=10)
+    ndof, nsub, nel = 3 * pb.nnodes, xfil.size, pb.nelem
+    bytes32 = 4 * ndof + 4 * ndof + 2 * nsub + ndof      # x, y fp32, SIMP bf16, free mask
+    bytes64 = 8 * ndof + 8 * ndof + 8 * nsub + ndof
+    flops = nel * n ** 3 * 1200                           # 576 FMA + 24 scalings per sub-block
+    it_mx = its_mx[-1][0]
+    applies32 = 2 * (it_mx - 1)                           # residual + post-smooth per V-cycle
+    applies64 = it_mx                                     # initial residual + one per iteration
+    traffic = None
+    tp = os.path.join(ROOT, "profiles", "operator_traffic.json")
+    if os.path.exists(tp):
+        traffic = json.load(open(tp)).get(args.workload, {}).get("fp32_operator_bytes_per_launch")
+    ach32 = bytes32 / (ms_op32 * 1e-3) / 1e9
+    ach64_tf = flops / (ms_op64 * 1e-3) / 1e12
+    roofline = {"bound": "hbm", "achieved": round(ach32, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+                "frac": round(ach32 / peaks["hbm_gbs"], 4), "traffic": traffic,
+                "kernel": "k_fine_apply<float,bf16> (V-cycle finest-level operator)",
+                "algorithmic_bytes_per_launch": bytes32, "ms_per_launch": round(ms_op32, 4),
+                "peak_source": peak_kind}
+    kernels = {
+        "fine_op_fp32": {"ms": round(ms_op32, 4), "GBps": round(ach32, 1), "per_solve": applies32,
+                         "share_of_step": round(applies32 * ms_op32 / (total_ms / args.steps), 3)},
+        "fine_op_fp64": {"ms": round(ms_op64, 4), "TFLOPs_fp64": round(ach64_tf, 2),
+                         "GBps": round(bytes64 / (ms_op64 * 1e-3) / 1e9, 1), "per_solve": applies64,
+                         "share_of_step": round(applies64 * ms_op64 / (total_ms / args.steps), 3)},
+    }
+
+    value = world * args.steps / (total_ms * 1e-3)
+    lat = np.array(per_mx)
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64 outer CG / f32+bf16 V-cycle",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "mesh": list(spec["dims"]), "mr_n": n, "ndof": ndof,
+                   "nfree": int(pb.freedofs.size), "density_elements": int(nsub), "ngrids": spec["ngrids"],
+                   "cycle": "V", "omega": 0.6, "smooth": "1+1 Jacobi", "tol": 1e-8,
+                   "l2": "inputs larger than L2 (densities 113 MB, vectors 44 MB each)",
+                   "parallelism": f"replicas x{world}"},
+        "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3), "p99": round(float(np.percentile(lat, 99)), 3)},
+        "pcg_iterations": {"mixed": it_mx, "fp64": its_64[-1][0]},
+        "relres": {"mixed": its_mx[-1][1], "fp64": its_64[-1][1]},
+        "fp64": {"value": round(world * args.fp64_steps / (total64 * 1e-3), 4), "unit": "solves/s",
+                 "ms_per_step": round(total64 / args.fp64_steps, 3)},
+        "mixed_over_fp64": round((args.steps / total_ms) / (args.fp64_steps / total64), 3),
+        "setup_ms": round(stats_mx["ms_setup"], 3),
+        "e2e": {"value": round(world * e2e_steps / e2e_s, 4), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": int(launches),
+        "roofline": roofline,
+        "kernels": kernels,
+        "clocks": clk,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(args, pb, n, xfil, spec, its_64[-1][0])
+    if rank == 0:
+        print(json.dumps(line))
+    smx.close()
+    s64.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,185 @@
+/*
+ * tosp.h - C ABI of the B200 (sm_100a) equilibrium-solve library for
+ * TopOpt-SLP-3D ("tosp").
+ *
+ * The entry points replace, one for one, the MATLAB functions on the
+ * reference's per-iteration solve path.  Paths are relative to the reference
+ * project; "I/" abbreviates its "Implementation/" folder.  A MEX gateway keeps
+ * the MATLAB names and argument lists; heavy MATLAB arguments (A, P, M, R,
+ * perm, kv, W) become state held by an opaque handle.
+ *
+ * Conventions
+ *   - Node numbering, dof numbering and element order are the reference's:
+ *     node = (z*nx + x)*ny + y (y is the vertical axis), dof = 3*node + c.
+ *   - Index arrays crossing the ABI are 1-based int64 (MATLAB convention).
+ *   - Vectors are float64.  Every pointer argument may be host memory or CUDA
+ *     device memory of the handle's device (detected per call); device
+ *     pointers avoid host<->device copies.
+ *   - Every call returns a status code (TOSP_OK = 0); tosp_last_error() gives
+ *     the message of the last failing call on a handle.
+ *   - Calls on one handle are serialised on that handle's CUDA stream and
+ *     return after their results are written.  Distinct handles are
+ *     independent and may be used from different host threads.
+ */
+#ifndef TOSP_H
+#define TOSP_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ----------------------------------------------------- */
+#define TOSP_OK               0
+#define TOSP_NOT_CONVERGED    1   /* iteration cap reached (the reference returns silently) */
+#define TOSP_ERR_BAD_ARG     -1
+#define TOSP_ERR_CUDA        -2
+#define TOSP_ERR_OOM         -3   /* device allocation failed / over the HBM budget */
+#define TOSP_ERR_BREAKDOWN   -4   /* non-finite or non-positive curvature in CG */
+#define TOSP_ERR_UNSUPPORTED -5
+#define TOSP_ERR_STATE       -6   /* call order: e.g. solve before setup */
+#define TOSP_ERR_CANCELLED   -7
+#define TOSP_ERR_TIMEOUT     -8
+
+/* ---- precision of the multigrid preconditioner ------------------------ */
+#define TOSP_PREC_FP64   0   /* every level in FP64 (the reference's arithmetic) */
+#define TOSP_PREC_MIXED  1   /* V-cycle in FP32 with BF16 SIMP factors; outer CG,
+                                 coarsest solve, Grad and filter in FP64 */
+
+typedef struct tosp_handle tosp_handle;
+
+/* The fields of the reference's `str` struct used on the solve path
+ * (I/EnterData.m, I/StartMR.m) plus the SIMP/filter scalars that StrSLP
+ * passes to GlobalStiffMatrix/KelemProd/Grad/ApplyFilter. */
+typedef struct tosp_problem {
+    int32_t nelx, nely, nelz;      /* str.nelx/nely/nelz (displacement mesh)        */
+    double  el, eh, ew;            /* str.el/eh/ew element sizes                    */
+    double  E, nu;                 /* str.E, str.nu                                  */
+    double  p, emin;               /* SIMP exponent, void Young's modulus           */
+    int32_t mr_n;                  /* mr.n density sub-elements per direction (1 = mr.op false) */
+    int32_t opfilter;              /* 0 none, 1 Gaussian, 2 hat (I/ElemNeighborhood.m) */
+    double  rmin;                  /* filter radius, physical units                 */
+    const int64_t *freedofs;       /* str.freedofs, 1-based, ascending              */
+    int64_t nfree;
+    const int64_t *fixed_dens;     /* fixed elements of the density (= design) mesh, 1-based; may be NULL */
+    int64_t nfixed_dens;
+    const int64_t *free_dens_g;    /* str.freeDensG: displacement elements with sensitivities,
+                                      1-based; NULL = all elements                   */
+    int64_t nfree_dens_g;
+} tosp_problem;
+
+/* mg.* fields of I/TopOpt3D.m:171-190 used by the geometric multigrid. */
+typedef struct tosp_mg_params {
+    int32_t ngrids;        /* mg.ngrids (raised by the nmaxchol rule like I/StartStrSLP.m:123-133) */
+    int32_t cycle;         /* 0 V, 1 W, 2 full-multigrid V (mg.cycle)                  */
+    int32_t smoother;      /* 0 damped Jacobi (the only smoother of the matrix-free path) */
+    double  omega;         /* mg.omega                                                 */
+    int32_t smoothiter1;   /* pre-smoothing sweeps                                     */
+    int32_t smoothiter2;   /* post-smoothing sweeps                                    */
+    double  tolMG;         /* relative residual tolerance                             */
+    int32_t maxiterMG;     /* iteration cap                                            */
+    int32_t nmaxchol;      /* largest coarsest-grid system for the direct solve        */
+} tosp_mg_params;
+
+/* Statistics of the last tosp_solve_mg call. */
+typedef struct tosp_solve_stats {
+    int32_t it;            /* the reference's `it` (iterations + 1)                   */
+    double  relres;        /* final ||f - K u|| / ||f|| as tracked by CG              */
+    double  ms_setup;      /* device time of the last setup (tosp_setup_gmg)          */
+    double  ms_solve;      /* device time of the last solve                           */
+} tosp_solve_stats;
+
+/* Library version string. */
+const char *tosp_version(void);
+
+/* Fill *mg with the reference defaults of I/TopOpt3D.m:171-190 (W-cycle,
+ * Jacobi, omega 0.5, 1+1 sweeps, tol 1e-8, 5000 iterations, nmaxchol 60000,
+ * ngrids 3). */
+void tosp_default_mg_params(tosp_mg_params *mg);
+
+/* Create a solver for one problem on the current CUDA device.  Builds the
+ * sub-element stiffness blocks (I/ElemStiffMatrixGQMR.m:1), the dof/density
+ * maps (I/DegreesOfFreedom.m:1, I/StartMR.m:58-83), the filter weights
+ * (I/ElemNeighborhood.m:1) and the multigrid geometry (I/SetupGMG.m:16-44).
+ * `precision` is TOSP_PREC_FP64 or TOSP_PREC_MIXED. */
+int tosp_create(const tosp_problem *prob, const tosp_mg_params *mg, int32_t precision,
+                tosp_handle **out);
+
+/* Free a handle and all its device memory. */
+int tosp_destroy(tosp_handle *h);
+
+/* Message of the last failing call on `h` (or of the last failing
+ * tosp_create on this thread when h == NULL). */
+const char *tosp_last_error(const tosp_handle *h);
+
+/* Effective number of grids and coarsest-grid system size after the level rules. */
+int tosp_info(const tosp_handle *h, int32_t *ngrids, int64_t *ncoarse, int64_t *device_bytes);
+
+/* Replace the free dofs (and the load vector's support) after Elem2Fix fixes
+ * displacements: replaces the resetup of I/StrSLP.m:196-203.  The hierarchy is
+ * rebuilt by the next tosp_setup_gmg. */
+int tosp_set_freedofs(tosp_handle *h, const int64_t *freedofs, int64_t nfree);
+
+/* Densities -> K(rho) and the whole multigrid hierarchy.  Replaces
+ * GlobalStiffMatrix (I/GlobalStiffMatrix.m:1) + SetupGMG (I/SetupGMG.m:1), the
+ * Galerkin refresh of I/StrSLP.m:345-365 and SetupGMGWOK
+ * (I/WOK/SetupGMGWOK.m:1).  `xfil` are the filtered densities on the density
+ * mesh (length nelem*mr_n^3, reference element order). */
+int tosp_setup_gmg(tosp_handle *h, const double *xfil, int64_t ndens);
+
+/* y = K(rho) x on the free dofs: KelemProd (I/WOK/KelemProd.m:1). */
+int tosp_kelem_prod(tosp_handle *h, const double *x, double *y, int64_t nfree);
+
+/* One preconditioner application s = cycle(r) (VCycle/WCycle/FMVCycle,
+ * I/VCycle.m:1, I/WCycle.m:1, I/FMVCycle.m:1) on free-dof vectors. */
+int tosp_mg_cycle(tosp_handle *h, const double *r, double *s, int64_t nfree);
+
+/* MG-preconditioned CG: SolveMG (I/SolveMG.m:1) / SolveMGWOK
+ * (I/WOK/SolveMGWOK.m:1).  `x` is the warm start on entry and the solution on
+ * exit; `f` the load on the free dofs; *it receives the reference's `it`.
+ * Returns TOSP_NOT_CONVERGED (results still written) at the iteration cap. */
+int tosp_solve_mg(tosp_handle *h, double *x, const double *f, int64_t nfree,
+                  int32_t *it, double *relres);
+
+/* Compliance sensitivities followed by the transposed filter: Grad
+ * (I/Grad.m:1) / GradWOK (I/WOK/GradWOK.m:1).  `u` is the displacement on all
+ * 3*nnodes dofs; `fgrad` has one entry per density element.  The densities
+ * are those of the last tosp_setup_gmg.  `fgrad0` (may be NULL) receives the
+ * unfiltered sensitivities. */
+int tosp_grad(tosp_handle *h, const double *u, int64_t nfull, double *fgrad, double *fgrad0,
+              int64_t ndens);
+
+/* Filter: ApplyFilter (I/ApplyFilter.m:1) / ApplyFilterWOK
+ * (I/WOK/ApplyFilterWOK.m:1); trans = 0: (W x)./w, trans = 1: W'(x./w). */
+int tosp_apply_filter(tosp_handle *h, const double *x, double *y, int64_t ndens, int32_t trans);
+
+/* Row sums w of the filter matrix (the `w` of I/ElemNeighborhood.m:181). */
+int tosp_filter_weights(tosp_handle *h, double *w, int64_t ndens);
+
+/* Compliance F = f' u on the free dofs (I/StrSLP.m:167,424), FP64. */
+int tosp_compliance(tosp_handle *h, const double *f, const double *u, int64_t nfree, double *F);
+
+/* Statistics of the last setup/solve on the handle. */
+int tosp_last_stats(const tosp_handle *h, tosp_solve_stats *st);
+
+/* Number of kernel launches this library has issued since it was loaded
+ * (all handles).  Instrumentation for benchmarks. */
+int64_t tosp_kernel_launches(void);
+
+/* Time `reps` launches of the finest-level operator kernel on the handle's
+ * stream with CUDA events bracketing each launch (inputs are the handle's
+ * current vectors): `precision` TOSP_PREC_FP64 times the FP64 kernel of the
+ * outer CG, TOSP_PREC_MIXED the FP32/BF16 kernel of the V-cycle (mixed
+ * handles only).  Writes the mean device time per launch in ms. */
+int tosp_time_operator(tosp_handle *h, int32_t precision, int32_t reps, double *ms_per_launch);
+
+/* Host-only: the n^3 sub-element stiffness blocks kv (576 x n^3, column s is
+ * k{s}(:), column-major) of I/ElemStiffMatrixGQMR.m:1 for hex8 elements. */
+int tosp_elem_stiff_mr(double el, double eh, double ew, double nu, int32_t n, double *kv);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TOSP_H */

@@ -1,0 +1,231 @@
+"""GPU parity: the CUDA library (through the C ABI) against the oracle.
+
+Tolerances (FP64 path): operator and single cycles <= 1e-12 relative (only
+summation order differs); Grad/filter <= 1e-12; full solves: same iteration
+count within one, relative residual <= tolMG checked with the oracle's own
+operator, compliance within 1e-9 relative of the oracle solve.  Mixed path:
+relative residual <= 1e-8 (checked with the oracle operator) and compliance
+within 1e-6 of the FP64 oracle.
+"""
+import numpy as np
+import pytest
+
+from oracle import fem, filt, gmg
+from tosp import problems as P
+
+pytestmark = pytest.mark.gpu
+
+P_SIMP, EMIN = 3.0, 1e-9
+
+
+def rel(a, b):
+    return np.abs(a - b).max() / max(np.abs(b).max(), 1e-300)
+
+
+def make(pb, n, seed=0, lo=0.001):
+    return np.random.default_rng(seed).uniform(lo, 1, pb.nelem * n ** 3)
+
+
+def oracle_hier(pb, n, dens, ngrids, omega, el=1.0):
+    ks = fem.elem_stiff_gqmr(pb.el, pb.eh, pb.ew, pb.nu, n)
+    K = fem.global_stiff_matrix(pb.nelx, pb.nely, pb.nelz, ks, dens, P_SIMP, EMIN, pb.freedofs)
+    H = gmg.setup_gmg(K, pb.nelx, pb.nely, pb.nelz, pb.freedofs, ngrids, omega)
+    return ks, K, H
+
+
+def solver(tosp, pb, n, prec=0, **mgkw):
+    kw = dict(ngrids=3, cycle=0, omega=0.6, tolMG=1e-8, maxiterMG=500)
+    kw.update(mgkw)
+    return tosp.Solver(pb, tosp.default_mg(**kw), precision=prec, mr_n=n, p=P_SIMP, emin=EMIN, opfilter=1,
+                       rmin=1.0 if n > 1 else 1.5)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3])
+def test_elem_stiff_matches_oracle(tosp_mod, n):
+    kv = tosp_mod.ElemStiffMatrixGQMR(1.0, 0.5, 2.0, 0.3, n)
+    ks = fem.elem_stiff_gqmr(1.0, 0.5, 2.0, 0.3, n)
+    assert rel(kv, fem.kv_matrix(ks)) <= 1e-13
+
+
+@pytest.mark.parametrize("dims,n", [((8, 4, 4), 2), ((6, 10, 2), 1), ((4, 4, 4), 3), ((16, 8, 8), 1),
+                                    ((10, 9, 3), 2), ((12, 16, 6), 2)])
+def test_kelem_prod_parity(tosp_mod, dims, n):
+    pb = P.cantilever(*dims)
+    dens = make(pb, n, seed=sum(dims))
+    s = solver(tosp_mod, pb, n)
+    s.SetupGMG(dens)
+    ks = fem.elem_stiff_gqmr(1, 1, 1, 0.3, n)
+    x = np.random.default_rng(1).standard_normal(pb.freedofs.size)
+    y = s.KelemProd(x)
+    yo = fem.kelem_prod(pb.nelx, pb.nely, pb.nelz, ks, dens, P_SIMP, EMIN, pb.freedofs, x)
+    assert rel(y, yo) <= 1e-12
+
+
+@pytest.mark.parametrize("cycle", [0, 1, 2])
+@pytest.mark.parametrize("dims,n,ngrids", [((8, 4, 4), 2, 3), ((16, 8, 8), 1, 3), ((16, 8, 8), 1, 4),
+                                           ((8, 8, 4), 3, 2)])
+def test_cycle_parity(tosp_mod, cycle, dims, n, ngrids):
+    pb = P.cantilever(*dims)
+    dens = make(pb, n, seed=7)
+    ks, K, H = oracle_hier(pb, n, dens, ngrids, 0.6)
+    s = solver(tosp_mod, pb, n, ngrids=ngrids, cycle=cycle)
+    s.SetupGMG(dens)
+    r = np.random.default_rng(2).standard_normal(pb.freedofs.size)
+    z = s.MGCycle(r)
+    zo = gmg.precondition(H, r, cycle, 1, 1)
+    assert rel(z, zo) <= 1e-10
+
+
+@pytest.mark.parametrize("cycle", [0, 1, 2])
+def test_solve_parity(tosp_mod, cycle):
+    pb = P.cantilever(16, 8, 8)
+    n = 2
+    dens = make(pb, n, seed=11)
+    ks, K, H = oracle_hier(pb, n, dens, 3, 0.6)
+    uo, ito = gmg.solve_mg(H, np.zeros(pb.f.size), pb.f, cycle, 1, 1, 1e-8, 500)
+    s = solver(tosp_mod, pb, n, cycle=cycle)
+    s.SetupGMG(dens)
+    u, it, relres, rc = s.SolveMG(np.zeros(pb.f.size), pb.f)
+    assert rc == 0
+    assert abs(it - ito) <= 1
+    assert np.linalg.norm(pb.f - K @ u) <= 1e-8 * np.linalg.norm(pb.f)
+    assert abs(pb.f @ u - pb.f @ uo) <= 1e-9 * abs(pb.f @ uo)
+    assert abs(s.Compliance(pb.f, u) - pb.f @ u) <= 1e-14 * abs(pb.f @ u)
+
+
+def test_solve_warm_start_and_iteration_cap(tosp_mod):
+    pb = P.cantilever(8, 4, 4)
+    dens = make(pb, 1, seed=5)
+    s = solver(tosp_mod, pb, 1, maxiterMG=2)
+    s.SetupGMG(dens)
+    u, it, rr, rc = s.SolveMG(np.zeros(pb.f.size), pb.f)
+    assert rc == 1 and it == 3          # the reference exits with it = maxiterMG + 1
+    s2 = solver(tosp_mod, pb, 1)
+    s2.SetupGMG(dens)
+    u2, it2, _, _ = s2.SolveMG(np.zeros(pb.f.size), pb.f)
+    u3, it3, _, _ = s2.SolveMG(u2, pb.f)  # warm start at the solution: no iteration (pcgp.opu0)
+    assert it3 <= 2
+
+
+@pytest.mark.parametrize("seed", [0, 13])
+def test_mixed_precision_solve(tosp_mod, seed):
+    pb = P.cantilever(16, 8, 8)
+    n = 2
+    dens = make(pb, n, seed=seed)
+    ks, K, H = oracle_hier(pb, n, dens, 3, 0.6)
+    uo, ito = gmg.solve_mg(H, np.zeros(pb.f.size), pb.f, 0, 1, 1, 1e-8, 500)
+    s = solver(tosp_mod, pb, n, prec=1)
+    s.SetupGMG(dens)
+    u, it, relres, rc = s.SolveMG(np.zeros(pb.f.size), pb.f)
+    assert rc == 0
+    assert np.linalg.norm(pb.f - K @ u) <= 1.0001e-8 * np.linalg.norm(pb.f)
+    assert abs(pb.f @ u - pb.f @ uo) <= 1e-6 * abs(pb.f @ uo)
+    # an FP32 V-cycle on i.i.d. densities with 1e9 stiffness contrast costs
+    # extra outer iterations (seed 13: 34 -> ~50, also in a NumPy FP32 emulation)
+    assert it <= 2 * ito
+
+
+@pytest.mark.parametrize("opfilter,rmin,n,sizes", [(1, 1.5, 1, (1, 1, 1)), (2, 2.5, 1, (1.0, 0.5, 2.0)),
+                                                   (1, 1.0, 2, (1, 1, 1)), (2, 1.2, 3, (1, 1, 1))])
+def test_filter_parity(tosp_mod, opfilter, rmin, n, sizes):
+    el, eh, ew = sizes
+    pb = P.build(6, 4, 4, [[0, 0, 0, 4 * eh, 0, 4 * ew, 1, 1, 1]], [[6 * el, 6 * el, 0, 0, 0, 0, 0, -1, 0]],
+                 el=el, eh=eh, ew=ew)
+    nd = pb.nelem * n ** 3
+    fixed = np.array([0, 5, 17, nd - 1])
+    s = tosp_mod.Solver(pb, tosp_mod.default_mg(), mr_n=n, opfilter=opfilter, rmin=rmin, fixed_dens=fixed)
+    W, w = filt.elem_neighborhood(pb.nelx * n, pb.nely * n, pb.nelz * n, el / n, eh / n, ew / n, rmin, opfilter,
+                                  fixed=fixed)
+    x = np.random.default_rng(4).uniform(0, 1, nd)
+    assert rel(s.FilterWeights(), w) <= 1e-13
+    assert rel(s.ApplyFilter(x), filt.apply_filter(x, W, w, opfilter, False)) <= 1e-13
+    assert rel(s.ApplyFilter(x, trans=True), filt.apply_filter(x, W, w, opfilter, True)) <= 1e-13
+
+
+@pytest.mark.parametrize("n", [1, 2, 3])
+def test_grad_parity(tosp_mod, n):
+    pb = P.cantilever(8, 4, 4)
+    dens = make(pb, n, seed=21)
+    free_g = np.arange(0, pb.nelem, 2) if n == 2 else None
+    rmin = 1.0 if n > 1 else 1.5
+    s = tosp_mod.Solver(pb, tosp_mod.default_mg(ngrids=3, cycle=0, omega=0.6), mr_n=n, p=P_SIMP, emin=EMIN,
+                        opfilter=1, rmin=rmin, free_dens_g=free_g)
+    s.SetupGMG(dens)
+    u = np.random.default_rng(9).standard_normal(3 * pb.nnodes)
+    u[np.setdiff1d(np.arange(3 * pb.nnodes), pb.freedofs)] = 0.0
+    g, g0 = s.Grad(u, return_unfiltered=True)
+    ks = fem.elem_stiff_gqmr(1, 1, 1, 0.3, n)
+    W, w = filt.elem_neighborhood(pb.nelx * n, pb.nely * n, pb.nelz * n, 1 / n, 1 / n, 1 / n, rmin, 1)
+    go, g0o = filt.grad(pb.nelx, pb.nely, pb.nelz, ks, u, dens, P_SIMP, EMIN, W, w, 1, free_elems=free_g)
+    assert rel(g0, g0o) <= 1e-12
+    assert rel(g, go) <= 1e-12
+
+
+def test_device_pointer_path(tosp_mod):
+    torch = pytest.importorskip("torch")
+    pb = P.cantilever(8, 4, 4)
+    dens = make(pb, 2, seed=3)
+    s = solver(tosp_mod, pb, 2)
+    s.SetupGMG(torch.tensor(dens, device="cuda"))
+    x = np.random.default_rng(1).standard_normal(pb.freedofs.size)
+    y_host = s.KelemProd(x)
+    xd = torch.tensor(x, device="cuda")
+    yd = torch.empty_like(xd)
+    rc = tosp_mod._lib.tosp_kelem_prod(s.h, xd.data_ptr(), yd.data_ptr(), x.size)
+    assert rc == 0
+    assert rel(yd.cpu().numpy(), y_host) <= 1e-14   # atomics: summation order may differ
+
+
+def test_error_codes(tosp_mod):
+    pb = P.cantilever(8, 4, 4)
+    s = solver(tosp_mod, pb, 1)
+    with pytest.raises(tosp_mod.TospError) as e:
+        s.SolveMG(np.zeros(pb.f.size), pb.f)           # before SetupGMG
+    assert e.value.code == -6
+    s.SetupGMG(make(pb, 1))
+    with pytest.raises(tosp_mod.TospError) as e:
+        s.KelemProd(np.zeros(5))
+    assert e.value.code == -1
+    odd = P.cantilever(9, 3, 3)                          # no geometric MG possible
+    so = solver(tosp_mod, odd, 1)
+    so.SetupGMG(make(odd, 1))
+    so.KelemProd(np.ones(odd.freedofs.size))
+    with pytest.raises(tosp_mod.TospError) as e:
+        so.SolveMG(np.zeros(odd.f.size), odd.f)
+    assert e.value.code == -5
+    with pytest.raises(tosp_mod.TospError):
+        tosp_mod.Solver(pb, tosp_mod.default_mg(cycle=7))
+
+
+def test_set_freedofs_resetup(tosp_mod):
+    """Elem2Fix-style change of the free dofs (I/StrSLP.m:196-203)."""
+    pb = P.cantilever(8, 4, 4)
+    dens = make(pb, 2, seed=8)
+    s = solver(tosp_mod, pb, 2)
+    fd2 = pb.freedofs[pb.freedofs % 7 != 3]
+    s.SetFreedofs(fd2)
+    s.SetupGMG(dens)
+    ks = fem.elem_stiff_gqmr(1, 1, 1, 0.3, 2)
+    x = np.random.default_rng(0).standard_normal(fd2.size)
+    assert rel(s.KelemProd(x), fem.kelem_prod(8, 4, 4, ks, dens, P_SIMP, EMIN, fd2, x)) <= 1e-12
+    K = fem.global_stiff_matrix(8, 4, 4, ks, dens, P_SIMP, EMIN, fd2)
+    H = gmg.setup_gmg(K, 8, 4, 4, fd2, 3, 0.6)
+    r = np.random.default_rng(1).standard_normal(fd2.size)
+    assert rel(s.MGCycle(r), gmg.precondition(H, r, 0, 1, 1)) <= 1e-10
+
+
+def test_fixture_problem_solve(tosp_mod):
+    """A reference fixture (mbb96x16x16quarter, supports on three faces) end to end."""
+    import os
+    G = np.load(os.path.join(os.path.dirname(__file__), "golden", "fixtures.npz"))
+    name = "mbb96x16x16quarter"
+    nelx, nely, nelz = [int(v) for v in G[name + "/dims"]]
+    pb = P.build(nelx, nely, nelz, G[name + "/supp"], G[name + "/loads"])
+    dens = np.full(pb.nelem, 0.3)
+    ks, K, H = oracle_hier(pb, 1, dens, 3, 0.5)
+    uo, ito = gmg.solve_mg(H, np.zeros(pb.f.size), pb.f, 1, 1, 1, 1e-8, 500)
+    s = tosp_mod.Solver(pb, tosp_mod.default_mg(), mr_n=1, p=P_SIMP, emin=EMIN, rmin=1.5)
+    s.SetupGMG(dens)
+    u, it, rr, rc = s.SolveMG(np.zeros(pb.f.size), pb.f)
+    assert abs(it - ito) <= 1
+    assert abs(pb.f @ u - pb.f @ uo) <= 1e-9 * abs(pb.f @ uo)

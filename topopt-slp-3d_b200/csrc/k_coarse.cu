@@ -1,0 +1,407 @@
+// Multigrid levels: Galerkin coarse operators, stencil products, Jacobi
+// smoothing and the trilinear transfers.
+//
+// The reference forms A{l+1} = P{l}' A{l} P{l} with sparse products
+// (I/SetupGMG.m:45-49, I/StrSLP.m:345-346), P restricted to the free rows and
+// columns (I/Prolongation.m:53-55).  Here the same matrix is built element by
+// element: a coarse element E is the union of 8 children c, and
+//     Abar_E = sum_c  Pi_c' (M_c K_c M_c) Pi_c,
+// where Pi_c = W_c (x) I3 interpolates E's 8 nodes to c's 8 nodes and M_c zeroes
+// the child's fixed dofs.  Summing Abar_E over E and zeroing the coarse fixed
+// dofs gives P'AP on the free dofs exactly.  For the apply, the element
+// matrices are assembled into a 27-point node stencil of 3x3 blocks.
+#include "tosp_internal.h"
+
+namespace tosp {
+
+static int num_sms_c() {
+    static int n = 0;
+    if (!n) {
+        int dev;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    }
+    return n;
+}
+
+static unsigned grid_for(int64_t n, int threads, int max_per_sm = 16) {
+    int64_t b = (n + threads - 1) / threads;
+    int64_t cap = (int64_t)max_per_sm * num_sms_c();
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (unsigned)b;
+}
+
+__device__ __forceinline__ double phi1(int f, int A) {
+    const int d = f - 2 * A;
+    return d == 0 ? 1.0 : ((d == 1 || d == -1) ? 0.5 : 0.0);
+}
+
+// Interpolation weight of coarse local node A at the local node a of child c.
+__device__ __forceinline__ double wchild(int c, int a, int A) {
+    const int cdx = (c >> 1) & 1, cdy = c & 1, cdz = (c >> 2) & 1;
+    const int ax = (a >> 1) & 1, ay = a & 1, az = (a >> 2) & 1;
+    const int Ax = (A >> 1) & 1, Ay = A & 1, Az = (A >> 2) & 1;
+    return phi1(cdx + ax, Ax) * phi1(cdy + ay, Ay) * phi1(cdz + az, Az);
+}
+
+__device__ __forceinline__ int pidx(int i, int j) {   // packed upper index, i <= j
+    return i * 24 - (i * (i - 1)) / 2 + (j - i);
+}
+
+constexpr int CB_THREADS = 192;   // 576 / 3 entries per thread
+
+// One CTA per coarse element: accumulate the 8 children's triple products.
+// FROM_FINE: children are fine elements, K_c = sum_s w_s KE_s;
+// otherwise K_c is the stored element matrix of the finer level.
+template <bool FROM_FINE, int N>
+__global__ void __launch_bounds__(CB_THREADS)
+k_coarse_build(const double *__restrict__ w, const double *__restrict__ kepack, const double *__restrict__ Af,
+               const uint8_t *__restrict__ fmask, Grid gf, int nelx_d, int nely_d, double *__restrict__ Ac,
+               Grid gc) {
+    constexpr int NS = N * N * N;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *ke = reinterpret_cast<double *>(smem_raw);          // NS*300 (FROM_FINE only)
+    double *Kc = ke + (FROM_FINE ? NS * KE_PACK : 0);            // 576
+    double *T = Kc + 576;                                        // 576
+    double *Wc = T + 576;                                        // 64
+    double *wsub = Wc + 64;                                      // NS
+    uint8_t *fr = reinterpret_cast<uint8_t *>(wsub + NS);        // 24
+    const int tid = threadIdx.x;
+    if (FROM_FINE)
+        for (int i = tid; i < NS * KE_PACK; i += CB_THREADS) ke[i] = kepack[i];
+
+    for (int64_t E = blockIdx.x; E < gc.nelem; E += gridDim.x) {
+        const int cy = (int)(E % gc.nely), cx = (int)((E / gc.nely) % gc.nelx),
+                  cz = (int)(E / ((int64_t)gc.nely * gc.nelx));
+        double acc[3] = {0.0, 0.0, 0.0};
+#pragma unroll 1
+        for (int c = 0; c < 8; ++c) {
+            const int fx = 2 * cx + ((c >> 1) & 1), fy = 2 * cy + (c & 1), fz = 2 * cz + ((c >> 2) & 1);
+            __syncthreads();
+            if (tid < 64) Wc[tid] = wchild(c, tid >> 3, tid & 7);
+            if (tid < 24) {
+                const int a = tid / 3, comp = tid % 3;
+                const int64_t node = ((int64_t)(fz + ((a >> 2) & 1)) * gf.nx + (fx + ((a >> 1) & 1))) * gf.ny +
+                                     (fy + (a & 1));
+                fr[tid] = fmask[3 * node + comp];
+            }
+            if (FROM_FINE && tid < NS) {
+                const int s = tid, sy = s % N, sx = (s / N) % N, sz = s / (N * N);
+                wsub[s] = w[((int64_t)(fz * N + sz) * nelx_d + (fx * N + sx)) * nely_d + (fy * N + sy)];
+            }
+            __syncthreads();
+            const int64_t child = ((int64_t)fz * gf.nelx + fx) * gf.nely + fy;
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const int e = tid + r * CB_THREADS;
+                const int i = e / 24, j = e % 24;
+                double v;
+                if (FROM_FINE) {
+                    const int pi = i <= j ? pidx(i, j) : pidx(j, i);
+                    v = 0.0;
+                    for (int s = 0; s < NS; ++s) v += wsub[s] * ke[s * KE_PACK + pi];
+                } else {
+                    v = Af[child * 576 + e];
+                }
+                Kc[e] = (fr[i] && fr[j]) ? v : 0.0;
+            }
+            __syncthreads();
+            // T[i][B*3+cb] = sum_b Kc[i][b*3+cb] W[b][B]
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const int e = tid + r * CB_THREADS;
+                const int i = e / 24, j = e % 24, B = j / 3, cb = j % 3;
+                double v = 0.0;
+#pragma unroll
+                for (int b = 0; b < 8; ++b) v += Kc[i * 24 + b * 3 + cb] * Wc[b * 8 + B];
+                T[e] = v;
+            }
+            __syncthreads();
+            // Abar[A*3+ca][j] += sum_a W[a][A] T[a*3+ca][j]
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                const int e = tid + r * CB_THREADS;
+                const int i = e / 24, j = e % 24, A = i / 3, ca = i % 3;
+                double v = 0.0;
+#pragma unroll
+                for (int a = 0; a < 8; ++a) v += Wc[a * 8 + A] * T[(a * 3 + ca) * 24 + j];
+                acc[r] += v;
+            }
+        }
+#pragma unroll
+        for (int r = 0; r < 3; ++r) Ac[E * 576 + tid + r * CB_THREADS] = acc[r];
+    }
+}
+
+template <bool FROM_FINE, int N>
+static void launch_cb(const double *w, const double *kepack, const double *Af, const uint8_t *fm, const Grid &gf,
+                      int nelx_d, int nely_d, double *Ac, const Grid &gc, cudaStream_t st) {
+    constexpr int NS = N * N * N;
+    const size_t smem = sizeof(double) * ((FROM_FINE ? NS * KE_PACK : 0) + 576 * 2 + 64 + NS) + 32;
+    auto kern = k_coarse_build<FROM_FINE, N>;
+    cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, CB_THREADS, smem);
+    if (per_sm < 1) per_sm = 1;
+    int64_t grid = (int64_t)per_sm * num_sms_c();
+    if (grid > gc.nelem) grid = gc.nelem;
+    kern<<<(unsigned)grid, CB_THREADS, smem, st>>>(w, kepack, Af, fm, gf, nelx_d, nely_d, Ac, gc); count_launch();
+}
+
+void launch_coarse_from_fine(const double *w, const uint8_t *freemask_f, const double *kepack, double *Ac,
+                             const FineGeom &fg, const Grid &gc, int n, cudaStream_t st) {
+    if (n == 1) launch_cb<true, 1>(w, kepack, nullptr, freemask_f, fg.g, fg.nelx_d, fg.nely_d, Ac, gc, st);
+    else if (n == 2) launch_cb<true, 2>(w, kepack, nullptr, freemask_f, fg.g, fg.nelx_d, fg.nely_d, Ac, gc, st);
+    else launch_cb<true, 3>(w, kepack, nullptr, freemask_f, fg.g, fg.nelx_d, fg.nely_d, Ac, gc, st);
+}
+
+void launch_coarse_from_coarse(const double *Af, const uint8_t *freemask_f, const Grid &gf, double *Ac,
+                               const Grid &gc, cudaStream_t st) {
+    launch_cb<false, 1>(nullptr, nullptr, Af, freemask_f, gf, 0, 0, Ac, gc, st);
+}
+
+// ---------------------------------------------------------------------------
+// 27-point stencil assembly: block (I, I+o) = sum over the elements holding
+// both nodes of the matching 3x3 block, with the level's fixed dofs zeroed.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_assemble_stencil(const double *__restrict__ Ae, const uint8_t *__restrict__ fmask, Grid g,
+                                   T *__restrict__ stv, T *__restrict__ invdiag, double omega) {
+    for (int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; I < g.nnodes;
+         I += (int64_t)gridDim.x * blockDim.x) {
+        const int y = (int)(I % g.ny), x = (int)((I / g.ny) % g.nx), z = (int)(I / ((int64_t)g.ny * g.nx));
+        uint8_t fi[3];
+        for (int c = 0; c < 3; ++c) fi[c] = fmask[3 * I + c];
+        for (int o = 0; o < 27; ++o) {
+            const int oy = o % 3 - 1, ox = (o / 3) % 3 - 1, oz = o / 9 - 1;
+            double blk[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+            const int jx = x + ox, jy = y + oy, jz = z + oz;
+            const bool jin = jx >= 0 && jx < g.nx && jy >= 0 && jy < g.ny && jz >= 0 && jz < g.nz;
+            uint8_t fj[3] = {0, 0, 0};
+            if (jin) {
+                const int64_t J = ((int64_t)jz * g.nx + jx) * g.ny + jy;
+                for (int c = 0; c < 3; ++c) fj[c] = fmask[3 * J + c];
+                for (int d = 0; d < 8; ++d) {
+                    const int dx = (d >> 1) & 1, dy = d & 1, dz = (d >> 2) & 1;
+                    const int bx = dx + ox, by = dy + oy, bz = dz + oz;
+                    if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
+                    const int exx = x - dx, eyy = y - dy, ezz = z - dz;
+                    if (exx < 0 || exx >= g.nelx || eyy < 0 || eyy >= g.nely || ezz < 0 || ezz >= g.nelz) continue;
+                    const int64_t E = ((int64_t)ezz * g.nelx + exx) * g.nely + eyy;
+                    const int aI = dz * 4 + dx * 2 + dy, aJ = bz * 4 + bx * 2 + by;
+                    const double *m = Ae + E * 576;
+                    for (int ci = 0; ci < 3; ++ci)
+                        for (int cj = 0; cj < 3; ++cj) blk[ci * 3 + cj] += m[(aI * 3 + ci) * 24 + aJ * 3 + cj];
+                }
+            }
+            for (int ci = 0; ci < 3; ++ci)
+                for (int cj = 0; cj < 3; ++cj) {
+                    const double v = (fi[ci] && fj[cj]) ? blk[ci * 3 + cj] : 0.0;
+                    stv[(int64_t)(o * 9 + ci * 3 + cj) * g.nnodes + I] = (T)v;
+                    if (o == 13 && ci == cj) invdiag[3 * I + ci] = (T)((fi[ci] && v != 0.0) ? omega / v : 0.0);
+                }
+        }
+    }
+}
+
+template <typename T>
+void launch_assemble_stencil(const double *Ae, const uint8_t *freemask, const Grid &g, T *stencil, T *invdiag,
+                             double omega, cudaStream_t st) {
+    k_assemble_stencil<T><<<grid_for(g.nnodes, 128), 128, 0, st>>>(Ae, freemask, g, stencil, invdiag, omega); count_launch();
+}
+template void launch_assemble_stencil<double>(const double *, const uint8_t *, const Grid &, double *, double *,
+                                              double, cudaStream_t);
+template void launch_assemble_stencil<float>(const double *, const uint8_t *, const Grid &, float *, float *,
+                                             double, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Stencil products.  One thread per node, 3 dofs.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(128)
+k_stencil(const T *__restrict__ stv, const T *__restrict__ x, const T *__restrict__ b, const T *__restrict__ invdiag,
+          T *__restrict__ y, Grid g, int mode) {
+    for (int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; I < g.nnodes;
+         I += (int64_t)gridDim.x * blockDim.x) {
+        const int yy = (int)(I % g.ny), xx = (int)((I / g.ny) % g.nx), zz = (int)(I / ((int64_t)g.ny * g.nx));
+        T a0 = 0, a1 = 0, a2 = 0;
+#pragma unroll
+        for (int o = 0; o < 27; ++o) {
+            const int oy = o % 3 - 1, ox = (o / 3) % 3 - 1, oz = o / 9 - 1;
+            const int jx = xx + ox, jy = yy + oy, jz = zz + oz;
+            if (jx < 0 || jx >= g.nx || jy < 0 || jy >= g.ny || jz < 0 || jz >= g.nz) continue;
+            const int64_t J = I + ((int64_t)oz * g.nx + ox) * g.ny + oy;
+            const T x0 = x[3 * J], x1 = x[3 * J + 1], x2 = x[3 * J + 2];
+            const T *s = stv + (int64_t)(o * 9) * g.nnodes + I;
+            a0 += s[0] * x0 + s[g.nnodes] * x1 + s[2 * g.nnodes] * x2;
+            a1 += s[3 * g.nnodes] * x0 + s[4 * g.nnodes] * x1 + s[5 * g.nnodes] * x2;
+            a2 += s[6 * g.nnodes] * x0 + s[7 * g.nnodes] * x1 + s[8 * g.nnodes] * x2;
+        }
+        if (mode == 0) {
+            y[3 * I] = a0; y[3 * I + 1] = a1; y[3 * I + 2] = a2;
+        } else if (mode == 1) {
+            y[3 * I] = b[3 * I] - a0; y[3 * I + 1] = b[3 * I + 1] - a1; y[3 * I + 2] = b[3 * I + 2] - a2;
+        } else {
+            y[3 * I] = x[3 * I] + invdiag[3 * I] * (b[3 * I] - a0);
+            y[3 * I + 1] = x[3 * I + 1] + invdiag[3 * I + 1] * (b[3 * I + 1] - a1);
+            y[3 * I + 2] = x[3 * I + 2] + invdiag[3 * I + 2] * (b[3 * I + 2] - a2);
+        }
+    }
+}
+
+template <typename T>
+void launch_stencil(const T *st_vals, const T *x, const T *b, const T *invdiag, T *y, const Grid &g, int mode,
+                    cudaStream_t st) {
+    k_stencil<T><<<grid_for(g.nnodes, 128), 128, 0, st>>>(st_vals, x, b, invdiag, y, g, mode); count_launch();
+}
+template void launch_stencil<double>(const double *, const double *, const double *, const double *, double *,
+                                     const Grid &, int, cudaStream_t);
+template void launch_stencil<float>(const float *, const float *, const float *, const float *, float *,
+                                    const Grid &, int, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Elementwise smoother pieces for the matrix-free finest level.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_residual(const T *b, const T *t, T *r, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        r[i] = b[i] - t[i];
+}
+template <typename T>
+void launch_residual(const T *b, const T *t, T *r, int64_t n, cudaStream_t st) {
+    k_residual<T><<<grid_for(n, 256), 256, 0, st>>>(b, t, r, n); count_launch();
+}
+template void launch_residual<double>(const double *, const double *, double *, int64_t, cudaStream_t);
+template void launch_residual<float>(const float *, const float *, float *, int64_t, cudaStream_t);
+
+// x = x + invD (b - t), or x = invD b for the first sweep from a zero guess
+// (b - A*0 = b exactly, so the product is skipped).
+template <typename T>
+__global__ void k_jacobi(T *x, const T *b, const T *t, const T *invd, int64_t n, int first) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] = first ? invd[i] * b[i] : x[i] + invd[i] * (b[i] - t[i]);
+}
+template <typename T>
+void launch_jacobi_update(T *x, const T *b, const T *t, const T *invdiag, int64_t n, int first, cudaStream_t st) {
+    k_jacobi<T><<<grid_for(n, 256), 256, 0, st>>>(x, b, t, invdiag, n, first); count_launch();
+}
+template void launch_jacobi_update<double>(double *, const double *, const double *, const double *, int64_t, int,
+                                           cudaStream_t);
+template void launch_jacobi_update<float>(float *, const float *, const float *, const float *, int64_t, int,
+                                          cudaStream_t);
+
+template <typename T>
+__global__ void k_invert_diag(const T *diag, const uint8_t *fm, T *invd, double omega, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double d = (double)diag[i];
+        invd[i] = (T)((fm[i] && d != 0.0) ? omega / d : 0.0);
+    }
+}
+template <typename T>
+void launch_invert_diag(const T *diag, const uint8_t *freemask, T *invdiag, double omega, int64_t n,
+                        cudaStream_t st) {
+    k_invert_diag<T><<<grid_for(n, 256), 256, 0, st>>>(diag, freemask, invdiag, omega, n); count_launch();
+}
+template void launch_invert_diag<double>(const double *, const uint8_t *, double *, double, int64_t, cudaStream_t);
+
+// ---------------------------------------------------------------------------
+// Trilinear transfers (I/Prolongation.m:24-52 weights 1, 1/2, 1/4, 1/8).
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void k_prolong(const T *__restrict__ xc, T *__restrict__ xf, const uint8_t *__restrict__ fmf, Grid gf,
+                          Grid gc, int accumulate) {
+    for (int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; I < gf.nnodes;
+         I += (int64_t)gridDim.x * blockDim.x) {
+        const int fy = (int)(I % gf.ny), fx = (int)((I / gf.ny) % gf.nx), fz = (int)(I / ((int64_t)gf.ny * gf.nx));
+        const int x0 = fx >> 1, y0 = fy >> 1, z0 = fz >> 1;
+        const int nxs = (fx & 1) ? 2 : 1, nys = (fy & 1) ? 2 : 1, nzs = (fz & 1) ? 2 : 1;
+        const T wx = (fx & 1) ? T(0.5) : T(1), wy = (fy & 1) ? T(0.5) : T(1), wz = (fz & 1) ? T(0.5) : T(1);
+        T v0 = 0, v1 = 0, v2 = 0;
+        for (int kz = 0; kz < nzs; ++kz)
+            for (int kx = 0; kx < nxs; ++kx)
+                for (int ky = 0; ky < nys; ++ky) {
+                    const int64_t J = ((int64_t)(z0 + kz) * gc.nx + (x0 + kx)) * gc.ny + (y0 + ky);
+                    const T wt = wx * wy * wz;
+                    v0 += wt * xc[3 * J];
+                    v1 += wt * xc[3 * J + 1];
+                    v2 += wt * xc[3 * J + 2];
+                }
+        const T v[3] = {v0, v1, v2};
+        for (int c = 0; c < 3; ++c) {
+            const int64_t d = 3 * I + c;
+            if (accumulate) {
+                if (fmf[d]) xf[d] += v[c];
+            } else {
+                xf[d] = fmf[d] ? v[c] : T(0);
+            }
+        }
+    }
+}
+
+template <typename T>
+void launch_prolong(const T *xc, T *xf, const uint8_t *freemask_f, const Grid &gf, const Grid &gc, bool accumulate,
+                    cudaStream_t st) {
+    k_prolong<T><<<grid_for(gf.nnodes, 256), 256, 0, st>>>(xc, xf, freemask_f, gf, gc, accumulate ? 1 : 0); count_launch();
+}
+template void launch_prolong<double>(const double *, double *, const uint8_t *, const Grid &, const Grid &, bool,
+                                     cudaStream_t);
+template void launch_prolong<float>(const float *, float *, const uint8_t *, const Grid &, const Grid &, bool,
+                                    cudaStream_t);
+
+template <typename T>
+__global__ void k_restrict(const T *__restrict__ rf, T *__restrict__ bc, const uint8_t *__restrict__ fmc, Grid gf,
+                           Grid gc) {
+    for (int64_t J = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; J < gc.nnodes;
+         J += (int64_t)gridDim.x * blockDim.x) {
+        const int cy = (int)(J % gc.ny), cx = (int)((J / gc.ny) % gc.nx), cz = (int)(J / ((int64_t)gc.ny * gc.nx));
+        T v0 = 0, v1 = 0, v2 = 0;
+        for (int dz = -1; dz <= 1; ++dz) {
+            const int fz = 2 * cz + dz;
+            if (fz < 0 || fz >= gf.nz) continue;
+            for (int dx = -1; dx <= 1; ++dx) {
+                const int fx = 2 * cx + dx;
+                if (fx < 0 || fx >= gf.nx) continue;
+                for (int dy = -1; dy <= 1; ++dy) {
+                    const int fy = 2 * cy + dy;
+                    if (fy < 0 || fy >= gf.ny) continue;
+                    const T wt = (dx ? T(0.5) : T(1)) * (dy ? T(0.5) : T(1)) * (dz ? T(0.5) : T(1));
+                    const int64_t I = ((int64_t)fz * gf.nx + fx) * gf.ny + fy;
+                    v0 += wt * rf[3 * I];
+                    v1 += wt * rf[3 * I + 1];
+                    v2 += wt * rf[3 * I + 2];
+                }
+            }
+        }
+        bc[3 * J] = fmc[3 * J] ? v0 : T(0);
+        bc[3 * J + 1] = fmc[3 * J + 1] ? v1 : T(0);
+        bc[3 * J + 2] = fmc[3 * J + 2] ? v2 : T(0);
+    }
+}
+
+template <typename T>
+void launch_restrict(const T *rf, T *bc, const uint8_t *freemask_c, const Grid &gf, const Grid &gc, cudaStream_t st) {
+    k_restrict<T><<<grid_for(gc.nnodes, 256), 256, 0, st>>>(rf, bc, freemask_c, gf, gc); count_launch();
+}
+template void launch_restrict<double>(const double *, double *, const uint8_t *, const Grid &, const Grid &,
+                                      cudaStream_t);
+template void launch_restrict<float>(const float *, float *, const uint8_t *, const Grid &, const Grid &,
+                                     cudaStream_t);
+
+// Coarse dof is free when the fine dof at the same position is free
+// (I/Prolongation.m:38-46,54).
+__global__ void k_coarse_mask(const uint8_t *fmf, uint8_t *fmc, Grid gf, Grid gc) {
+    for (int64_t J = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; J < gc.nnodes;
+         J += (int64_t)gridDim.x * blockDim.x) {
+        const int cy = (int)(J % gc.ny), cx = (int)((J / gc.ny) % gc.nx), cz = (int)(J / ((int64_t)gc.ny * gc.nx));
+        const int64_t I = ((int64_t)(2 * cz) * gf.nx + 2 * cx) * gf.ny + 2 * cy;
+        for (int c = 0; c < 3; ++c) fmc[3 * J + c] = fmf[3 * I + c];
+    }
+}
+
+void launch_coarse_freemask(const uint8_t *freemask_f, uint8_t *freemask_c, const Grid &gf, const Grid &gc,
+                            cudaStream_t st) {
+    k_coarse_mask<<<grid_for(gc.nnodes, 256), 256, 0, st>>>(freemask_f, freemask_c, gf, gc); count_launch();
+}
+
+}  // namespace tosp

@@ -1,0 +1,126 @@
+// Vector kernels of the FP64 outer CG (I/SolveMG.m:26-53) and the free-dof
+// boundary conversions.  Dot products use a fixed two-stage reduction tree
+// (RED_BLOCKS partial sums, then one block), so results are bitwise
+// reproducible run to run.
+#include "tosp_internal.h"
+
+namespace tosp {
+
+static unsigned gridv(int64_t n) {
+    int64_t b = (n + 255) / 256;
+    if (b > 8192) b = 8192;
+    if (b < 1) b = 1;
+    return (unsigned)b;
+}
+
+__global__ void k_scatter(const double *v, const int64_t *idx, int64_t nfree, double *full) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nfree; i += (int64_t)gridDim.x * blockDim.x)
+        full[idx[i]] = v[i];
+}
+void launch_scatter_free(const double *v, const int64_t *idx, int64_t nfree, double *full, cudaStream_t st) {
+    k_scatter<<<gridv(nfree), 256, 0, st>>>(v, idx, nfree, full); count_launch();
+}
+
+__global__ void k_gather(const double *full, const int64_t *idx, int64_t nfree, double *v) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nfree; i += (int64_t)gridDim.x * blockDim.x)
+        v[i] = full[idx[i]];
+}
+void launch_gather_free(const double *full, const int64_t *idx, int64_t nfree, double *v, cudaStream_t st) {
+    k_gather<<<gridv(nfree), 256, 0, st>>>(full, idx, nfree, v); count_launch();
+}
+
+template <typename TI, typename TO>
+__global__ void k_convert(const TI *a, TO *b, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        b[i] = (TO)a[i];
+}
+template <typename TI, typename TO>
+void launch_convert(const TI *a, TO *b, int64_t n, cudaStream_t st) {
+    k_convert<TI, TO><<<gridv(n), 256, 0, st>>>(a, b, n); count_launch();
+}
+template void launch_convert<double, float>(const double *, float *, int64_t, cudaStream_t);
+template void launch_convert<float, double>(const float *, double *, int64_t, cudaStream_t);
+
+__device__ __forceinline__ double block_sum(double v, double *sh) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    double s = 0.0;
+    if (threadIdx.x == 0)
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) s += sh[i];
+    __syncthreads();
+    return s;   // valid in thread 0
+}
+
+__global__ void k_dot_partial(const double *a, const double *b, int64_t n, double *partials) {
+    __shared__ double sh[32];
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        s += a[i] * b[i];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+__global__ void k_reduce_final(const double *partials, int np, double *out) {
+    __shared__ double sh[32];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) s += partials[i];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) out[0] = s;
+}
+
+void launch_dot(const double *a, const double *b, int64_t n, double *partials, double *out, cudaStream_t st) {
+    k_dot_partial<<<RED_BLOCKS, 256, 0, st>>>(a, b, n, partials); count_launch();
+    k_reduce_final<<<1, 256, 0, st>>>(partials, RED_BLOCKS, out); count_launch();
+}
+
+// Scalar slots (see solver.cpp): 0 rho, 1 gamma2 (previous rho), 2 d'q, 3 r'r.
+__global__ void k_pcg_direction(double *d, const double *s, const double *scal, int64_t n, int first) {
+    const double beta = first ? 0.0 : scal[0] / scal[1];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        d[i] = first ? s[i] : beta * d[i] + s[i];
+}
+void launch_pcg_direction(double *d, const double *s, const double *scal, int64_t n, int first, cudaStream_t st) {
+    k_pcg_direction<<<gridv(n), 256, 0, st>>>(d, s, scal, n, first); count_launch();
+}
+
+// x += alpha d ; r -= alpha q ; partial sums of r'r  (alpha = rho / d'q)
+__global__ void k_pcg_update(double *x, double *r, const double *d, const double *q, const double *scal, int64_t n,
+                             double *partials) {
+    __shared__ double sh[32];
+    const double alpha = scal[0] / scal[2];
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        x[i] += alpha * d[i];
+        const double ri = r[i] - alpha * q[i];
+        r[i] = ri;
+        s += ri * ri;
+    }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+}
+
+// finalize r'r into slot 3 and roll gamma2 = rho
+__global__ void k_pcg_finalize(const double *partials, int np, double *scal) {
+    __shared__ double sh[32];
+    double s = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) s += partials[i];
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) {
+        scal[3] = s;
+        scal[1] = scal[0];
+    }
+}
+
+void launch_pcg_update(double *x, double *r, const double *d, const double *q, double *scal, double *partials,
+                       int64_t n, cudaStream_t st) {
+    k_pcg_update<<<RED_BLOCKS, 256, 0, st>>>(x, r, d, q, scal, n, partials); count_launch();
+    k_pcg_finalize<<<1, 256, 0, st>>>(partials, RED_BLOCKS, scal); count_launch();
+}
+
+__global__ void k_set_scalar(double *dst, const double *src) { *dst = *src; }
+void launch_set_scalar(double *dst, const double *src, cudaStream_t st) { k_set_scalar<<<1, 1, 0, st>>>(dst, src); count_launch(); }
+
+}  // namespace tosp

@@ -1,0 +1,919 @@
+// Handle, multigrid hierarchy, cycles and the MG-preconditioned CG, plus the
+// extern "C" entry points of tosp.h.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <utility>
+#include <string>
+#include <vector>
+
+#include "tosp_internal.h"
+
+using namespace tosp;
+
+#include <atomic>
+static std::atomic<long long> g_launches{0};
+void tosp::count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long tosp::launch_count() { return g_launches.load(std::memory_order_relaxed); }
+
+namespace {
+
+thread_local std::string g_create_error;
+
+struct Level {
+    Grid g;
+    uint8_t *fm = nullptr;     // free flag per dof
+    double *Ae = nullptr;      // Galerkin element matrices (levels >= 1), FP64
+    void *st = nullptr;        // 27-point stencil (levels 1..L-2), cycle precision
+    void *invd = nullptr;      // omega / diag(A), 0 on fixed dofs, cycle precision
+    void *b = nullptr, *x = nullptr, *r = nullptr, *t = nullptr;   // cycle vectors
+};
+
+}  // namespace
+
+struct tosp_handle {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    // problem
+    int n = 1, ns = 1, precision = TOSP_PREC_FP64;
+    double E = 1, nu = 0.3, p = 3, emin = 1e-9, el = 1, eh = 1, ew = 1, rmin = 1.5;
+    int opfilter = 1;
+    tosp_mg_params mg{};
+    int ngrids = 2;
+    bool mg_ok = true;         // false: no geometric hierarchy possible (operator/Grad/filter only)
+    std::string mg_msg;
+    FineGeom fg{};
+    Grid dens{};               // density (= design) mesh as a grid of elements
+    int64_t nfree = 0;
+    int64_t *d_freeidx = nullptr;
+    // constants
+    double *d_ke64 = nullptr;
+    float *d_ke32 = nullptr;
+    // densities
+    double *d_rho = nullptr, *d_w64 = nullptr;
+    __nv_bfloat16 *d_wbf = nullptr;
+    uint8_t *d_free_elem = nullptr;
+    // filter
+    FilterTap *d_taps = nullptr;
+    int ntaps = 0;
+    uint8_t *d_fixed = nullptr;
+    double *d_fw = nullptr;
+    // hierarchy
+    std::vector<Level> lev;
+    double *d_diag64 = nullptr;     // diag of the finest operator
+    double *d_Adense = nullptr, *d_Xinv = nullptr;
+    int64_t ncoarse = 0, npad = 0;
+    int *d_info = nullptr;
+    bool setup_done = false;
+    // CG (FP64, full-length vectors with zeros on fixed dofs)
+    double *cx = nullptr, *cr = nullptr, *cd = nullptr, *cq = nullptr, *cs = nullptr, *cf = nullptr;
+    double *d_partials = nullptr, *d_scal = nullptr, *h_scal = nullptr;
+    // staging
+    double *d_stage_a = nullptr, *d_stage_b = nullptr;
+    int64_t stage_len = 0;
+    double *d_ufull = nullptr, *d_g0 = nullptr, *d_gf = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    tosp_solve_stats stats{};
+    int64_t bytes = 0;
+    std::vector<void *> allocs;
+};
+
+namespace {
+
+#define CK(call)                                                                         \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess) {                                                         \
+            h->err = std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " #call; \
+            return (e_ == cudaErrorMemoryAllocation) ? TOSP_ERR_OOM : TOSP_ERR_CUDA;     \
+        }                                                                                \
+    } while (0)
+
+#define CKL()                                                                   \
+    do {                                                                        \
+        cudaError_t e_ = cudaGetLastError();                                    \
+        if (e_ != cudaSuccess) {                                                \
+            h->err = std::string("CUDA launch error: ") + cudaGetErrorString(e_); \
+            return TOSP_ERR_CUDA;                                               \
+        }                                                                       \
+    } while (0)
+
+#define TRY(x)                   \
+    do {                         \
+        int rc_ = (x);           \
+        if (rc_ != TOSP_OK) return rc_; \
+    } while (0)
+
+template <typename T>
+int dalloc(tosp_handle *h, T **p, int64_t count) {
+    *p = nullptr;
+    if (count <= 0) count = 1;
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, sizeof(T) * (size_t)count);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        h->err = "device allocation of " + std::to_string(sizeof(T) * count) + " bytes failed: " +
+                 cudaGetErrorString(e);
+        return TOSP_ERR_OOM;
+    }
+    h->allocs.push_back(q);
+    h->bytes += (int64_t)sizeof(T) * count;
+    *p = static_cast<T *>(q);
+    return TOSP_OK;
+}
+
+bool is_device_ptr(const void *p) {
+    if (!p) return false;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Copy `count` doubles from a host or device pointer into device memory.
+int load_vec(tosp_handle *h, double *dst, const double *src, int64_t count) {
+    CK(cudaMemcpyAsync(dst, src, sizeof(double) * count, cudaMemcpyDefault, h->stream));
+    return TOSP_OK;
+}
+int store_vec(tosp_handle *h, double *dst, const double *src, int64_t count) {
+    CK(cudaMemcpyAsync(dst, src, sizeof(double) * count, cudaMemcpyDefault, h->stream));
+    return TOSP_OK;
+}
+
+int sync(tosp_handle *h) {
+    CK(cudaStreamSynchronize(h->stream));
+    CKL();
+    return TOSP_OK;
+}
+
+// ----- level rules (I/StartStrSLP.m:107-133) --------------------------------
+int choose_levels(int nelx, int nely, int nelz, int ngrids, int nmaxchol, std::string &msg) {
+    auto divisible = [&](int k) {
+        const int m = 1 << (k - 1);
+        return nelx % m == 0 && nely % m == 0 && nelz % m == 0;
+    };
+    int ng = ngrids < 2 ? 2 : ngrids;
+    while (ng >= 2 && !divisible(ng)) --ng;
+    if (ng < 2) {
+        msg = "geometric multigrid needs even element counts (the reference falls back to AMG, not provided)";
+        return -1;
+    }
+    for (;;) {
+        const double m = (double)(1 << (ng - 1));
+        const double nc = (nelx / m + 1) * (nely / m + 1) * (nelz / m + 1) * 3;
+        if (nc <= nmaxchol) break;
+        if (divisible(ng + 1)) ++ng;
+        else {
+            msg = "coarsest system larger than nmaxchol and no further level possible "
+                  "(the reference switches to PCG on the coarsest grid, not provided)";
+            return -1;
+        }
+    }
+    return ng;
+}
+
+// ----- operators -------------------------------------------------------------
+// y = K x at the finest level in the cycle precision (zeroes y first).
+template <typename T>
+int fine_apply(tosp_handle *h, const T *x, T *y) {
+    CK(cudaMemsetAsync(y, 0, sizeof(T) * h->fg.g.ndof, h->stream));
+    if constexpr (sizeof(T) == 8) {
+        launch_fine_apply<double, double>(x, y, h->d_w64, h->lev[0].fm, h->d_ke64, h->fg, h->n, false, h->stream);
+    } else {
+        launch_fine_apply<float, __nv_bfloat16>(x, y, h->d_wbf, h->lev[0].fm, h->d_ke32, h->fg, h->n, false,
+                                                h->stream);
+    }
+    CKL();
+    return TOSP_OK;
+}
+
+int fine_apply64(tosp_handle *h, const double *x, double *y) { return fine_apply<double>(h, x, y); }
+
+template <typename T>
+int smooth(tosp_handle *h, int l, int niter, bool x_zero) {
+    Level &L = h->lev[l];
+    const int64_t nd = L.g.ndof;
+    T *b = (T *)L.b;
+    if (niter == 0 && x_zero) CK(cudaMemsetAsync(L.x, 0, sizeof(T) * nd, h->stream));
+    for (int it = 0; it < niter; ++it) {
+        const bool first = x_zero && it == 0;
+        if (first) {
+            launch_jacobi_update<T>((T *)L.x, b, nullptr, (const T *)L.invd, nd, 1, h->stream);
+        } else if (l == 0) {
+            TRY(fine_apply<T>(h, (const T *)L.x, (T *)L.t));
+            launch_jacobi_update<T>((T *)L.x, b, (const T *)L.t, (const T *)L.invd, nd, 0, h->stream);
+        } else {
+            launch_stencil<T>((const T *)L.st, (const T *)L.x, b, (const T *)L.invd, (T *)L.t, L.g, 2, h->stream);
+            std::swap(L.x, L.t);
+        }
+        CKL();
+    }
+    return TOSP_OK;
+}
+
+template <typename T>
+int residual(tosp_handle *h, int l) {
+    Level &L = h->lev[l];
+    if (l == 0) {
+        TRY(fine_apply<T>(h, (const T *)L.x, (T *)L.t));
+        launch_residual<T>((const T *)L.b, (const T *)L.t, (T *)L.r, L.g.ndof, h->stream);
+    } else {
+        launch_stencil<T>((const T *)L.st, (const T *)L.x, (const T *)L.b, nullptr, (T *)L.r, L.g, 1, h->stream);
+    }
+    CKL();
+    return TOSP_OK;
+}
+
+template <typename T>
+int coarse_solve(tosp_handle *h) {
+    Level &C = h->lev[h->ngrids - 1];
+    launch_dense_solve<T>(h->d_Xinv, (const T *)C.b, (T *)C.x, C.g.ndof, h->npad, h->stream);
+    CKL();
+    return TOSP_OK;
+}
+
+// VCycle / WCycle (I/VCycle.m:23-43, I/WCycle.m:23-44) on level l, right-hand
+// side lev[l].b, iterate lev[l].x (zero when x_zero).
+template <typename T>
+int cycle_vw(tosp_handle *h, int l, bool x_zero, bool wcycle) {
+    const int Lc = h->ngrids - 1;
+    Level &L = h->lev[l];
+    Level &C = h->lev[l + 1];
+    TRY(smooth<T>(h, l, h->mg.smoothiter1, x_zero));
+    TRY(residual<T>(h, l));
+    launch_restrict<T>((const T *)L.r, (T *)C.b, C.fm, L.g, C.g, h->stream);
+    CKL();
+    if (l + 1 == Lc) {
+        TRY(coarse_solve<T>(h));
+    } else {
+        TRY(cycle_vw<T>(h, l + 1, true, wcycle));
+        if (wcycle) TRY(cycle_vw<T>(h, l + 1, false, wcycle));
+    }
+    launch_prolong<T>((const T *)C.x, (T *)L.x, L.fm, L.g, C.g, true, h->stream);
+    CKL();
+    TRY(smooth<T>(h, l, h->mg.smoothiter2, false));
+    return TOSP_OK;
+}
+
+// FMVCycle (I/FMVCycle.m:22-39).
+template <typename T>
+int cycle_fmv(tosp_handle *h, int l) {
+    const int Lc = h->ngrids - 1;
+    Level &L = h->lev[l];
+    Level &C = h->lev[l + 1];
+    launch_restrict<T>((const T *)L.b, (T *)C.b, C.fm, L.g, C.g, h->stream);
+    CKL();
+    if (l + 1 == Lc) TRY(coarse_solve<T>(h));
+    else TRY(cycle_fmv<T>(h, l + 1));
+    launch_prolong<T>((const T *)C.x, (T *)L.x, L.fm, L.g, C.g, false, h->stream);
+    CKL();
+    return cycle_vw<T>(h, l, false, false);
+}
+
+// s = M^{-1} r on full-length FP64 vectors (r, s distinct from the level buffers).
+int precondition(tosp_handle *h, const double *r, double *s) {
+    Level &F = h->lev[0];
+    const int64_t nd = F.g.ndof;
+    if (h->precision == TOSP_PREC_FP64) {
+        CK(cudaMemcpyAsync(F.b, r, sizeof(double) * nd, cudaMemcpyDeviceToDevice, h->stream));
+        if (h->mg.cycle == 2) TRY(cycle_fmv<double>(h, 0));
+        else TRY(cycle_vw<double>(h, 0, true, h->mg.cycle == 1));
+        CK(cudaMemcpyAsync(s, F.x, sizeof(double) * nd, cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+        launch_convert<double, float>(r, (float *)F.b, nd, h->stream);
+        CKL();
+        if (h->mg.cycle == 2) TRY(cycle_fmv<float>(h, 0));
+        else TRY(cycle_vw<float>(h, 0, true, h->mg.cycle == 1));
+        launch_convert<float, double>((const float *)F.x, s, nd, h->stream);
+        CKL();
+    }
+    return TOSP_OK;
+}
+
+int ensure_stage(tosp_handle *h, int64_t len) {
+    if (h->stage_len >= len) return TOSP_OK;
+    TRY(dalloc(h, &h->d_stage_a, len));
+    TRY(dalloc(h, &h->d_stage_b, len));
+    h->stage_len = len;
+    return TOSP_OK;
+}
+
+// Free-dof vector (host or device) -> full-length device vector.
+int free_to_full(tosp_handle *h, const double *v, double *full) {
+    const double *src = v;
+    if (!is_device_ptr(v)) {
+        TRY(ensure_stage(h, h->nfree));
+        TRY(load_vec(h, h->d_stage_a, v, h->nfree));
+        src = h->d_stage_a;
+    }
+    CK(cudaMemsetAsync(full, 0, sizeof(double) * h->fg.g.ndof, h->stream));
+    launch_scatter_free(src, h->d_freeidx, h->nfree, full, h->stream);
+    CKL();
+    return TOSP_OK;
+}
+
+int full_to_free(tosp_handle *h, const double *full, double *v) {
+    if (is_device_ptr(v)) {
+        launch_gather_free(full, h->d_freeidx, h->nfree, v, h->stream);
+        CKL();
+        return TOSP_OK;
+    }
+    TRY(ensure_stage(h, h->nfree));
+    launch_gather_free(full, h->d_freeidx, h->nfree, h->d_stage_b, h->stream);
+    CKL();
+    TRY(store_vec(h, v, h->d_stage_b, h->nfree));
+    return TOSP_OK;
+}
+
+int build_masks(tosp_handle *h, const int64_t *freedofs, int64_t nfree) {
+    const Grid &g0 = h->lev[0].g;
+    std::vector<int64_t> idx(nfree);
+    std::vector<uint8_t> fm(g0.ndof, 0);
+    int64_t prev = -1;
+    for (int64_t i = 0; i < nfree; ++i) {
+        const int64_t d = freedofs[i] - 1;
+        if (d < 0 || d >= g0.ndof) {
+            h->err = "freedofs entry out of range at position " + std::to_string(i);
+            return TOSP_ERR_BAD_ARG;
+        }
+        if (d <= prev) {
+            h->err = "freedofs must be strictly ascending";
+            return TOSP_ERR_BAD_ARG;
+        }
+        prev = d;
+        idx[i] = d;
+        fm[d] = 1;
+    }
+    if (h->d_freeidx == nullptr || h->nfree < nfree) TRY(dalloc(h, &h->d_freeidx, nfree));
+    h->nfree = nfree;
+    CK(cudaMemcpy(h->d_freeidx, idx.data(), sizeof(int64_t) * nfree, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->lev[0].fm, fm.data(), g0.ndof, cudaMemcpyHostToDevice));
+    for (int l = 0; l + 1 < h->ngrids; ++l)
+        launch_coarse_freemask(h->lev[l].fm, h->lev[l + 1].fm, h->lev[l].g, h->lev[l + 1].g, h->stream);
+    CKL();
+    h->setup_done = false;
+    return sync(h);
+}
+
+int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg, int precision) {
+    if (!pb || !mg) {
+        h->err = "null problem or mg parameters";
+        return TOSP_ERR_BAD_ARG;
+    }
+    if (pb->nelx < 1 || pb->nely < 1 || pb->nelz < 1 || !(pb->el > 0) || !(pb->eh > 0) || !(pb->ew > 0)) {
+        h->err = "invalid mesh dimensions or element sizes";
+        return TOSP_ERR_BAD_ARG;
+    }
+    if (pb->mr_n < 1 || pb->mr_n > 3) {
+        h->err = "mr_n must be 1, 2 or 3";
+        return TOSP_ERR_UNSUPPORTED;
+    }
+    if (pb->opfilter < 0 || pb->opfilter > 2 || (pb->opfilter != 0 && !(pb->rmin > 0))) {
+        h->err = "opfilter must be 0, 1 or 2 with rmin > 0";
+        return TOSP_ERR_BAD_ARG;
+    }
+    if (mg->cycle < 0 || mg->cycle > 2 || mg->smoother != 0 || mg->smoothiter1 < 0 || mg->smoothiter2 < 0 ||
+        !(mg->omega > 0) || mg->maxiterMG < 0) {
+        h->err = "unsupported mg parameters (cycle 0/1/2, Jacobi smoother, omega > 0)";
+        return TOSP_ERR_UNSUPPORTED;
+    }
+    if (precision != TOSP_PREC_FP64 && precision != TOSP_PREC_MIXED) {
+        h->err = "precision must be TOSP_PREC_FP64 or TOSP_PREC_MIXED";
+        return TOSP_ERR_BAD_ARG;
+    }
+    if (!pb->freedofs || pb->nfree <= 0) {
+        h->err = "freedofs missing";
+        return TOSP_ERR_BAD_ARG;
+    }
+    CK(cudaGetDevice(&h->device));
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&h->ev0));
+    CK(cudaEventCreate(&h->ev1));
+    h->n = pb->mr_n;
+    h->ns = h->n * h->n * h->n;
+    h->precision = precision;
+    h->E = pb->E; h->nu = pb->nu; h->p = pb->p; h->emin = pb->emin;
+    h->el = pb->el; h->eh = pb->eh; h->ew = pb->ew;
+    h->opfilter = pb->opfilter; h->rmin = pb->rmin;
+    h->mg = *mg;
+    std::string msg;
+    int ng = choose_levels(pb->nelx, pb->nely, pb->nelz, mg->ngrids, mg->nmaxchol, msg);
+    if (ng < 0) {
+        // the operator, Grad and the filter still work; SolveMG/cycles report why not
+        h->mg_ok = false;
+        h->mg_msg = msg;
+        ng = 1;
+    }
+    h->ngrids = ng;
+    h->lev.resize(ng);
+    for (int l = 0; l < ng; ++l)
+        h->lev[l].g = make_grid(pb->nelx >> l, pb->nely >> l, pb->nelz >> l);
+    const Grid &g0 = h->lev[0].g;
+    FineGeom &fg = h->fg;
+    fg.g = g0;
+    fg.nelx_d = pb->nelx * h->n;
+    fg.nely_d = pb->nely * h->n;
+    fg.nbx = (g0.nelx + BX - 1) / BX;
+    fg.nby = (g0.nely + BY - 1) / BY;
+    fg.nbz = (g0.nelz + BZ - 1) / BZ;
+    fg.nbricks = (int64_t)fg.nbx * fg.nby * fg.nbz;
+    h->dens = make_grid(pb->nelx * h->n, pb->nely * h->n, pb->nelz * h->n);
+    h->ncoarse = h->mg_ok ? h->lev[ng - 1].g.ndof : 0;
+    h->npad = (h->ncoarse + 31) / 32 * 32;
+    if (h->npad > 24576) {
+        h->err = "coarsest system too large for the dense direct solve: " + std::to_string(h->ncoarse) +
+                 " dofs; use more grids";
+        return TOSP_ERR_UNSUPPORTED;
+    }
+
+    // constant blocks
+    std::vector<double> ks, packed;
+    elem_stiff_mr(pb->el, pb->eh, pb->ew, pb->nu, h->n, ks);
+    pack_upper(ks, h->ns, packed);
+    std::vector<float> packed32(packed.begin(), packed.end());
+    TRY(dalloc(h, &h->d_ke64, (int64_t)packed.size()));
+    TRY(dalloc(h, &h->d_ke32, (int64_t)packed.size()));
+    CK(cudaMemcpy(h->d_ke64, packed.data(), sizeof(double) * packed.size(), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(h->d_ke32, packed32.data(), sizeof(float) * packed32.size(), cudaMemcpyHostToDevice));
+
+    // levels
+    const size_t tsz = precision == TOSP_PREC_FP64 ? 8 : 4;
+    for (int l = 0; l < ng; ++l) {
+        Level &L = h->lev[l];
+        TRY(dalloc(h, &L.fm, L.g.ndof));
+        uint8_t *vb;
+        TRY(dalloc(h, &vb, (int64_t)tsz * L.g.ndof * 4));
+        L.b = vb;
+        L.x = vb + tsz * L.g.ndof;
+        L.r = vb + 2 * tsz * L.g.ndof;
+        L.t = vb + 3 * tsz * L.g.ndof;
+        if (l >= 1) TRY(dalloc(h, &L.Ae, L.g.nelem * 576));
+        if (l >= 1 && l < ng - 1) {
+            uint8_t *sp;
+            TRY(dalloc(h, &sp, (int64_t)tsz * L.g.nnodes * STENCIL_VALS));
+            L.st = sp;
+        }
+        if (l < ng - 1 || !h->mg_ok) {
+            uint8_t *ip;
+            TRY(dalloc(h, &ip, (int64_t)tsz * L.g.ndof));
+            L.invd = ip;
+        }
+    }
+    TRY(dalloc(h, &h->d_diag64, g0.ndof));
+    if (h->mg_ok) {
+        TRY(dalloc(h, &h->d_Adense, h->npad * h->npad));
+        TRY(dalloc(h, &h->d_Xinv, h->npad * h->npad));
+    }
+    TRY(dalloc(h, &h->d_info, 1));
+    // densities
+    const int64_t nd = h->dens.nelem;
+    TRY(dalloc(h, &h->d_rho, nd));
+    TRY(dalloc(h, &h->d_w64, nd));
+    if (precision == TOSP_PREC_MIXED) TRY(dalloc(h, &h->d_wbf, nd));
+    TRY(dalloc(h, &h->d_free_elem, g0.nelem));
+    {
+        std::vector<uint8_t> fe(g0.nelem, pb->free_dens_g ? 0 : 1);
+        if (pb->free_dens_g) {
+            for (int64_t i = 0; i < pb->nfree_dens_g; ++i) {
+                const int64_t e = pb->free_dens_g[i] - 1;
+                if (e < 0 || e >= g0.nelem) {
+                    h->err = "free_dens_g entry out of range";
+                    return TOSP_ERR_BAD_ARG;
+                }
+                fe[e] = 1;
+            }
+        }
+        CK(cudaMemcpy(h->d_free_elem, fe.data(), g0.nelem, cudaMemcpyHostToDevice));
+    }
+    // CG vectors
+    TRY(dalloc(h, &h->cx, g0.ndof));
+    TRY(dalloc(h, &h->cr, g0.ndof));
+    TRY(dalloc(h, &h->cd, g0.ndof));
+    TRY(dalloc(h, &h->cq, g0.ndof));
+    TRY(dalloc(h, &h->cs, g0.ndof));
+    TRY(dalloc(h, &h->cf, g0.ndof));
+    TRY(dalloc(h, &h->d_partials, RED_BLOCKS));
+    TRY(dalloc(h, &h->d_scal, 16));
+    CK(cudaMallocHost(&h->h_scal, sizeof(double) * 16));
+    TRY(dalloc(h, &h->d_ufull, g0.ndof));
+    TRY(dalloc(h, &h->d_g0, nd));
+    TRY(dalloc(h, &h->d_gf, nd));
+    // filter
+    {
+        std::vector<FilterTap> taps;
+        if (pb->opfilter != 0) {
+            const double eld = pb->el / h->n, ehd = pb->eh / h->n, ewd = pb->ew / h->n;
+            filter_taps(pb->rmin, eld, ehd, ewd, pb->opfilter, taps);
+        }
+        h->ntaps = (int)taps.size();
+        if (h->ntaps) {
+            TRY(dalloc(h, &h->d_taps, h->ntaps));
+            CK(cudaMemcpy(h->d_taps, taps.data(), sizeof(FilterTap) * taps.size(), cudaMemcpyHostToDevice));
+        }
+        if (pb->fixed_dens && pb->nfixed_dens > 0) {
+            std::vector<uint8_t> fx(nd, 0);
+            for (int64_t i = 0; i < pb->nfixed_dens; ++i) {
+                const int64_t e = pb->fixed_dens[i] - 1;
+                if (e < 0 || e >= nd) {
+                    h->err = "fixed_dens entry out of range";
+                    return TOSP_ERR_BAD_ARG;
+                }
+                fx[e] = 1;
+            }
+            TRY(dalloc(h, &h->d_fixed, nd));
+            CK(cudaMemcpy(h->d_fixed, fx.data(), nd, cudaMemcpyHostToDevice));
+        }
+        TRY(dalloc(h, &h->d_fw, nd));
+        if (h->ntaps) {
+            launch_filter(nullptr, h->d_fw, nullptr, h->d_fixed, h->d_taps, h->ntaps, h->dens.nelx, h->dens.nely,
+                          h->dens.nelz, 0, 1, h->stream);
+            CKL();
+        }
+    }
+    return build_masks(h, pb->freedofs, pb->nfree);
+}
+
+template <typename T>
+int setup_levels(tosp_handle *h) {
+    const int ng = h->ngrids;
+    const int64_t nd0 = h->lev[0].g.ndof;
+    // finest diagonal (FP64) -> omega/diag in the cycle precision
+    CK(cudaMemsetAsync(h->d_diag64, 0, sizeof(double) * nd0, h->stream));
+    launch_fine_apply<double, double>(nullptr, h->d_diag64, h->d_w64, h->lev[0].fm, h->d_ke64, h->fg, h->n, true,
+                                      h->stream);
+    CKL();
+    if constexpr (sizeof(T) == 8) {
+        launch_invert_diag<double>(h->d_diag64, h->lev[0].fm, (double *)h->lev[0].invd, h->mg.omega, nd0, h->stream);
+    } else {
+        launch_invert_diag<double>(h->d_diag64, h->lev[0].fm, h->cs, h->mg.omega, nd0, h->stream);
+        launch_convert<double, float>(h->cs, (float *)h->lev[0].invd, nd0, h->stream);
+    }
+    CKL();
+    launch_coarse_from_fine(h->d_w64, h->lev[0].fm, h->d_ke64, h->lev[1].Ae, h->fg, h->lev[1].g, h->n, h->stream);
+    CKL();
+    for (int l = 1; l < ng - 1; ++l) {
+        Level &L = h->lev[l];
+        launch_assemble_stencil<T>(L.Ae, L.fm, L.g, (T *)L.st, (T *)L.invd, h->mg.omega, h->stream);
+        launch_coarse_from_coarse(L.Ae, L.fm, L.g, h->lev[l + 1].Ae, h->lev[l + 1].g, h->stream);
+        CKL();
+    }
+    Level &C = h->lev[ng - 1];
+    launch_dense_assemble(C.Ae, C.fm, C.g, h->d_Adense, h->npad, h->stream);
+    CKL();
+    dense_cholesky_inverse(h->d_Adense, h->d_Xinv, h->npad, h->d_info, h->stream);
+    CKL();
+    int info = 0;
+    CK(cudaMemcpyAsync(&info, h->d_info, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    TRY(sync(h));
+    if (info != 0) {
+        h->err = "coarsest-grid Cholesky failed: non-positive pivot at dof " + std::to_string(info - 1);
+        return TOSP_ERR_BREAKDOWN;
+    }
+    return TOSP_OK;
+}
+
+int check_len(tosp_handle *h, int64_t got, int64_t want, const char *what) {
+    if (got != want) {
+        h->err = std::string(what) + ": length " + std::to_string(got) + " != expected " + std::to_string(want);
+        return TOSP_ERR_BAD_ARG;
+    }
+    return TOSP_OK;
+}
+
+int need_mg(tosp_handle *h) {
+    if (!h->mg_ok) {
+        h->err = h->mg_msg;
+        return TOSP_ERR_UNSUPPORTED;
+    }
+    return TOSP_OK;
+}
+
+int need_setup(tosp_handle *h) {
+    if (!h->setup_done) {
+        h->err = "tosp_setup_gmg must be called first (densities/hierarchy missing)";
+        return TOSP_ERR_STATE;
+    }
+    return TOSP_OK;
+}
+
+int read_scalars(tosp_handle *h) {
+    CK(cudaMemcpyAsync(h->h_scal, h->d_scal, sizeof(double) * 8, cudaMemcpyDeviceToHost, h->stream));
+    return sync(h);
+}
+
+int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
+    const int64_t nd = h->lev[0].g.ndof;
+    // r = f - K x
+    TRY(fine_apply64(h, h->cx, h->cq));
+    launch_residual<double>(h->cf, h->cq, h->cr, nd, h->stream);
+    CKL();
+    launch_dot(h->cf, h->cf, nd, h->d_partials, h->d_scal + 4, h->stream);
+    launch_dot(h->cr, h->cr, nd, h->d_partials, h->d_scal + 3, h->stream);
+    CKL();
+    TRY(read_scalars(h));
+    const double nf = std::sqrt(h->h_scal[4]);
+    double nr = std::sqrt(h->h_scal[3]) / nf;
+    int it = 1;
+    int rc = TOSP_OK;
+    while (nr > h->mg.tolMG && it <= h->mg.maxiterMG) {
+        TRY(precondition(h, h->cr, h->cs));
+        launch_dot(h->cr, h->cs, nd, h->d_partials, h->d_scal + 0, h->stream);
+        launch_pcg_direction(h->cd, h->cs, h->d_scal, nd, it == 1 ? 1 : 0, h->stream);
+        CKL();
+        TRY(fine_apply64(h, h->cd, h->cq));
+        launch_dot(h->cd, h->cq, nd, h->d_partials, h->d_scal + 2, h->stream);
+        launch_pcg_update(h->cx, h->cr, h->cd, h->cq, h->d_scal, h->d_partials, nd, h->stream);
+        CKL();
+        TRY(read_scalars(h));
+        const double dq = h->h_scal[2], rr = h->h_scal[3];
+        if (!(dq > 0.0) || !std::isfinite(rr)) {
+            h->err = "CG breakdown: d'q = " + std::to_string(dq) + ", r'r = " + std::to_string(rr);
+            rc = TOSP_ERR_BREAKDOWN;
+            break;
+        }
+        nr = std::sqrt(rr) / nf;
+        ++it;
+    }
+    if (rc == TOSP_OK && nr > h->mg.tolMG && it > h->mg.maxiterMG) rc = TOSP_NOT_CONVERGED;
+    if (it_out) *it_out = it;
+    if (relres_out) *relres_out = nr;
+    h->stats.it = it;
+    h->stats.relres = nr;
+    return rc;
+}
+
+}  // namespace
+
+// =============================================================================
+// C ABI
+// =============================================================================
+extern "C" {
+
+const char *tosp_version(void) { return "tosp 0.1 (sm_100a)"; }
+
+void tosp_default_mg_params(tosp_mg_params *mg) {
+    if (!mg) return;
+    mg->ngrids = 3;
+    mg->cycle = 1;
+    mg->smoother = 0;
+    mg->omega = 0.5;
+    mg->smoothiter1 = 1;
+    mg->smoothiter2 = 1;
+    mg->tolMG = 1e-8;
+    mg->maxiterMG = 5000;
+    mg->nmaxchol = 60000;
+}
+
+int tosp_create(const tosp_problem *prob, const tosp_mg_params *mg, int32_t precision, tosp_handle **out) {
+    if (!out) {
+        g_create_error = "null output handle pointer";
+        return TOSP_ERR_BAD_ARG;
+    }
+    *out = nullptr;
+    tosp_handle *h = new (std::nothrow) tosp_handle();
+    if (!h) {
+        g_create_error = "host allocation failed";
+        return TOSP_ERR_OOM;
+    }
+    const int rc = create_impl(h, prob, mg, precision);
+    if (rc != TOSP_OK) {
+        g_create_error = h->err;
+        tosp_destroy(h);
+        return rc;
+    }
+    *out = h;
+    return TOSP_OK;
+}
+
+int tosp_destroy(tosp_handle *h) {
+    if (!h) return TOSP_OK;
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    for (void *p : h->allocs) cudaFree(p);
+    if (h->h_scal) cudaFreeHost(h->h_scal);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return TOSP_OK;
+}
+
+const char *tosp_last_error(const tosp_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+
+int tosp_info(const tosp_handle *h, int32_t *ngrids, int64_t *ncoarse, int64_t *device_bytes) {
+    if (!h) return TOSP_ERR_BAD_ARG;
+    if (ngrids) *ngrids = h->ngrids;
+    if (ncoarse) *ncoarse = h->ncoarse;
+    if (device_bytes) *device_bytes = h->bytes;
+    return TOSP_OK;
+}
+
+int tosp_set_freedofs(tosp_handle *h, const int64_t *freedofs, int64_t nfree) {
+    if (!h || !freedofs || nfree <= 0) return TOSP_ERR_BAD_ARG;
+    cudaSetDevice(h->device);
+    return build_masks(h, freedofs, nfree);
+}
+
+int tosp_setup_gmg(tosp_handle *h, const double *xfil, int64_t ndens) {
+    if (!h || !xfil) return TOSP_ERR_BAD_ARG;
+    cudaSetDevice(h->device);
+    TRY(check_len(h, ndens, h->dens.nelem, "densities"));
+    CK(cudaEventRecord(h->ev0, h->stream));
+    TRY(load_vec(h, h->d_rho, xfil, ndens));
+    launch_simp(h->d_rho, h->d_w64, h->d_wbf, ndens, h->p, h->emin, h->E, h->stream);
+    CKL();
+    h->setup_done = false;
+    if (h->mg_ok) {
+        const int rc = h->precision == TOSP_PREC_FP64 ? setup_levels<double>(h) : setup_levels<float>(h);
+        if (rc != TOSP_OK) return rc;
+    }
+    CK(cudaEventRecord(h->ev1, h->stream));
+    TRY(sync(h));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->stats.ms_setup = ms;
+    h->setup_done = true;
+    return TOSP_OK;
+}
+
+int tosp_kelem_prod(tosp_handle *h, const double *x, double *y, int64_t nfree) {
+    if (!h || !x || !y) return TOSP_ERR_BAD_ARG;
+    cudaSetDevice(h->device);
+    TRY(check_len(h, nfree, h->nfree, "x"));
+    TRY(need_setup(h));
+    TRY(free_to_full(h, x, h->cd));
+    TRY(fine_apply64(h, h->cd, h->cq));
+    TRY(full_to_free(h, h->cq, y));
+    return sync(h);
+}
+
+int tosp_mg_cycle(tosp_handle *h, const double *r, double *s, int64_t nfree) {
+    if (!h || !r || !s) return TOSP_ERR_BAD_ARG;
+    cudaSetDevice(h->device);
+    TRY(check_len(h, nfree, h->nfree, "r"));
+    TRY(need_mg(h));
+    TRY(need_setup(h));
+    TRY(free_to_full(h, r, h->cr));
+    TRY(precondition(h, h->cr, h->cs));
+    TRY(full_to_free(h, h->cs, s));
+    return sync(h);
+}
+
+int tosp_solve_mg(tosp_handle *h, double *x, const double *f, int64_t nfree, int32_t *it, double *relres) {
+    if (!h || !x || !f) return TOSP_ERR_BAD_ARG;
+    cudaSetDevice(h->device);
+    TRY(check_len(h, nfree, h->nfree, "x/f"));
+    TRY(need_mg(h));
+    TRY(need_setup(h));
+    CK(cudaEventRecord(h->ev0, h->stream));
+    TRY(free_to_full(h, x, h->cx));
+    TRY(free_to_full(h, f, h->cf));
+    const int rc = solve_impl(h, it, relres);
+    if (rc < 0) return rc;
+    TRY(full_to_free(h, h->cx, x));
+    CK(cudaEventRecord(h->ev1, h->stream));
+    TRY(sync(h));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    h->stats.ms_solve = ms;
+    return rc;
+}
+
+int tosp_apply_filter(tosp_handle *h, const double *x, double *y, int64_t ndens, int32_t trans) {
+    if (!h || !x || !y) return TOSP_ERR_BAD_ARG;
+    cudaSetDevice(h->device);
+    TRY(check_len(h, ndens, h->dens.nelem, "x"));
+    const bool din = is_device_ptr(x), dout = is_device_ptr(y);
+    const double *src = x;
+    if (!din) {
+        TRY(load_vec(h, h->d_g0, x, ndens));
+        src = h->d_g0;
+    }
+    double *dst = dout ? y : h->d_gf;
+    if (h->opfilter == 0 || h->ntaps == 0) {
+        CK(cudaMemcpyAsync(dst, src, sizeof(double) * ndens, cudaMemcpyDefault, h->stream));
+    } else {
+        launch_filter(src, dst, h->d_fw, h->d_fixed, h->d_taps, h->ntaps, h->dens.nelx, h->dens.nely, h->dens.nelz,
+                      trans ? 1 : 0, 0, h->stream);
+        CKL();
+    }
+    if (!dout) TRY(store_vec(h, y, dst, ndens));
+    return sync(h);
+}
+
+int tosp_filter_weights(tosp_handle *h, double *w, int64_t ndens) {
+    if (!h || !w) return TOSP_ERR_BAD_ARG;
+    cudaSetDevice(h->device);
+    TRY(check_len(h, ndens, h->dens.nelem, "w"));
+    if (h->opfilter == 0) {
+        h->err = "no filter (opfilter = 0)";
+        return TOSP_ERR_STATE;
+    }
+    TRY(store_vec(h, w, h->d_fw, ndens));
+    return sync(h);
+}
+
+int tosp_grad(tosp_handle *h, const double *u, int64_t nfull, double *fgrad, double *fgrad0, int64_t ndens) {
+    if (!h || !u || !fgrad) return TOSP_ERR_BAD_ARG;
+    cudaSetDevice(h->device);
+    TRY(check_len(h, nfull, h->lev[0].g.ndof, "u"));
+    TRY(check_len(h, ndens, h->dens.nelem, "fgrad"));
+    TRY(need_setup(h));
+    const double *du = u;
+    if (!is_device_ptr(u)) {
+        TRY(load_vec(h, h->d_ufull, u, nfull));
+        du = h->d_ufull;
+    }
+    launch_grad(du, h->d_rho, h->d_free_elem, h->d_ke64, h->d_g0, h->fg, h->n, h->p, h->emin, h->E, h->stream);
+    CKL();
+    const bool dout = is_device_ptr(fgrad);
+    double *dst = dout ? fgrad : h->d_gf;
+    if (h->opfilter == 0 || h->ntaps == 0) {
+        CK(cudaMemcpyAsync(dst, h->d_g0, sizeof(double) * ndens, cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+        launch_filter(h->d_g0, dst, h->d_fw, h->d_fixed, h->d_taps, h->ntaps, h->dens.nelx, h->dens.nely,
+                      h->dens.nelz, 1, 0, h->stream);
+        CKL();
+    }
+    if (!dout) TRY(store_vec(h, fgrad, dst, ndens));
+    if (fgrad0) TRY(store_vec(h, fgrad0, h->d_g0, ndens));
+    return sync(h);
+}
+
+int tosp_compliance(tosp_handle *h, const double *f, const double *u, int64_t nfree, double *F) {
+    if (!h || !f || !u || !F) return TOSP_ERR_BAD_ARG;
+    cudaSetDevice(h->device);
+    TRY(check_len(h, nfree, h->nfree, "f/u"));
+    TRY(ensure_stage(h, nfree));
+    TRY(load_vec(h, h->d_stage_a, f, nfree));
+    TRY(load_vec(h, h->d_stage_b, u, nfree));
+    launch_dot(h->d_stage_a, h->d_stage_b, nfree, h->d_partials, h->d_scal + 8, h->stream);
+    CKL();
+    CK(cudaMemcpyAsync(h->h_scal + 8, h->d_scal + 8, sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+    TRY(sync(h));
+    *F = h->h_scal[8];
+    return TOSP_OK;
+}
+
+int tosp_last_stats(const tosp_handle *h, tosp_solve_stats *st) {
+    if (!h || !st) return TOSP_ERR_BAD_ARG;
+    *st = h->stats;
+    return TOSP_OK;
+}
+
+int64_t tosp_kernel_launches(void) { return (int64_t)launch_count(); }
+
+int tosp_time_operator(tosp_handle *h, int32_t precision, int32_t reps, double *ms_per_launch) {
+    if (!h || !ms_per_launch || reps < 1) return TOSP_ERR_BAD_ARG;
+    cudaSetDevice(h->device);
+    TRY(need_setup(h));
+    if (precision == TOSP_PREC_MIXED && h->precision != TOSP_PREC_MIXED) {
+        h->err = "the FP32/BF16 operator exists only on TOSP_PREC_MIXED handles";
+        return TOSP_ERR_STATE;
+    }
+    const Grid &g0 = h->lev[0].g;
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    double total = 0.0;
+    for (int r = 0; r < reps; ++r) {
+        if (precision == TOSP_PREC_FP64) {
+            CK(cudaMemsetAsync(h->cq, 0, sizeof(double) * g0.ndof, h->stream));
+            CK(cudaEventRecord(a, h->stream));
+            launch_fine_apply<double, double>(h->cd, h->cq, h->d_w64, h->lev[0].fm, h->d_ke64, h->fg, h->n, false,
+                                              h->stream);
+        } else {
+            Level &F = h->lev[0];
+            CK(cudaMemsetAsync(F.t, 0, sizeof(float) * g0.ndof, h->stream));
+            CK(cudaEventRecord(a, h->stream));
+            launch_fine_apply<float, __nv_bfloat16>((const float *)F.x, (float *)F.t, h->d_wbf, F.fm, h->d_ke32,
+                                                    h->fg, h->n, false, h->stream);
+        }
+        CKL();
+        CK(cudaEventRecord(b, h->stream));
+        CK(cudaEventSynchronize(b));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        total += ms;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    *ms_per_launch = total / reps;
+    return TOSP_OK;
+}
+
+int tosp_elem_stiff_mr(double el, double eh, double ew, double nu, int32_t n, double *kv) {
+    if (!kv || n < 1 || n > 4 || !(el > 0) || !(eh > 0) || !(ew > 0)) return TOSP_ERR_BAD_ARG;
+    std::vector<double> ks;
+    elem_stiff_mr(el, eh, ew, nu, n, ks);
+    const int ns = n * n * n;
+    for (int s = 0; s < ns; ++s)
+        for (int j = 0; j < 24; ++j)
+            for (int i = 0; i < 24; ++i) kv[(size_t)s * 576 + j * 24 + i] = ks[(size_t)s * 576 + i * 24 + j];
+    return TOSP_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,147 @@
+// Internal declarations shared by the tosp CUDA sources.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "tosp.h"
+
+namespace tosp {
+
+// Count of kernel launches issued by this library (all handles, all threads).
+void count_launch();
+long long launch_count();
+
+// ---------------------------------------------------------------------------
+// Geometry of one structured hex8 grid (reference numbering: y fastest, then
+// x, then z; dof = 3*node + component).
+// ---------------------------------------------------------------------------
+struct Grid {
+    int nelx, nely, nelz;
+    int nx, ny, nz;
+    int64_t nnodes, ndof, nelem;
+};
+
+inline Grid make_grid(int nelx, int nely, int nelz) {
+    Grid g;
+    g.nelx = nelx; g.nely = nely; g.nelz = nelz;
+    g.nx = nelx + 1; g.ny = nely + 1; g.nz = nelz + 1;
+    g.nnodes = (int64_t)g.nx * g.ny * g.nz;
+    g.ndof = 3 * g.nnodes;
+    g.nelem = (int64_t)nelx * nely * nelz;
+    return g;
+}
+
+// Element-brick tiling of the fine-level operator: a CTA owns BX x BY x BZ
+// elements (y fastest) and the (BX+1)(BY+1)(BZ+1) nodes around them.
+constexpr int BX = 4, BY = 8, BZ = 4;
+constexpr int BRICK_ELEMS = BX * BY * BZ;            // 128 threads, one element each
+constexpr int NBX = BX + 1, NBY = BY + 1, NBZ = BZ + 1;
+constexpr int BRICK_NODES = NBX * NBY * NBZ;         // 225
+constexpr int KE_PACK = 300;                          // upper triangle of a 24x24 block
+
+struct FineGeom {
+    Grid g;
+    int nelx_d, nely_d;        // density mesh (n x finer)
+    int nbx, nby, nbz;         // bricks per direction
+    int64_t nbricks;
+};
+
+// Coarse-level stencil: 27 neighbour blocks of 3x3 per node, stored
+// offset-major / node-minor: st[(o*9 + ci*3 + cj) * nnodes + node].
+constexpr int STENCIL_VALS = 27 * 9;
+
+// ---------------------------------------------------------------------------
+// Host helpers (ke.cpp)
+// ---------------------------------------------------------------------------
+// Sub-element stiffness blocks of I/ElemStiffMatrixGQMR.m (hex8): ks[s][i][j].
+void elem_stiff_mr(double el, double eh, double ew, double nu, int n, std::vector<double> &ks);
+// Pack the upper triangles (row-major i <= j) of ns 24x24 blocks.
+void pack_upper(const std::vector<double> &ks, int ns, std::vector<double> &packed);
+
+struct FilterTap { int dx, dy, dz; double w; };
+// Neighbour offsets/weights of I/ElemNeighborhood.m:93-122 (all signs).
+void filter_taps(double rmin, double el, double eh, double ew, int opfilter, std::vector<FilterTap> &taps);
+
+// ---------------------------------------------------------------------------
+// Kernel launchers.  All take the stream of the handle.
+// ---------------------------------------------------------------------------
+// SIMP factors w = emin + (E-emin) rho^p, in FP64 and BF16.
+void launch_simp(const double *rho, double *w64, __nv_bfloat16 *wbf, int64_t n, double p, double emin,
+                 double E, cudaStream_t st);
+
+// Fine MR operator y = K(w) x (y must be zeroed by the caller; fixed dofs of
+// y stay zero).  diag_only: y = diag(K(w)).
+template <typename T, typename TW>
+void launch_fine_apply(const T *x, T *y, const TW *w, const uint8_t *freemask, const T *kepack,
+                       const FineGeom &fg, int n, bool diag_only, cudaStream_t st);
+
+// Sensitivities g0 (I/Grad.m:24-49), zero for elements not in freeDensG.
+void launch_grad(const double *u, const double *rho, const uint8_t *free_elem, const double *kepack,
+                 double *g0, const FineGeom &fg, int n, double p, double emin, double E, cudaStream_t st);
+
+// Galerkin coarse element matrices (FP64, 576 per coarse element).
+void launch_coarse_from_fine(const double *w, const uint8_t *freemask_f, const double *kepack,
+                             double *Ac, const FineGeom &fg, const Grid &gc, int n, cudaStream_t st);
+void launch_coarse_from_coarse(const double *Af, const uint8_t *freemask_f, const Grid &gf,
+                               double *Ac, const Grid &gc, cudaStream_t st);
+// Node stencil from element matrices (masked), plus omega/diag.
+template <typename T>
+void launch_assemble_stencil(const double *Ae, const uint8_t *freemask, const Grid &g, T *stencil,
+                             T *invdiag, double omega, cudaStream_t st);
+// Stencil products: mode 0: y = A x; 1: y = b - A x; 2: y = x + invD (b - A x).
+template <typename T>
+void launch_stencil(const T *st_vals, const T *x, const T *b, const T *invdiag, T *y, const Grid &g,
+                    int mode, cudaStream_t st);
+// Fine-level helpers: y = b - t ; x = x + invD (b - t) ; x = invD b
+template <typename T>
+void launch_residual(const T *b, const T *t, T *r, int64_t n, cudaStream_t st);
+template <typename T>
+void launch_jacobi_update(T *x, const T *b, const T *t, const T *invdiag, int64_t n, int first,
+                          cudaStream_t st);
+template <typename T>
+void launch_invert_diag(const T *diag, const uint8_t *freemask, T *invdiag, double omega, int64_t n,
+                        cudaStream_t st);
+// Transfers (masked).  prolong: xf (+)= P xc ; restrict: bc = P^T rf.
+template <typename T>
+void launch_prolong(const T *xc, T *xf, const uint8_t *freemask_f, const Grid &gf, const Grid &gc,
+                    bool accumulate, cudaStream_t st);
+template <typename T>
+void launch_restrict(const T *rf, T *bc, const uint8_t *freemask_c, const Grid &gf, const Grid &gc,
+                     cudaStream_t st);
+void launch_coarse_freemask(const uint8_t *freemask_f, uint8_t *freemask_c, const Grid &gf,
+                            const Grid &gc, cudaStream_t st);
+
+// Coarsest direct solve: dense SPD matrix (padded to a multiple of 32, fixed
+// dofs decoupled with a unit diagonal), Cholesky, explicit inverse, GEMV.
+void launch_dense_assemble(const double *Ae, const uint8_t *freemask, const Grid &g, double *A,
+                           int64_t npad, cudaStream_t st);
+int dense_cholesky_inverse(double *A, double *X, int64_t npad, int *d_info, cudaStream_t st);
+template <typename T>
+void launch_dense_solve(const double *X, const T *b, T *x, int64_t n, int64_t npad, cudaStream_t st);
+
+// Filter (I/ApplyFilter.m): trans 0: (W x)./w, 1: W (x./w); weights: w = W 1.
+void launch_filter(const double *x, double *y, const double *wsum, const uint8_t *fixed,
+                   const FilterTap *taps_dev, int ntaps, int nelx, int nely, int nelz, int trans,
+                   int weights_only, cudaStream_t st);
+
+// Vector kernels.
+void launch_scatter_free(const double *v, const int64_t *idx, int64_t nfree, double *full, cudaStream_t st);
+void launch_gather_free(const double *full, const int64_t *idx, int64_t nfree, double *v, cudaStream_t st);
+template <typename TI, typename TO>
+void launch_convert(const TI *a, TO *b, int64_t n, cudaStream_t st);
+// Deterministic dot products: out[0] = sum a*b (fixed reduction tree).
+constexpr int RED_BLOCKS = 592;
+void launch_dot(const double *a, const double *b, int64_t n, double *partials, double *out, cudaStream_t st);
+// PCG pieces (scalars in device memory, see solver.cpp for the slots).
+void launch_pcg_direction(double *d, const double *s, const double *scal, int64_t n, int first,
+                          cudaStream_t st);
+void launch_pcg_update(double *x, double *r, const double *d, const double *q, double *scal, double *partials,
+                       int64_t n, cudaStream_t st);
+void launch_set_scalar(double *dst, const double *src, cudaStream_t st);
+
+}  // namespace tosp

@@ -1,0 +1,273 @@
+"""Python binding of the tosp C ABI (``include/tosp.h``).
+
+The functions keep the names and argument meaning of the reference MATLAB
+functions they replace (``SetupGMG``/``SetupGMGWOK``, ``SolveMG``,
+``KelemProd``, ``Grad``, ``ApplyFilter``, ``ElemStiffMatrixGQMR``) so host
+code reads like the reference's ``StrSLP``; the heavy MATLAB arguments
+(``A, P, M, R, perm, kv, W``) live inside a :class:`Solver` handle.
+
+Indices crossing the ABI are 1-based like MATLAB; the Python layer takes the
+0-based arrays of :mod:`tosp.problems` and converts.  The CUDA library must be
+built (``python topopt-slp-3d_b200/build.py``); importing this module without
+it raises ``ImportError`` - there is no CPU fallback.
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import problems  # noqa: F401
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libtosp.so")
+
+TOSP_OK = 0
+TOSP_NOT_CONVERGED = 1
+PREC_FP64 = 0
+PREC_MIXED = 1
+STATUS = {0: "OK", 1: "NOT_CONVERGED", -1: "BAD_ARG", -2: "CUDA_ERROR", -3: "OOM", -4: "BREAKDOWN",
+          -5: "UNSUPPORTED", -6: "STATE", -7: "CANCELLED", -8: "TIMEOUT"}
+
+
+class TospError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"tosp error {code} ({STATUS.get(code, '?')}): {msg}")
+        self.code = code
+
+
+class _Problem(C.Structure):
+    _fields_ = [("nelx", C.c_int32), ("nely", C.c_int32), ("nelz", C.c_int32),
+                ("el", C.c_double), ("eh", C.c_double), ("ew", C.c_double),
+                ("E", C.c_double), ("nu", C.c_double), ("p", C.c_double), ("emin", C.c_double),
+                ("mr_n", C.c_int32), ("opfilter", C.c_int32), ("rmin", C.c_double),
+                ("freedofs", C.POINTER(C.c_int64)), ("nfree", C.c_int64),
+                ("fixed_dens", C.POINTER(C.c_int64)), ("nfixed_dens", C.c_int64),
+                ("free_dens_g", C.POINTER(C.c_int64)), ("nfree_dens_g", C.c_int64)]
+
+
+class MgParams(C.Structure):
+    """The ``mg.*`` struct of the reference (I/TopOpt3D.m:171-190)."""
+    _fields_ = [("ngrids", C.c_int32), ("cycle", C.c_int32), ("smoother", C.c_int32), ("omega", C.c_double),
+                ("smoothiter1", C.c_int32), ("smoothiter2", C.c_int32), ("tolMG", C.c_double),
+                ("maxiterMG", C.c_int32), ("nmaxchol", C.c_int32)]
+
+
+class SolveStats(C.Structure):
+    _fields_ = [("it", C.c_int32), ("relres", C.c_double), ("ms_setup", C.c_double), ("ms_solve", C.c_double)]
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"tosp CUDA library not built: {LIB_PATH} missing "
+                          "(run python topopt-slp-3d_b200/build.py)")
+    lib = C.CDLL(LIB_PATH)
+    P = C.POINTER
+    d = C.c_void_p   # double* (host or device address)
+    sig = {
+        "tosp_version": (C.c_char_p, []),
+        "tosp_default_mg_params": (None, [P(MgParams)]),
+        "tosp_create": (C.c_int, [P(_Problem), P(MgParams), C.c_int32, P(C.c_void_p)]),
+        "tosp_destroy": (C.c_int, [C.c_void_p]),
+        "tosp_last_error": (C.c_char_p, [C.c_void_p]),
+        "tosp_info": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int64), P(C.c_int64)]),
+        "tosp_set_freedofs": (C.c_int, [C.c_void_p, P(C.c_int64), C.c_int64]),
+        "tosp_setup_gmg": (C.c_int, [C.c_void_p, d, C.c_int64]),
+        "tosp_kelem_prod": (C.c_int, [C.c_void_p, d, d, C.c_int64]),
+        "tosp_mg_cycle": (C.c_int, [C.c_void_p, d, d, C.c_int64]),
+        "tosp_solve_mg": (C.c_int, [C.c_void_p, d, d, C.c_int64, P(C.c_int32), P(C.c_double)]),
+        "tosp_grad": (C.c_int, [C.c_void_p, d, C.c_int64, d, d, C.c_int64]),
+        "tosp_apply_filter": (C.c_int, [C.c_void_p, d, d, C.c_int64, C.c_int32]),
+        "tosp_filter_weights": (C.c_int, [C.c_void_p, d, C.c_int64]),
+        "tosp_compliance": (C.c_int, [C.c_void_p, d, d, C.c_int64, P(C.c_double)]),
+        "tosp_last_stats": (C.c_int, [C.c_void_p, P(SolveStats)]),
+        "tosp_elem_stiff_mr": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32, d]),
+        "tosp_kernel_launches": (C.c_int64, []),
+        "tosp_time_operator": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, P(C.c_double)]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+_lib = _load()
+
+
+def exported_symbols():
+    """Names of the entry points bound from the library."""
+    return [n for n in dir(_lib) if n.startswith("tosp_")]
+
+
+def kernel_launches():
+    """Kernel launches issued by the library since load (all handles)."""
+    return int(_lib.tosp_kernel_launches())
+
+
+def version():
+    return _lib.tosp_version().decode()
+
+
+def _ptr(a):
+    """Address of a float64 NumPy array (host) or a CUDA tensor (device)."""
+    if isinstance(a, np.ndarray):
+        assert a.dtype == np.float64 and a.flags.c_contiguous
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):   # torch.Tensor on the GPU (device pointer path)
+        return a.data_ptr()
+    raise TypeError("expected a float64 numpy array or a CUDA tensor")
+
+
+def _i64(a):
+    a = np.ascontiguousarray(a, dtype=np.int64)
+    return a, a.ctypes.data_as(C.POINTER(C.c_int64))
+
+
+def default_mg(**kw):
+    mg = MgParams()
+    _lib.tosp_default_mg_params(C.byref(mg))
+    for k, v in kw.items():
+        setattr(mg, k, v)
+    return mg
+
+
+def ElemStiffMatrixGQMR(el, eh, ew, nu, n):
+    """``kv`` of I/ElemStiffMatrixGQMR.m (576 x n^3, column s = k{s}(:))."""
+    kv = np.zeros((n ** 3, 576))
+    rc = _lib.tosp_elem_stiff_mr(el, eh, ew, nu, n, kv.ctypes.data)
+    if rc:
+        raise TospError(rc, "tosp_elem_stiff_mr")
+    return kv.T.copy()
+
+
+class Solver:
+    """A solve handle: problem, multigrid hierarchy and device state.
+
+    ``pb`` is a :class:`tosp.problems.Problem` (0-based arrays).  ``mr_n`` is
+    the multiresolution factor (density sub-elements per direction; design
+    mesh = density mesh).  ``fixed_dens`` (0-based, density mesh) defaults
+    to the problem's ``fixed_dens`` when ``mr_n == 1``.
+    """
+
+    def __init__(self, pb, mg=None, precision=PREC_FP64, mr_n=1, p=3.0, emin=1e-9, opfilter=1, rmin=1.5,
+                 fixed_dens=None, free_dens_g=None):
+        self.pb = pb
+        self.mr_n = mr_n
+        self.mg = mg if mg is not None else default_mg()
+        fd1, fdp = _i64(np.asarray(pb.freedofs) + 1)
+        if fixed_dens is None and mr_n == 1 and pb.fixed_dens is not None:
+            fixed_dens = pb.fixed_dens
+        self._keep = [fd1]
+        prob = _Problem(pb.nelx, pb.nely, pb.nelz, pb.el, pb.eh, pb.ew, pb.E, pb.nu, p, emin, mr_n, opfilter, rmin,
+                        fdp, fd1.size, None, 0, None, 0)
+        if fixed_dens is not None and len(fixed_dens):
+            fx1, fxp = _i64(np.asarray(fixed_dens) + 1)
+            self._keep.append(fx1)
+            prob.fixed_dens, prob.nfixed_dens = fxp, fx1.size
+        if free_dens_g is not None:
+            fg1, fgp = _i64(np.asarray(free_dens_g) + 1)
+            self._keep.append(fg1)
+            prob.free_dens_g, prob.nfree_dens_g = fgp, fg1.size
+        h = C.c_void_p()
+        rc = _lib.tosp_create(C.byref(prob), C.byref(self.mg), precision, C.byref(h))
+        if rc != TOSP_OK:
+            raise TospError(rc, _lib.tosp_last_error(None).decode())
+        self.h = h
+        self.nfree = int(np.asarray(pb.freedofs).size)
+        self.ndens = pb.nelem * mr_n ** 3
+        self.nfull = 3 * pb.nnodes
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.tosp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc, allow=(TOSP_OK,)):
+        if rc not in allow:
+            raise TospError(rc, _lib.tosp_last_error(self.h).decode())
+        return rc
+
+    def info(self):
+        ng, nc, nb = C.c_int32(), C.c_int64(), C.c_int64()
+        self._check(_lib.tosp_info(self.h, C.byref(ng), C.byref(nc), C.byref(nb)))
+        return {"ngrids": ng.value, "ncoarse": nc.value, "device_bytes": nb.value}
+
+    def stats(self):
+        st = SolveStats()
+        self._check(_lib.tosp_last_stats(self.h, C.byref(st)))
+        return {"it": st.it, "relres": st.relres, "ms_setup": st.ms_setup, "ms_solve": st.ms_solve}
+
+    # -- reference entry points ------------------------------------------------
+    def SetupGMG(self, xfil):
+        """Densities -> K(rho) and the multigrid hierarchy (GlobalStiffMatrix +
+        SetupGMG / SetupGMGWOK)."""
+        n = self.ndens
+        if isinstance(xfil, np.ndarray):
+            xfil = np.ascontiguousarray(xfil, dtype=np.float64)
+            assert xfil.size == n
+        self._check(_lib.tosp_setup_gmg(self.h, _ptr(xfil), n))
+
+    def KelemProd(self, x):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty_like(x)
+        self._check(_lib.tosp_kelem_prod(self.h, _ptr(x), _ptr(y), x.size))
+        return y
+
+    def MGCycle(self, r):
+        """One VCycle/WCycle/FMVCycle application s = M^{-1} r (free dofs)."""
+        r = np.ascontiguousarray(r, dtype=np.float64)
+        s = np.empty_like(r)
+        self._check(_lib.tosp_mg_cycle(self.h, _ptr(r), _ptr(s), r.size))
+        return s
+
+    def SolveMG(self, x, f):
+        """``[x, it] = SolveMG(x, f, ...)``: returns (x, it, relres, status)."""
+        x = np.array(x, dtype=np.float64, copy=True)
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        it, rr = C.c_int32(), C.c_double()
+        rc = self._check(_lib.tosp_solve_mg(self.h, _ptr(x), _ptr(f), x.size, C.byref(it), C.byref(rr)),
+                         allow=(TOSP_OK, TOSP_NOT_CONVERGED))
+        return x, it.value, rr.value, rc
+
+    def Grad(self, u_full, return_unfiltered=False):
+        u = np.ascontiguousarray(u_full, dtype=np.float64)
+        g = np.empty(self.ndens)
+        g0 = np.empty(self.ndens) if return_unfiltered else None
+        self._check(_lib.tosp_grad(self.h, _ptr(u), u.size, _ptr(g), _ptr(g0) if g0 is not None else None,
+                                   self.ndens))
+        return (g, g0) if return_unfiltered else g
+
+    def ApplyFilter(self, x, trans=False):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty_like(x)
+        self._check(_lib.tosp_apply_filter(self.h, _ptr(x), _ptr(y), x.size, 1 if trans else 0))
+        return y
+
+    def FilterWeights(self):
+        w = np.empty(self.ndens)
+        self._check(_lib.tosp_filter_weights(self.h, _ptr(w), self.ndens))
+        return w
+
+    def Compliance(self, f, u):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        u = np.ascontiguousarray(u, dtype=np.float64)
+        F = C.c_double()
+        self._check(_lib.tosp_compliance(self.h, _ptr(f), _ptr(u), f.size, C.byref(F)))
+        return F.value
+
+    def time_operator(self, precision=PREC_FP64, reps=10):
+        """Mean device time (ms) of one finest-level operator kernel launch."""
+        ms = C.c_double()
+        self._check(_lib.tosp_time_operator(self.h, precision, reps, C.byref(ms)))
+        return ms.value
+
+    def SetFreedofs(self, freedofs):
+        fd1, fdp = _i64(np.asarray(freedofs) + 1)
+        self._check(_lib.tosp_set_freedofs(self.h, fdp, fd1.size))
+        self.nfree = fd1.size
