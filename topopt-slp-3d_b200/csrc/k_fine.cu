@@ -1,10 +1,14 @@
 // Fine-level multiresolution hex8 operator, its diagonal, the SIMP factors
 // and the compliance sensitivities.
 //
-// Operator (I/WOK/KelemProd.m:57-100): y_e = sum_s w_s KE_s u_e for every
-// displacement element e, scatter-added over the nodes.  The n^3 blocks KE_s
-// are the same for every element; they live in shared memory as packed upper
-// triangles (each stored entry feeds two FMAs).  A persistent CTA walks
+// Operator (I/WOK/KelemProd.m:57-100): y_e = K_e u_e with
+// K_e = sum_s w_s KE_s for every displacement element e, scatter-added over
+// the nodes.  The n^3 blocks KE_s are the same for every element; they live in
+// shared memory pair-major (for each upper-triangle entry (i,j) the n^3 block
+// values are contiguous), so each thread forms one entry of its K_e with
+// vector loads and n^3 FMAs and uses it twice (y_i += k u_j, y_j += k u_i):
+// 300 (n^3 + 2) FMAs per element instead of 600 n^3 for block-by-block
+// products.  A persistent CTA walks
 // element bricks of BX x BY x BZ: it stages the brick's nodal values in
 // shared memory, each thread forms one element's 24 outputs, the outputs are
 // summed into a shared node brick in 8 parity colours (elements of one colour
@@ -12,11 +16,12 @@
 // only this brick touches and atomics on the brick faces.
 #include <cuda_bf16.h>
 
+#include <utility>
+
 #include "tosp_internal.h"
 
 namespace tosp {
 
-template <typename T> __device__ __forceinline__ T to_t(double v) { return (T)v; }
 __device__ __forceinline__ float wval(__nv_bfloat16 v) { return __bfloat162float(v); }
 __device__ __forceinline__ double wval(double v) { return v; }
 __device__ __forceinline__ float wval(float v) { return v; }
@@ -24,17 +29,71 @@ __device__ __forceinline__ float wval(float v) { return v; }
 __device__ __forceinline__ void atomic_add(double *p, double v) { atomicAdd(p, v); }
 __device__ __forceinline__ void atomic_add(float *p, float v) { atomicAdd(p, v); }
 
-template <typename T, typename TW, int N, bool DIAG>
+// Row/column of packed upper-triangle entry t (row-major, i <= j).
+__host__ __device__ constexpr int pair_i(int t) {
+    int i = 0;
+    while (t >= 24 - i) {
+        t -= 24 - i;
+        ++i;
+    }
+    return i;
+}
+__host__ __device__ constexpr int pair_j(int t) { return pair_i(t) + (t - (pair_i(t) * 24 - pair_i(t) * (pair_i(t) - 1) / 2)); }
+
+template <typename T> struct Vec;
+template <> struct Vec<float> { using type = float4; static constexpr int W = 4; };
+template <> struct Vec<double> { using type = double2; static constexpr int W = 2; };
+
+__device__ __forceinline__ float dot_vec(const float4 v, const float *w) { return w[0] * v.x + w[1] * v.y + w[2] * v.z + w[3] * v.w; }
+__device__ __forceinline__ double dot_vec(const double2 v, const double *w) { return w[0] * v.x + w[1] * v.y; }
+
+// One packed entry t of the element matrix: k = sum_s w_s KE_s[i][j], then
+// y_i += k u_j and (for i != j) y_j += k u_i.
+template <typename T, int NSP, int t>
+__device__ __forceinline__ void pair_step(const T *__restrict__ kt, const T (&w)[NSP], const T (&u)[24],
+                                          T (&acc)[24]) {
+    constexpr int i = pair_i(t), j = pair_j(t);
+    T k;
+    if constexpr (NSP == 1) {
+        k = w[0] * kt[t];
+    } else {
+        constexpr int W = Vec<T>::W;
+        const typename Vec<T>::type *kv = reinterpret_cast<const typename Vec<T>::type *>(kt + t * NSP);
+        k = dot_vec(kv[0], w);
+#pragma unroll
+        for (int q = 1; q < NSP / W; ++q) k += dot_vec(kv[q], w + q * W);
+    }
+    if constexpr (i == j) {
+        acc[i] += k * u[i];
+    } else {
+        acc[i] += k * u[j];
+        acc[j] += k * u[i];
+    }
+}
+
+template <typename T, int NSP, int... Ts>
+__device__ __forceinline__ void all_pairs(const T *__restrict__ kt, const T (&w)[NSP], const T (&u)[24], T (&acc)[24],
+                                          std::integer_sequence<int, Ts...>) {
+    (pair_step<T, NSP, Ts>(kt, w, u, acc), ...);
+}
+
+template <typename T, int N> struct FineShape {
+    static constexpr int NS = N * N * N;
+    static constexpr int NSP = (N == 1) ? 1 : (NS + Vec<T>::W - 1) / Vec<T>::W * Vec<T>::W;
+};
+
+// Operator: persistent CTAs over element bricks; see the file header.
+template <typename T, typename TW, int N>
 __global__ void __launch_bounds__(BRICK_ELEMS)
 k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ w,
-             const uint8_t *__restrict__ freemask, const T *__restrict__ kepack, FineGeom fg) {
-    constexpr int NS = N * N * N;
+             const uint8_t *__restrict__ freemask, const T *__restrict__ ktg, FineGeom fg) {
+    constexpr int NS = FineShape<T, N>::NS, NSP = FineShape<T, N>::NSP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *ke = reinterpret_cast<T *>(smem_raw);             // NS * 300
-    T *xs = ke + NS * KE_PACK;                             // BRICK_NODES * 3
-    T *ys = xs + BRICK_NODES * 3;                          // BRICK_NODES * 3
+    T *kt = reinterpret_cast<T *>(smem_raw);               // KE_PACK * NSP (pair-major)
+    T *xs = kt + KE_PACK * NSP;                             // BRICK_NODES * 3
+    T *ys = xs + BRICK_NODES * 3;                           // BRICK_NODES * 3
     const int tid = threadIdx.x;
-    for (int i = tid; i < NS * KE_PACK; i += BRICK_ELEMS) ke[i] = kepack[i];
+    for (int i = tid; i < KE_PACK * NSP; i += BRICK_ELEMS) kt[i] = ktg[i];
 
     const Grid &g = fg.g;
     const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
@@ -45,14 +104,13 @@ k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ 
         const int bbx = (int)((brick / fg.nby) % fg.nbx);
         const int bbz = (int)(brick / ((int64_t)fg.nby * fg.nbx));
         const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
-        __syncthreads();   // previous brick done with xs/ys (and ke loaded)
+        __syncthreads();   // previous brick done with xs/ys (and kt loaded)
         for (int i = tid; i < BRICK_NODES * 3; i += BRICK_ELEMS) {
             const int ln = i / 3, c = i - 3 * ln;
             const int ny_ = ln % NBY, nx_ = (ln / NBY) % NBX, nz_ = ln / (NBY * NBX);
             const int gx = ex0 + nx_, gy = ey0 + ny_, gz = ez0 + nz_;
             T v = T(0);
-            if (!DIAG && gx < g.nx && gy < g.ny && gz < g.nz)
-                v = x[3 * (((int64_t)gz * g.nx + gx) * g.ny + gy) + c];
+            if (gx < g.nx && gy < g.ny && gz < g.nz) v = x[3 * (((int64_t)gz * g.nx + gx) * g.ny + gy) + c];
             xs[i] = v;
             ys[i] = T(0);
         }
@@ -65,46 +123,24 @@ k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ 
         for (int i = 0; i < 24; ++i) acc[i] = T(0);
         if (valid) {
             T u[24];
-            if (!DIAG) {
 #pragma unroll
-                for (int a = 0; a < 8; ++a) {
-                    const int dx = (a >> 1) & 1, dy = a & 1, dz = (a >> 2) & 1;
-                    const int ln = ((lz + dz) * NBX + (lx + dx)) * NBY + (ly + dy);
+            for (int a = 0; a < 8; ++a) {
+                const int dx = (a >> 1) & 1, dy = a & 1, dz = (a >> 2) & 1;
+                const int ln = ((lz + dz) * NBX + (lx + dx)) * NBY + (ly + dy);
 #pragma unroll
-                    for (int c = 0; c < 3; ++c) u[3 * a + c] = xs[3 * ln + c];
-                }
+                for (int c = 0; c < 3; ++c) u[3 * a + c] = xs[3 * ln + c];
             }
-#pragma unroll 1
-            for (int s = 0; s < NS; ++s) {
-                const int sy = s % N, sx = (s / N) % N, sz = s / (N * N);
-                const int64_t di = ((int64_t)(ez * N + sz) * fg.nelx_d + (ex * N + sx)) * fg.nely_d + (ey * N + sy);
-                const T ws = (T)wval(w[di]);
-                const T *k = ke + s * KE_PACK;
-                if (DIAG) {
-                    int t = 0;
+            T wv[NSP];
 #pragma unroll
-                    for (int i = 0; i < 24; ++i) {
-                        acc[i] += ws * k[t];
-                        t += 24 - i;
-                    }
+            for (int s = 0; s < NSP; ++s) {
+                if (s < NS) {
+                    const int sy = s % N, sx = (s / N) % N, sz = s / (N * N);
+                    wv[s] = (T)wval(w[((int64_t)(ez * N + sz) * fg.nelx_d + (ex * N + sx)) * fg.nely_d + (ey * N + sy)]);
                 } else {
-                    T wu[24];
-#pragma unroll
-                    for (int i = 0; i < 24; ++i) wu[i] = ws * u[i];
-                    int t = 0;
-#pragma unroll
-                    for (int i = 0; i < 24; ++i) {
-                        acc[i] += k[t] * wu[i];
-                        ++t;
-#pragma unroll
-                        for (int j = i + 1; j < 24; ++j) {
-                            const T kij = k[t++];
-                            acc[i] += kij * wu[j];
-                            acc[j] += kij * wu[i];
-                        }
-                    }
+                    wv[s] = T(0);
                 }
             }
+            all_pairs<T, NSP>(kt, wv, u, acc, std::make_integer_sequence<int, KE_PACK>{});
         }
         // colour-ordered accumulation into the node brick
 #pragma unroll 1
@@ -136,56 +172,92 @@ k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ 
     }
 }
 
-static int g_num_sms = 0;
-static int num_sms() {
-    if (!g_num_sms) {
-        int dev;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+// Diagonal of K(w): one thread per element, atomics (setup only).
+template <int N>
+__global__ void k_fine_diag(double *__restrict__ y, const double *__restrict__ w, const uint8_t *__restrict__ freemask,
+                            const double *__restrict__ ktg, FineGeom fg) {
+    constexpr int NS = N * N * N, NSP = FineShape<double, N>::NSP;
+    const Grid &g = fg.g;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < g.nelem;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int ey = (int)(e % g.nely), ex = (int)((e / g.nely) % g.nelx), ez = (int)(e / ((int64_t)g.nely * g.nelx));
+        for (int i = 0; i < 24; ++i) {
+            const int t = i * 24 - i * (i - 1) / 2;
+            double d = 0.0;
+            for (int s = 0; s < NS; ++s) {
+                const int sy = s % N, sx = (s / N) % N, sz = s / (N * N);
+                d += w[((int64_t)(ez * N + sz) * fg.nelx_d + (ex * N + sx)) * fg.nely_d + (ey * N + sy)] *
+                     ktg[t * NSP + s];
+            }
+            const int a = i / 3, c = i % 3;
+            const int64_t node = ((int64_t)(ez + ((a >> 2) & 1)) * g.nx + (ex + ((a >> 1) & 1))) * g.ny + (ey + (a & 1));
+            if (freemask[3 * node + c]) atomicAdd(&y[3 * node + c], d);
+        }
     }
-    return g_num_sms;
 }
 
-template <typename T, typename TW, int N, bool DIAG>
-static void launch_fine_t(const T *x, T *y, const TW *w, const uint8_t *fm, const T *kp, const FineGeom &fg,
-                          cudaStream_t st) {
-    constexpr int NS = N * N * N;
-    const size_t smem = sizeof(T) * (NS * KE_PACK + 2 * BRICK_NODES * 3);
-    auto kern = k_fine_apply<T, TW, N, DIAG>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_set = true;
+static int num_sms() {
+    static int n = 0;
+    if (!n) {
+        int dev;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
     }
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BRICK_ELEMS, smem);
-    if (per_sm < 1) per_sm = 1;
+    return n;
+}
+
+int fine_nsp(int n, int elem_bytes) {
+    if (n == 1) return 1;
+    const int ns = n * n * n, vw = elem_bytes == 8 ? 2 : 4;
+    return (ns + vw - 1) / vw * vw;
+}
+
+template <typename T, typename TW, int N>
+static void launch_fine_t(const T *x, T *y, const TW *w, const uint8_t *fm, const T *kt, const FineGeom &fg,
+                          cudaStream_t st) {
+    constexpr int NSP = FineShape<T, N>::NSP;
+    const size_t smem = sizeof(T) * (KE_PACK * NSP + 2 * BRICK_NODES * 3);
+    auto kern = k_fine_apply<T, TW, N>;
+    static int attr_dev = -1;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (attr_dev != dev) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_dev = dev;
+    }
+    static int per_sm = 0;
+    if (!per_sm) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BRICK_ELEMS, smem);
+        if (per_sm < 1) per_sm = 1;
+    }
     int64_t grid = (int64_t)per_sm * num_sms();
     if (grid > fg.nbricks) grid = fg.nbricks;
     if (grid < 1) grid = 1;
-    kern<<<(unsigned)grid, BRICK_ELEMS, smem, st>>>(x, y, w, fm, kp, fg); count_launch();
+    kern<<<(unsigned)grid, BRICK_ELEMS, smem, st>>>(x, y, w, fm, kt, fg); count_launch();
 }
 
 template <typename T, typename TW>
-void launch_fine_apply(const T *x, T *y, const TW *w, const uint8_t *freemask, const T *kepack,
-                       const FineGeom &fg, int n, bool diag_only, cudaStream_t st) {
-    if (n == 1) {
-        if (diag_only) launch_fine_t<T, TW, 1, true>(x, y, w, freemask, kepack, fg, st);
-        else launch_fine_t<T, TW, 1, false>(x, y, w, freemask, kepack, fg, st);
-    } else if (n == 2) {
-        if (diag_only) launch_fine_t<T, TW, 2, true>(x, y, w, freemask, kepack, fg, st);
-        else launch_fine_t<T, TW, 2, false>(x, y, w, freemask, kepack, fg, st);
-    } else {
-        if (diag_only) launch_fine_t<T, TW, 3, true>(x, y, w, freemask, kepack, fg, st);
-        else launch_fine_t<T, TW, 3, false>(x, y, w, freemask, kepack, fg, st);
-    }
+void launch_fine_apply(const T *x, T *y, const TW *w, const uint8_t *freemask, const T *kt, const FineGeom &fg, int n,
+                       cudaStream_t st) {
+    if (n == 1) launch_fine_t<T, TW, 1>(x, y, w, freemask, kt, fg, st);
+    else if (n == 2) launch_fine_t<T, TW, 2>(x, y, w, freemask, kt, fg, st);
+    else launch_fine_t<T, TW, 3>(x, y, w, freemask, kt, fg, st);
 }
 
 template void launch_fine_apply<double, double>(const double *, double *, const double *, const uint8_t *,
-                                                const double *, const FineGeom &, int, bool, cudaStream_t);
-template void launch_fine_apply<float, __nv_bfloat16>(const float *, float *, const __nv_bfloat16 *,
-                                                      const uint8_t *, const float *, const FineGeom &, int,
-                                                      bool, cudaStream_t);
+                                                const double *, const FineGeom &, int, cudaStream_t);
+template void launch_fine_apply<float, __nv_bfloat16>(const float *, float *, const __nv_bfloat16 *, const uint8_t *,
+                                                      const float *, const FineGeom &, int, cudaStream_t);
+
+void launch_fine_diag(double *y, const double *w, const uint8_t *freemask, const double *kt64, const FineGeom &fg,
+                      int n, cudaStream_t st) {
+    int64_t blocks = (fg.g.nelem + 255) / 256;
+    if (blocks > 16 * num_sms()) blocks = 16 * num_sms();
+    if (blocks < 1) blocks = 1;
+    if (n == 1) { k_fine_diag<1><<<(unsigned)blocks, 256, 0, st>>>(y, w, freemask, kt64, fg); count_launch(); }
+    else if (n == 2) { k_fine_diag<2><<<(unsigned)blocks, 256, 0, st>>>(y, w, freemask, kt64, fg); count_launch(); }
+    else { k_fine_diag<3><<<(unsigned)blocks, 256, 0, st>>>(y, w, freemask, kt64, fg); count_launch(); }
+}
 
 // ---------------------------------------------------------------------------
 // SIMP factors emin + (E - emin) rho^p (I/GlobalStiffMatrix.m:49,

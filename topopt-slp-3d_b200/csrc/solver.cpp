@@ -49,8 +49,9 @@ struct tosp_handle {
     int64_t nfree = 0;
     int64_t *d_freeidx = nullptr;
     // constants
-    double *d_ke64 = nullptr;
-    float *d_ke32 = nullptr;
+    double *d_ke64 = nullptr;       // blocks packed per s (coarse build, Grad)
+    double *d_kt64 = nullptr;       // pair-major layout of the fine operator
+    float *d_kt32 = nullptr;
     // densities
     double *d_rho = nullptr, *d_w64 = nullptr;
     __nv_bfloat16 *d_wbf = nullptr;
@@ -182,10 +183,9 @@ template <typename T>
 int fine_apply(tosp_handle *h, const T *x, T *y) {
     CK(cudaMemsetAsync(y, 0, sizeof(T) * h->fg.g.ndof, h->stream));
     if constexpr (sizeof(T) == 8) {
-        launch_fine_apply<double, double>(x, y, h->d_w64, h->lev[0].fm, h->d_ke64, h->fg, h->n, false, h->stream);
+        launch_fine_apply<double, double>(x, y, h->d_w64, h->lev[0].fm, h->d_kt64, h->fg, h->n, h->stream);
     } else {
-        launch_fine_apply<float, __nv_bfloat16>(x, y, h->d_wbf, h->lev[0].fm, h->d_ke32, h->fg, h->n, false,
-                                                h->stream);
+        launch_fine_apply<float, __nv_bfloat16>(x, y, h->d_wbf, h->lev[0].fm, h->d_kt32, h->fg, h->n, h->stream);
     }
     CKL();
     return TOSP_OK;
@@ -434,11 +434,22 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
     std::vector<double> ks, packed;
     elem_stiff_mr(pb->el, pb->eh, pb->ew, pb->nu, h->n, ks);
     pack_upper(ks, h->ns, packed);
-    std::vector<float> packed32(packed.begin(), packed.end());
     TRY(dalloc(h, &h->d_ke64, (int64_t)packed.size()));
-    TRY(dalloc(h, &h->d_ke32, (int64_t)packed.size()));
     CK(cudaMemcpy(h->d_ke64, packed.data(), sizeof(double) * packed.size(), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(h->d_ke32, packed32.data(), sizeof(float) * packed32.size(), cudaMemcpyHostToDevice));
+    {
+        const int nsp64 = fine_nsp(h->n, 8), nsp32 = fine_nsp(h->n, 4);
+        std::vector<double> kt64((size_t)KE_PACK * nsp64, 0.0);
+        std::vector<float> kt32((size_t)KE_PACK * nsp32, 0.0f);
+        for (int t = 0; t < KE_PACK; ++t)
+            for (int s = 0; s < h->ns; ++s) {
+                kt64[(size_t)t * nsp64 + s] = packed[(size_t)s * KE_PACK + t];
+                kt32[(size_t)t * nsp32 + s] = (float)packed[(size_t)s * KE_PACK + t];
+            }
+        TRY(dalloc(h, &h->d_kt64, (int64_t)kt64.size()));
+        TRY(dalloc(h, &h->d_kt32, (int64_t)kt32.size()));
+        CK(cudaMemcpy(h->d_kt64, kt64.data(), sizeof(double) * kt64.size(), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(h->d_kt32, kt32.data(), sizeof(float) * kt32.size(), cudaMemcpyHostToDevice));
+    }
 
     // levels
     const size_t tsz = precision == TOSP_PREC_FP64 ? 8 : 4;
@@ -543,8 +554,7 @@ int setup_levels(tosp_handle *h) {
     const int64_t nd0 = h->lev[0].g.ndof;
     // finest diagonal (FP64) -> omega/diag in the cycle precision
     CK(cudaMemsetAsync(h->d_diag64, 0, sizeof(double) * nd0, h->stream));
-    launch_fine_apply<double, double>(nullptr, h->d_diag64, h->d_w64, h->lev[0].fm, h->d_ke64, h->fg, h->n, true,
-                                      h->stream);
+    launch_fine_diag(h->d_diag64, h->d_w64, h->lev[0].fm, h->d_kt64, h->fg, h->n, h->stream);
     CKL();
     if constexpr (sizeof(T) == 8) {
         launch_invert_diag<double>(h->d_diag64, h->lev[0].fm, (double *)h->lev[0].invd, h->mg.omega, nd0, h->stream);
@@ -883,14 +893,14 @@ int tosp_time_operator(tosp_handle *h, int32_t precision, int32_t reps, double *
         if (precision == TOSP_PREC_FP64) {
             CK(cudaMemsetAsync(h->cq, 0, sizeof(double) * g0.ndof, h->stream));
             CK(cudaEventRecord(a, h->stream));
-            launch_fine_apply<double, double>(h->cd, h->cq, h->d_w64, h->lev[0].fm, h->d_ke64, h->fg, h->n, false,
+            launch_fine_apply<double, double>(h->cd, h->cq, h->d_w64, h->lev[0].fm, h->d_kt64, h->fg, h->n,
                                               h->stream);
         } else {
             Level &F = h->lev[0];
             CK(cudaMemsetAsync(F.t, 0, sizeof(float) * g0.ndof, h->stream));
             CK(cudaEventRecord(a, h->stream));
-            launch_fine_apply<float, __nv_bfloat16>((const float *)F.x, (float *)F.t, h->d_wbf, F.fm, h->d_ke32,
-                                                    h->fg, h->n, false, h->stream);
+            launch_fine_apply<float, __nv_bfloat16>((const float *)F.x, (float *)F.t, h->d_wbf, F.fm, h->d_kt32,
+                                                    h->fg, h->n, h->stream);
         }
         CKL();
         CK(cudaEventRecord(b, h->stream));

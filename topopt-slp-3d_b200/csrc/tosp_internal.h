@@ -75,10 +75,15 @@ void launch_simp(const double *rho, double *w64, __nv_bfloat16 *wbf, int64_t n, 
                  double E, cudaStream_t st);
 
 // Fine MR operator y = K(w) x (y must be zeroed by the caller; fixed dofs of
-// y stay zero).  diag_only: y = diag(K(w)).
+// y stay zero).  kt: the n^3 blocks pair-major, see fine_nsp.
 template <typename T, typename TW>
-void launch_fine_apply(const T *x, T *y, const TW *w, const uint8_t *freemask, const T *kepack,
-                       const FineGeom &fg, int n, bool diag_only, cudaStream_t st);
+void launch_fine_apply(const T *x, T *y, const TW *w, const uint8_t *freemask, const T *kt, const FineGeom &fg,
+                       int n, cudaStream_t st);
+// y += diag(K(w)) (y zeroed by the caller).
+void launch_fine_diag(double *y, const double *w, const uint8_t *freemask, const double *kt64, const FineGeom &fg,
+                      int n, cudaStream_t st);
+// Stride of the pair-major block layout: entry t of block s at kt[t*nsp + s].
+int fine_nsp(int n, int elem_bytes);
 
 // Sensitivities g0 (I/Grad.m:24-49), zero for elements not in freeDensG.
 void launch_grad(const double *u, const double *rho, const uint8_t *free_elem, const double *kepack,
