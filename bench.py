@@ -188,6 +188,8 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--cpu-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--ngrids", type=int, default=0, help="override the workload's grid count")
+    ap.add_argument("--flexible", type=int, default=1, help="flexible (Polak-Ribiere) CG beta in both arms")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
@@ -223,8 +225,9 @@ def main():
     spec0 = WORKLOADS[args.workload]
     nelx, nely, nelz = spec0["dims"]
     pb0 = tosp.problems.cantilever(nelx, nely, nelz)
-    mg = tosp.default_mg(ngrids=spec0["ngrids"], cycle=0, omega=0.6, smoothiter1=1, smoothiter2=1, tolMG=1e-8,
-                         maxiterMG=1000)
+    ngrids = args.ngrids or spec0["ngrids"]
+    mg = tosp.default_mg(ngrids=ngrids, cycle=0, omega=0.6, smoothiter1=1, smoothiter2=1, tolMG=1e-8,
+                         maxiterMG=1000, flexible=args.flexible)
     n = spec0["n"]
     kw = dict(mr_n=n, p=3.0, emin=1e-9, opfilter=1, rmin=spec0["rmin"])
     holder["s64"] = tosp.Solver(pb0, mg, precision=tosp.PREC_FP64, **kw)
@@ -352,7 +355,7 @@ def main():
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 outer CG / f32+bf16 V-cycle",
         "data": "synthetic",
         "config": {"workload": args.workload, "mesh": list(spec["dims"]), "mr_n": n, "ndof": ndof,
-                   "nfree": int(pb.freedofs.size), "density_elements": int(nsub), "ngrids": spec["ngrids"],
+                   "nfree": int(pb.freedofs.size), "density_elements": int(nsub), "ngrids": ngrids, "cg_beta": "flexible" if args.flexible else "reference",
                    "cycle": "V", "omega": 0.6, "smooth": "1+1 Jacobi", "tol": 1e-8,
                    "l2": "inputs larger than L2 (densities 113 MB, vectors 44 MB each)",
                    "parallelism": f"replicas x{world}"},

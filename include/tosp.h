@@ -80,6 +80,10 @@ typedef struct tosp_mg_params {
     double  tolMG;         /* relative residual tolerance                             */
     int32_t maxiterMG;     /* iteration cap                                            */
     int32_t nmaxchol;      /* largest coarsest-grid system for the direct solve        */
+    int32_t flexible;      /* 0: beta = rho/rho_old as in I/SolveMG.m:43-46 (default);
+                              1: flexible (Polak-Ribiere) beta = r'(s - s_old)/rho_old,
+                              robust to a preconditioner that varies between applications
+                              (FP32 V-cycle with atomics)                                    */
 } tosp_mg_params;
 
 /* Statistics of the last tosp_solve_mg call. */

@@ -4,9 +4,9 @@
 // amd + sparse chol and applies eH = R\(R'\rH(perm)) in every cycle
 // (I/SetupGMG.m:51-59, I/VCycle.m:40).  Here the coarsest matrix is assembled
 // densely (fixed dofs decoupled with a unit diagonal, padded to a multiple of
-// 32 with identity), factored A = L L' by a blocked right-looking Cholesky,
-// and inverted once (L Y = I, L' X = Y, both blocked over 32x32 tiles), so that
-// each cycle's coarse solve is a single FP64 GEMV that runs from L2.
+// 32 with identity) and inverted once per setup in place by a blocked
+// symmetric sweep, so that each cycle's coarse solve is a single FP64 GEMV
+// that runs from L2.
 #include "tosp_internal.h"
 
 namespace tosp {
@@ -45,161 +45,97 @@ void launch_dense_assemble(const double *Ae, const uint8_t *freemask, const Grid
     k_dense_unitdiag<<<64, 256, 0, st>>>(A, freemask, g.ndof, npad); count_launch();
 }
 
-// --- blocked Cholesky ------------------------------------------------------
-__global__ void k_potrf_tile(double *A, int64_t npad, int k, int *info) {
-    __shared__ double s[TS][TS + 1];
-    const int tx = threadIdx.x;   // 32 threads, one per row
-    double *base = A + (int64_t)k * TS * npad + (int64_t)k * TS;
-    for (int c = 0; c < TS; ++c) s[tx][c] = base[(int64_t)tx * npad + c];
-    __syncthreads();
-    for (int j = 0; j < TS; ++j) {
-        if (tx == j) {
-            const double d = s[j][j];
-            if (!(d > 0.0)) {
-                atomicExch(info, 1 + k * TS + j);
-                s[j][j] = 1.0;
-            } else {
-                s[j][j] = sqrt(d);
-            }
-        }
-        __syncthreads();
-        if (tx > j) s[tx][j] /= s[j][j];
-        __syncthreads();
-        if (tx > j)
-            for (int l = j + 1; l <= tx; ++l) s[tx][l] -= s[tx][j] * s[l][j];
-        __syncthreads();
-    }
-    for (int c = 0; c < TS; ++c) base[(int64_t)tx * npad + c] = (c <= tx) ? s[tx][c] : 0.0;
-}
+// --- blocked symmetric sweep (block Gauss-Jordan) ----------------------------
+// Sweeping block k of a symmetric matrix:  P = A_kk,  C_i = A_ik P^{-1},
+//   A_ij -= C_i A_kj (i, j != k),  A_ik = C_i,  A_kj = C_j',  A_kk = -P^{-1}.
+// After all blocks the array holds -A^{-1}.  Every pivot block is a Schur
+// complement of the SPD matrix (a leading-block Cholesky factor exists), so no
+// pivoting is needed.  Each step is one small pivot inversion plus an
+// embarrassingly parallel rank-32 update of the whole matrix.
 
-// L_ik = A_ik L_kk^{-T} for tile rows i > k.
-__global__ void k_trsm_panel(double *A, int64_t npad, int k) {
-    __shared__ double L[TS][TS + 1];
-    __shared__ double X[TS][TS + 1];
-    const int tx = threadIdx.x;
-    const int i = k + 1 + blockIdx.x;
-    const double *lk = A + (int64_t)k * TS * npad + (int64_t)k * TS;
-    double *ai = A + (int64_t)i * TS * npad + (int64_t)k * TS;
-    for (int c = 0; c < TS; ++c) {
-        L[tx][c] = lk[(int64_t)tx * npad + c];
-        X[tx][c] = ai[(int64_t)tx * npad + c];
+// P^{-1} of the 32x32 pivot block by a scalar sweep in shared memory.
+__global__ void k_sweep_pivot(const double *A, int64_t npad, int k, double *Pinv, int *info) {
+    __shared__ double S[TS][TS + 1];
+    const int r = threadIdx.y, c = threadIdx.x;   // 32 x 32
+    S[r][c] = A[(int64_t)(k * TS + r) * npad + k * TS + c];
+    for (int p = 0; p < TS; ++p) {
+        __syncthreads();
+        const double d = S[p][p];
+        double v;
+        if (r == p && c == p) v = -1.0 / d;
+        else if (c == p) v = S[r][p] / d;
+        else if (r == p) v = S[p][c] / d;
+        else v = S[r][c] - S[r][p] * S[p][c] / d;
+        if (r == 0 && c == 0 && !(d > 0.0)) atomicExch(info, 1 + k * TS + p);
+        __syncthreads();
+        S[r][c] = v;
     }
     __syncthreads();
-    for (int j = 0; j < TS; ++j) {
-        double v = X[tx][j];
-        for (int p = 0; p < j; ++p) v -= X[tx][p] * L[j][p];
-        X[tx][j] = v / L[j][j];
-    }
-    for (int c = 0; c < TS; ++c) ai[(int64_t)tx * npad + c] = X[tx][c];
+    Pinv[r * TS + c] = -S[r][c];
 }
 
-// A_ij -= L_ik L_jk' for the lower tiles k < j <= i.
-__global__ void k_syrk(double *A, int64_t npad, int k) {
-    __shared__ double Li[TS][TS + 1];
-    __shared__ double Lj[TS][TS + 1];
+// C_i = A_ik P^{-1} for every row block i != k.
+__global__ void k_sweep_panel(const double *A, int64_t npad, int k, const double *Pinv, double *C) {
+    __shared__ double At[TS][TS + 1];
+    __shared__ double Pt[TS][TS + 1];
+    const int i = blockIdx.x;
+    if (i == k) return;
+    const int r = threadIdx.y, c = threadIdx.x;
+    At[r][c] = A[(int64_t)(i * TS + r) * npad + k * TS + c];
+    Pt[r][c] = Pinv[r * TS + c];
+    __syncthreads();
+    double v = 0.0;
+#pragma unroll 8
+    for (int q = 0; q < TS; ++q) v += At[r][q] * Pt[q][c];
+    C[(int64_t)(i * TS + r) * TS + c] = v;
+}
+
+// A_ij -= C_i A_kj for all tiles with i != k and j != k.
+__global__ void k_sweep_update(double *A, int64_t npad, int k, const double *C, int nb) {
+    __shared__ double Ct[TS][TS + 1];
+    __shared__ double Rt[TS][TS + 1];
     const int t = blockIdx.x;
-    int row = (int)((sqrt(8.0 * t + 1.0) - 1.0) / 2.0);
-    while ((row + 1) * (row + 2) / 2 <= t) ++row;
-    while (row * (row + 1) / 2 > t) --row;
-    const int col = t - row * (row + 1) / 2;
-    const int i = k + 1 + row, j = k + 1 + col;
-    const int tid = threadIdx.x;   // 256 threads
-    const double *li = A + (int64_t)i * TS * npad + (int64_t)k * TS;
-    const double *lj = A + (int64_t)j * TS * npad + (int64_t)k * TS;
-    for (int e = tid; e < TS * TS; e += blockDim.x) {
-        const int r = e / TS, c = e % TS;
-        Li[r][c] = li[(int64_t)r * npad + c];
-        Lj[r][c] = lj[(int64_t)r * npad + c];
-    }
+    const int i = t / nb, j = t % nb;
+    if (i == k || j == k) return;
+    const int r = threadIdx.y, c = threadIdx.x;
+    Ct[r][c] = C[(int64_t)(i * TS + r) * TS + c];
+    Rt[r][c] = A[(int64_t)(k * TS + r) * npad + j * TS + c];
     __syncthreads();
-    double *aij = A + (int64_t)i * TS * npad + (int64_t)j * TS;
-    for (int e = tid; e < TS * TS; e += blockDim.x) {
-        const int r = e / TS, c = e % TS;
-        double v = 0.0;
+    double v = 0.0;
 #pragma unroll 8
-        for (int p = 0; p < TS; ++p) v += Li[r][p] * Lj[c][p];
-        aij[(int64_t)r * npad + c] -= v;
+    for (int q = 0; q < TS; ++q) v += Ct[r][q] * Rt[q][c];
+    A[(int64_t)(i * TS + r) * npad + j * TS + c] -= v;
+}
+
+// Column and row blocks of k: A_ik = C_i, A_ki = C_i', A_kk = -P^{-1}.
+__global__ void k_sweep_setrc(double *A, int64_t npad, int k, const double *C, const double *Pinv) {
+    const int i = blockIdx.x;
+    const int r = threadIdx.y, c = threadIdx.x;
+    if (i == k) {
+        A[(int64_t)(k * TS + r) * npad + k * TS + c] = -Pinv[r * TS + c];
+    } else {
+        const double v = C[(int64_t)(i * TS + r) * TS + c];
+        A[(int64_t)(i * TS + r) * npad + k * TS + c] = v;
+        A[(int64_t)(k * TS + c) * npad + i * TS + r] = v;
     }
 }
 
-// --- inverse from the factor -------------------------------------------------
-// Forward: Y_kc = L_kk^{-1} (I_kc - sum_{c<=j<k} L_kj Y_jc), c <= k.
-__global__ void k_fwd(const double *A, double *Y, int64_t npad, int k) {
-    __shared__ double Lt[TS][TS + 1];
-    __shared__ double Bt[TS][TS + 1];
-    __shared__ double acc[TS][TS + 1];
-    const int c = blockIdx.x;   // column tile
-    const int r = threadIdx.y, q = threadIdx.x;   // 32 x 32
-    double v = (c == k && r == q) ? 1.0 : 0.0;
-    for (int j = c; j < k; ++j) {
-        Lt[r][q] = A[(int64_t)(k * TS + r) * npad + j * TS + q];
-        Bt[r][q] = Y[(int64_t)(j * TS + r) * npad + c * TS + q];
-        __syncthreads();
-#pragma unroll 8
-        for (int p = 0; p < TS; ++p) v -= Lt[r][p] * Bt[p][q];
-        __syncthreads();
-    }
-    acc[r][q] = v;
-    Lt[r][q] = A[(int64_t)(k * TS + r) * npad + k * TS + q];
-    __syncthreads();
-    if (r == 0) {   // one thread per column solves down the tile
-        for (int rr = 0; rr < TS; ++rr) {
-            double z = acc[rr][q];
-            for (int p = 0; p < rr; ++p) z -= Lt[rr][p] * acc[p][q];
-            acc[rr][q] = z / Lt[rr][rr];
-        }
-    }
-    __syncthreads();
-    Y[(int64_t)(k * TS + r) * npad + c * TS + q] = acc[r][q];
+__global__ void k_negate(double *A, int64_t nn) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nn; i += (int64_t)gridDim.x * blockDim.x)
+        A[i] = -A[i];
 }
 
-// Backward (in place over Y): X_kc = L_kk^{-T} (Y_kc - sum_{j>k} L_jk' X_jc).
-__global__ void k_bwd(const double *A, double *X, int64_t npad, int k, int nb) {
-    __shared__ double Lt[TS][TS + 1];
-    __shared__ double Bt[TS][TS + 1];
-    __shared__ double acc[TS][TS + 1];
-    const int c = blockIdx.x;
-    const int r = threadIdx.y, q = threadIdx.x;
-    double v = X[(int64_t)(k * TS + r) * npad + c * TS + q];
-    for (int j = k + 1; j < nb; ++j) {
-        Lt[r][q] = A[(int64_t)(j * TS + r) * npad + k * TS + q];   // L_jk[r][q]
-        Bt[r][q] = X[(int64_t)(j * TS + r) * npad + c * TS + q];
-        __syncthreads();
-#pragma unroll 8
-        for (int p = 0; p < TS; ++p) v -= Lt[p][r] * Bt[p][q];
-        __syncthreads();
-    }
-    acc[r][q] = v;
-    Lt[r][q] = A[(int64_t)(k * TS + r) * npad + k * TS + q];
-    __syncthreads();
-    if (r == 0) {
-        for (int rr = TS - 1; rr >= 0; --rr) {
-            double z = acc[rr][q];
-            for (int p = rr + 1; p < TS; ++p) z -= Lt[p][rr] * acc[p][q];
-            acc[rr][q] = z / Lt[rr][rr];
-        }
-    }
-    __syncthreads();
-    X[(int64_t)(k * TS + r) * npad + c * TS + q] = acc[r][q];
-}
-
-int dense_cholesky_inverse(double *A, double *X, int64_t npad, int *d_info, cudaStream_t st) {
+int dense_sweep_inverse(double *A, double *C, double *Pinv, int64_t npad, int *d_info, cudaStream_t st) {
     const int nb = (int)(npad / TS);
+    const dim3 blk(TS, TS);
     cudaMemsetAsync(d_info, 0, sizeof(int), st);
     for (int k = 0; k < nb; ++k) {
-        k_potrf_tile<<<1, TS, 0, st>>>(A, npad, k, d_info); count_launch();
-        const int m = nb - k - 1;
-        if (m > 0) {
-            k_trsm_panel<<<m, TS, 0, st>>>(A, npad, k); count_launch();
-            k_syrk<<<m * (m + 1) / 2, 256, 0, st>>>(A, npad, k); count_launch();
-        }
+        k_sweep_pivot<<<1, blk, 0, st>>>(A, npad, k, Pinv, d_info); count_launch();
+        k_sweep_panel<<<nb, blk, 0, st>>>(A, npad, k, Pinv, C); count_launch();
+        k_sweep_update<<<nb * nb, blk, 0, st>>>(A, npad, k, C, nb); count_launch();
+        k_sweep_setrc<<<nb, blk, 0, st>>>(A, npad, k, C, Pinv); count_launch();
     }
-    const dim3 blk(TS, TS);
-    // tiles above the block diagonal of L^{-1} are zero and are read by the
-    // backward sweep
-    cudaMemsetAsync(X, 0, sizeof(double) * npad * npad, st);
-    for (int k = 0; k < nb; ++k) k_fwd<<<k + 1, blk, 0, st>>>(A, X, npad, k); count_launch();
-    for (int k = nb - 1; k >= 0; --k) k_bwd<<<nb, blk, 0, st>>>(A, X, npad, k, nb); count_launch();
+    k_negate<<<1024, 256, 0, st>>>(A, npad * npad); count_launch();
     return 0;
 }
 

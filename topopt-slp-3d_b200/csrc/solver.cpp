@@ -64,12 +64,12 @@ struct tosp_handle {
     // hierarchy
     std::vector<Level> lev;
     double *d_diag64 = nullptr;     // diag of the finest operator
-    double *d_Adense = nullptr, *d_Xinv = nullptr;
+    double *d_Adense = nullptr, *d_sweepC = nullptr, *d_pinv = nullptr;   // coarsest: A, then A^{-1}
     int64_t ncoarse = 0, npad = 0;
     int *d_info = nullptr;
     bool setup_done = false;
     // CG (FP64, full-length vectors with zeros on fixed dofs)
-    double *cx = nullptr, *cr = nullptr, *cd = nullptr, *cq = nullptr, *cs = nullptr, *cf = nullptr;
+    double *cx = nullptr, *cr = nullptr, *cd = nullptr, *cq = nullptr, *cs = nullptr, *cf = nullptr, *cso = nullptr;
     double *d_partials = nullptr, *d_scal = nullptr, *h_scal = nullptr;
     // staging
     double *d_stage_a = nullptr, *d_stage_b = nullptr;
@@ -231,7 +231,7 @@ int residual(tosp_handle *h, int l) {
 template <typename T>
 int coarse_solve(tosp_handle *h) {
     Level &C = h->lev[h->ngrids - 1];
-    launch_dense_solve<T>(h->d_Xinv, (const T *)C.b, (T *)C.x, C.g.ndof, h->npad, h->stream);
+    launch_dense_solve<T>(h->d_Adense, (const T *)C.b, (T *)C.x, C.g.ndof, h->npad, h->stream);
     CKL();
     return TOSP_OK;
 }
@@ -477,7 +477,8 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
     TRY(dalloc(h, &h->d_diag64, g0.ndof));
     if (h->mg_ok) {
         TRY(dalloc(h, &h->d_Adense, h->npad * h->npad));
-        TRY(dalloc(h, &h->d_Xinv, h->npad * h->npad));
+        TRY(dalloc(h, &h->d_sweepC, h->npad * 32));
+        TRY(dalloc(h, &h->d_pinv, 32 * 32));
     }
     TRY(dalloc(h, &h->d_info, 1));
     // densities
@@ -507,6 +508,7 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
     TRY(dalloc(h, &h->cq, g0.ndof));
     TRY(dalloc(h, &h->cs, g0.ndof));
     TRY(dalloc(h, &h->cf, g0.ndof));
+    if (mg->flexible) TRY(dalloc(h, &h->cso, g0.ndof));
     TRY(dalloc(h, &h->d_partials, RED_BLOCKS));
     TRY(dalloc(h, &h->d_scal, 16));
     CK(cudaMallocHost(&h->h_scal, sizeof(double) * 16));
@@ -574,13 +576,13 @@ int setup_levels(tosp_handle *h) {
     Level &C = h->lev[ng - 1];
     launch_dense_assemble(C.Ae, C.fm, C.g, h->d_Adense, h->npad, h->stream);
     CKL();
-    dense_cholesky_inverse(h->d_Adense, h->d_Xinv, h->npad, h->d_info, h->stream);
+    dense_sweep_inverse(h->d_Adense, h->d_sweepC, h->d_pinv, h->npad, h->d_info, h->stream);
     CKL();
     int info = 0;
     CK(cudaMemcpyAsync(&info, h->d_info, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
     TRY(sync(h));
     if (info != 0) {
-        h->err = "coarsest-grid Cholesky failed: non-positive pivot at dof " + std::to_string(info - 1);
+        h->err = "coarsest-grid inversion failed: non-positive pivot at dof " + std::to_string(info - 1);
         return TOSP_ERR_BREAKDOWN;
     }
     return TOSP_OK;
@@ -632,7 +634,9 @@ int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
     while (nr > h->mg.tolMG && it <= h->mg.maxiterMG) {
         TRY(precondition(h, h->cr, h->cs));
         launch_dot(h->cr, h->cs, nd, h->d_partials, h->d_scal + 0, h->stream);
-        launch_pcg_direction(h->cd, h->cs, h->d_scal, nd, it == 1 ? 1 : 0, h->stream);
+        const bool flex = h->mg.flexible && it > 1;
+        if (flex) launch_dot(h->cr, h->cso, nd, h->d_partials, h->d_scal + 5, h->stream);
+        launch_pcg_direction(h->cd, h->cs, h->d_scal, nd, it == 1 ? 1 : (flex ? 2 : 0), h->stream);
         CKL();
         TRY(fine_apply64(h, h->cd, h->cq));
         launch_dot(h->cd, h->cq, nd, h->d_partials, h->d_scal + 2, h->stream);
@@ -647,6 +651,7 @@ int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
         }
         nr = std::sqrt(rr) / nf;
         ++it;
+        if (h->mg.flexible) std::swap(h->cs, h->cso);
     }
     if (rc == TOSP_OK && nr > h->mg.tolMG && it > h->mg.maxiterMG) rc = TOSP_NOT_CONVERGED;
     if (it_out) *it_out = it;
@@ -676,6 +681,7 @@ void tosp_default_mg_params(tosp_mg_params *mg) {
     mg->tolMG = 1e-8;
     mg->maxiterMG = 5000;
     mg->nmaxchol = 60000;
+    mg->flexible = 0;
 }
 
 int tosp_create(const tosp_problem *prob, const tosp_mg_params *mg, int32_t precision, tosp_handle **out) {

@@ -122,10 +122,11 @@ void launch_coarse_freemask(const uint8_t *freemask_f, uint8_t *freemask_c, cons
                             const Grid &gc, cudaStream_t st);
 
 // Coarsest direct solve: dense SPD matrix (padded to a multiple of 32, fixed
-// dofs decoupled with a unit diagonal), Cholesky, explicit inverse, GEMV.
+// dofs decoupled with a unit diagonal), explicit inverse in place by a blocked
+// symmetric sweep (C: npad x 32 workspace, Pinv: 32 x 32), GEMV.
 void launch_dense_assemble(const double *Ae, const uint8_t *freemask, const Grid &g, double *A,
                            int64_t npad, cudaStream_t st);
-int dense_cholesky_inverse(double *A, double *X, int64_t npad, int *d_info, cudaStream_t st);
+int dense_sweep_inverse(double *A, double *C, double *Pinv, int64_t npad, int *d_info, cudaStream_t st);
 template <typename T>
 void launch_dense_solve(const double *X, const T *b, T *x, int64_t n, int64_t npad, cudaStream_t st);
 
@@ -143,7 +144,7 @@ void launch_convert(const TI *a, TO *b, int64_t n, cudaStream_t st);
 constexpr int RED_BLOCKS = 592;
 void launch_dot(const double *a, const double *b, int64_t n, double *partials, double *out, cudaStream_t st);
 // PCG pieces (scalars in device memory, see solver.cpp for the slots).
-void launch_pcg_direction(double *d, const double *s, const double *scal, int64_t n, int first,
+void launch_pcg_direction(double *d, const double *s, const double *scal, int64_t n, int mode,
                           cudaStream_t st);
 void launch_pcg_update(double *x, double *r, const double *d, const double *q, double *scal, double *partials,
                        int64_t n, cudaStream_t st);

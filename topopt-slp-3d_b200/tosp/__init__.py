@@ -49,7 +49,7 @@ class MgParams(C.Structure):
     """The ``mg.*`` struct of the reference (I/TopOpt3D.m:171-190)."""
     _fields_ = [("ngrids", C.c_int32), ("cycle", C.c_int32), ("smoother", C.c_int32), ("omega", C.c_double),
                 ("smoothiter1", C.c_int32), ("smoothiter2", C.c_int32), ("tolMG", C.c_double),
-                ("maxiterMG", C.c_int32), ("nmaxchol", C.c_int32)]
+                ("maxiterMG", C.c_int32), ("nmaxchol", C.c_int32), ("flexible", C.c_int32)]
 
 
 class SolveStats(C.Structure):
