@@ -10,10 +10,10 @@
 // 300 (n^3 + 2) FMAs per element instead of 600 n^3 for block-by-block
 // products.  A persistent CTA walks
 // element bricks of BX x BY x BZ: it stages the brick's nodal values in
-// shared memory, each thread forms one element's 24 outputs, the outputs are
-// summed into a shared node brick in 8 parity colours (elements of one colour
-// share no node), and the brick is written back with plain stores for nodes
-// only this brick touches and atomics on the brick faces.
+// shared memory, each thread forms one element's 24 outputs into shared slots,
+// every brick node then gathers the contributions of its (up to 8) elements,
+// and the result is written with plain stores for nodes only this brick
+// touches and atomics on the brick faces.
 #include <cuda_bf16.h>
 
 #include <utility>
@@ -91,20 +91,19 @@ k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *kt = reinterpret_cast<T *>(smem_raw);               // KE_PACK * NSP (pair-major)
     T *xs = kt + KE_PACK * NSP;                             // BRICK_NODES * 3
-    T *ys = xs + BRICK_NODES * 3;                           // BRICK_NODES * 3
+    T *eo = xs + BRICK_NODES * 3;                           // 24 * BRICK_ELEMS element outputs
     const int tid = threadIdx.x;
     for (int i = tid; i < KE_PACK * NSP; i += BRICK_ELEMS) kt[i] = ktg[i];
 
     const Grid &g = fg.g;
     const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
-    const int color = (lx & 1) | ((ly & 1) << 1) | ((lz & 1) << 2);
 
     for (int64_t brick = blockIdx.x; brick < fg.nbricks; brick += gridDim.x) {
         const int bby = (int)(brick % fg.nby);
         const int bbx = (int)((brick / fg.nby) % fg.nbx);
         const int bbz = (int)(brick / ((int64_t)fg.nby * fg.nbx));
         const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
-        __syncthreads();   // previous brick done with xs/ys (and kt loaded)
+        __syncthreads();   // previous brick done with xs/eo (and kt loaded)
         for (int i = tid; i < BRICK_NODES * 3; i += BRICK_ELEMS) {
             const int ln = i / 3, c = i - 3 * ln;
             const int ny_ = ln % NBY, nx_ = (ln / NBY) % NBX, nz_ = ln / (NBY * NBX);
@@ -112,7 +111,6 @@ k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ 
             T v = T(0);
             if (gx < g.nx && gy < g.ny && gz < g.nz) v = x[3 * (((int64_t)gz * g.nx + gx) * g.ny + gy) + c];
             xs[i] = v;
-            ys[i] = T(0);
         }
         __syncthreads();
 
@@ -142,20 +140,11 @@ k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ 
             }
             all_pairs<T, NSP>(kt, wv, u, acc, std::make_integer_sequence<int, KE_PACK>{});
         }
-        // colour-ordered accumulation into the node brick
-#pragma unroll 1
-        for (int col = 0; col < 8; ++col) {
-            if (valid && col == color) {
+        // element outputs -> per-element slots, then every node gathers the
+        // (up to 8) contributions of the brick's elements around it
 #pragma unroll
-                for (int a = 0; a < 8; ++a) {
-                    const int dx = (a >> 1) & 1, dy = a & 1, dz = (a >> 2) & 1;
-                    const int ln = ((lz + dz) * NBX + (lx + dx)) * NBY + (ly + dy);
-#pragma unroll
-                    for (int c = 0; c < 3; ++c) ys[3 * ln + c] += acc[3 * a + c];
-                }
-            }
-            __syncthreads();
-        }
+        for (int k = 0; k < 24; ++k) eo[k * BRICK_ELEMS + tid] = acc[k];
+        __syncthreads();
         for (int i = tid; i < BRICK_NODES * 3; i += BRICK_ELEMS) {
             const int ln = i / 3, c = i - 3 * ln;
             const int ny_ = ln % NBY, nx_ = (ln / NBY) % NBX, nz_ = ln / (NBY * NBX);
@@ -163,9 +152,17 @@ k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ 
             if (gx < g.nx && gy < g.ny && gz < g.nz) {
                 const int64_t dof = 3 * (((int64_t)gz * g.nx + gx) * g.ny + gy) + c;
                 if (freemask[dof]) {
+                    T v = T(0);
+#pragma unroll
+                    for (int a = 0; a < 8; ++a) {
+                        const int dx = (a >> 1) & 1, dy = a & 1, dz = (a >> 2) & 1;
+                        const int ex_ = nx_ - dx, ey_ = ny_ - dy, ez_ = nz_ - dz;
+                        if (ex_ >= 0 && ex_ < BX && ey_ >= 0 && ey_ < BY && ez_ >= 0 && ez_ < BZ)
+                            v += eo[(3 * a + c) * BRICK_ELEMS + (ez_ * BX + ex_) * BY + ey_];
+                    }
                     const bool inner = nx_ > 0 && nx_ < BX && ny_ > 0 && ny_ < BY && nz_ > 0 && nz_ < BZ;
-                    if (inner) y[dof] = ys[i];
-                    else atomic_add(&y[dof], ys[i]);
+                    if (inner) y[dof] = v;
+                    else atomic_add(&y[dof], v);
                 }
             }
         }
@@ -216,7 +213,7 @@ template <typename T, typename TW, int N>
 static void launch_fine_t(const T *x, T *y, const TW *w, const uint8_t *fm, const T *kt, const FineGeom &fg,
                           cudaStream_t st) {
     constexpr int NSP = FineShape<T, N>::NSP;
-    const size_t smem = sizeof(T) * (KE_PACK * NSP + 2 * BRICK_NODES * 3);
+    const size_t smem = sizeof(T) * (KE_PACK * NSP + BRICK_NODES * 3 + 24 * BRICK_ELEMS);
     auto kern = k_fine_apply<T, TW, N>;
     static int attr_dev = -1;
     int dev = 0;
@@ -270,20 +267,26 @@ __device__ __forceinline__ double powp(double x, double p) {
     return pow(x, p);
 }
 
-__global__ void k_simp(const double *rho, double *w64, __nv_bfloat16 *wbf, int64_t n, double p, double emin,
-                       double E) {
+// wq (optional) receives the BF16-rounded factors widened back to FP64, so
+// that the mixed V-cycle's Galerkin hierarchy matches its finest operator.
+__global__ void k_simp(const double *rho, double *w64, __nv_bfloat16 *wbf, double *wq, int64_t n, double p,
+                       double emin, double E) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const double w = emin + (E - emin) * powp(rho[i], p);
         w64[i] = w;
-        if (wbf) wbf[i] = __double2bfloat16(w);
+        if (wbf) {
+            const __nv_bfloat16 b = __double2bfloat16(w);
+            wbf[i] = b;
+            if (wq) wq[i] = (double)__bfloat162float(b);
+        }
     }
 }
 
-void launch_simp(const double *rho, double *w64, __nv_bfloat16 *wbf, int64_t n, double p, double emin, double E,
-                 cudaStream_t st) {
+void launch_simp(const double *rho, double *w64, __nv_bfloat16 *wbf, double *wq, int64_t n, double p, double emin,
+                 double E, cudaStream_t st) {
     int64_t blocks = (n + 255) / 256;
     if (blocks > 4096) blocks = 4096;
-    k_simp<<<(unsigned)blocks, 256, 0, st>>>(rho, w64, wbf, n, p, emin, E); count_launch();
+    k_simp<<<(unsigned)blocks, 256, 0, st>>>(rho, w64, wbf, wq, n, p, emin, E); count_launch();
 }
 
 // ---------------------------------------------------------------------------

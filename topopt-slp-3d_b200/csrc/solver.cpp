@@ -54,6 +54,7 @@ struct tosp_handle {
     float *d_kt32 = nullptr;
     // densities
     double *d_rho = nullptr, *d_w64 = nullptr;
+    double *d_wq = nullptr;         // mixed: BF16-rounded factors in FP64 (V-cycle hierarchy)
     __nv_bfloat16 *d_wbf = nullptr;
     uint8_t *d_free_elem = nullptr;
     // filter
@@ -485,7 +486,10 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
     const int64_t nd = h->dens.nelem;
     TRY(dalloc(h, &h->d_rho, nd));
     TRY(dalloc(h, &h->d_w64, nd));
-    if (precision == TOSP_PREC_MIXED) TRY(dalloc(h, &h->d_wbf, nd));
+    if (precision == TOSP_PREC_MIXED) {
+        TRY(dalloc(h, &h->d_wbf, nd));
+        TRY(dalloc(h, &h->d_wq, nd));
+    }
     TRY(dalloc(h, &h->d_free_elem, g0.nelem));
     {
         std::vector<uint8_t> fe(g0.nelem, pb->free_dens_g ? 0 : 1);
@@ -556,7 +560,10 @@ int setup_levels(tosp_handle *h) {
     const int64_t nd0 = h->lev[0].g.ndof;
     // finest diagonal (FP64) -> omega/diag in the cycle precision
     CK(cudaMemsetAsync(h->d_diag64, 0, sizeof(double) * nd0, h->stream));
-    launch_fine_diag(h->d_diag64, h->d_w64, h->lev[0].fm, h->d_kt64, h->fg, h->n, h->stream);
+    // the V-cycle hierarchy is Galerkin-consistent with the V-cycle's finest
+    // operator: FP64 factors for the FP64 path, the BF16-rounded ones for mixed
+    const double *wh = h->d_wq ? h->d_wq : h->d_w64;
+    launch_fine_diag(h->d_diag64, wh, h->lev[0].fm, h->d_kt64, h->fg, h->n, h->stream);
     CKL();
     if constexpr (sizeof(T) == 8) {
         launch_invert_diag<double>(h->d_diag64, h->lev[0].fm, (double *)h->lev[0].invd, h->mg.omega, nd0, h->stream);
@@ -565,7 +572,7 @@ int setup_levels(tosp_handle *h) {
         launch_convert<double, float>(h->cs, (float *)h->lev[0].invd, nd0, h->stream);
     }
     CKL();
-    launch_coarse_from_fine(h->d_w64, h->lev[0].fm, h->d_ke64, h->lev[1].Ae, h->fg, h->lev[1].g, h->n, h->stream);
+    launch_coarse_from_fine(wh, h->lev[0].fm, h->d_ke64, h->lev[1].Ae, h->fg, h->lev[1].g, h->n, h->stream);
     CKL();
     for (int l = 1; l < ng - 1; ++l) {
         Level &L = h->lev[l];
@@ -739,7 +746,7 @@ int tosp_setup_gmg(tosp_handle *h, const double *xfil, int64_t ndens) {
     TRY(check_len(h, ndens, h->dens.nelem, "densities"));
     CK(cudaEventRecord(h->ev0, h->stream));
     TRY(load_vec(h, h->d_rho, xfil, ndens));
-    launch_simp(h->d_rho, h->d_w64, h->d_wbf, ndens, h->p, h->emin, h->E, h->stream);
+    launch_simp(h->d_rho, h->d_w64, h->d_wbf, h->d_wq, ndens, h->p, h->emin, h->E, h->stream);
     CKL();
     h->setup_done = false;
     if (h->mg_ok) {

@@ -70,8 +70,9 @@ void filter_taps(double rmin, double el, double eh, double ew, int opfilter, std
 // ---------------------------------------------------------------------------
 // Kernel launchers.  All take the stream of the handle.
 // ---------------------------------------------------------------------------
-// SIMP factors w = emin + (E-emin) rho^p, in FP64 and BF16.
-void launch_simp(const double *rho, double *w64, __nv_bfloat16 *wbf, int64_t n, double p, double emin,
+// SIMP factors w = emin + (E-emin) rho^p, in FP64 and (optionally) BF16 plus
+// the BF16 values widened to FP64.
+void launch_simp(const double *rho, double *w64, __nv_bfloat16 *wbf, double *wq, int64_t n, double p, double emin,
                  double E, cudaStream_t st);
 
 // Fine MR operator y = K(w) x (y must be zeroed by the caller; fixed dofs of
