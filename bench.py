@@ -178,6 +178,24 @@ def cpu_baseline(args, pb, n, xfil, spec, it_fp64):
                        f"{t3 - t0:.1f} s timed; full solve projected as setup + {it_fp64} x iteration + Grad")}
 
 
+def profile_kernels(args):
+    import torch
+    import tosp
+    from tosp.workloads import WORKLOADS, build_workload
+    spec = WORKLOADS[args.workload]
+    pb, n, xfil, spec = build_workload(args.workload)
+    mg = tosp.default_mg(ngrids=args.ngrids or spec["ngrids"], cycle=0, omega=0.6, tolMG=1e-8, maxiterMG=1000)
+    s = tosp.Solver(pb, mg, precision=tosp.PREC_MIXED, mr_n=n, p=3.0, emin=1e-9, opfilter=1, rmin=spec["rmin"])
+    s.SetupGMG(xfil)
+    r = np.random.default_rng(0).standard_normal(pb.freedofs.size)
+    s.KelemProd(r)       # k_fine_apply<double,double>
+    s.MGCycle(r)         # two k_fine_apply<float,bf16> launches
+    torch.cuda.synchronize()
+    s.close()
+    print("profile run done")
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -190,10 +208,15 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ngrids", type=int, default=0, help="override the workload's grid count")
     ap.add_argument("--flexible", type=int, default=1, help="flexible (Polak-Ribiere) CG beta in both arms")
+    ap.add_argument("--profile-kernels", action="store_true",
+                    help="one mixed-precision handle: setup, one FP64 product and one V-cycle, then exit "
+                         "(a short run for ncu captures of the operator kernels)")
     args = ap.parse_args()
     world, rank, local = dist_setup()
     if args.impl == "reference":
         return run_reference(args, world, rank)
+    if args.profile_kernels:
+        return profile_kernels(args)
 
     import torch
     import torch.distributed as dist
