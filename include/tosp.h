@@ -178,6 +178,18 @@ int64_t tosp_kernel_launches(void);
  * handles only).  Writes the mean device time per launch in ms. */
 int tosp_time_operator(tosp_handle *h, int32_t precision, int32_t reps, double *ms_per_launch);
 
+/* KelemProd for callers that cannot allocate device memory at call time
+ * (stream capture in progress, a host-managed GPU memory pool such as a
+ * MATLAB gpuArray session, or multi-stream pipelines where cudaMalloc would
+ * synchronise the device).  No counterpart in the reference: it is
+ * tosp_kelem_prod restricted to device pointers, with its scratch (two
+ * full-length vectors) taken from a fixed 16 MiB array built into the
+ * library instead of the handle.  Problems above 1,048,576 dofs (3*nnodes) are
+ * rejected with TOSP_ERR_BAD_ARG.  The first call on a device resolves the
+ * array's address and should come before any stream capture.  All calls share
+ * the array: calls whose GPU work overlaps race. */
+int tosp_kelem_prod_noalloc(tosp_handle *h, const double *x, double *y, int64_t nfree);
+
 /* Host-only: the n^3 sub-element stiffness blocks kv (576 x n^3, column s is
  * k{s}(:), column-major) of I/ElemStiffMatrixGQMR.m:1 for hex8 elements. */
 int tosp_elem_stiff_mr(double el, double eh, double ew, double nu, int32_t n, double *kv);

@@ -670,6 +670,29 @@ int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
 
 }  // namespace
 
+// KelemProd on device free-dof vectors with caller-provided full-length
+// scratch (xfull, yfull: ndof doubles each); allocates nothing.
+int tosp::kelem_prod_with_scratch(tosp_handle *h, const double *x, double *y, int64_t nfree, double *xfull,
+                                  double *yfull) {
+    if (!is_device_ptr(x) || !is_device_ptr(y)) {
+        h->err = "x and y must be device pointers (this entry point stages nothing)";
+        return TOSP_ERR_BAD_ARG;
+    }
+    TRY(check_len(h, nfree, h->nfree, "x"));
+    TRY(need_setup(h));
+    CK(cudaMemsetAsync(xfull, 0, sizeof(double) * h->fg.g.ndof, h->stream));
+    launch_scatter_free(x, h->d_freeidx, h->nfree, xfull, h->stream);
+    CKL();
+    TRY(fine_apply64(h, xfull, yfull));
+    launch_gather_free(yfull, h->d_freeidx, h->nfree, y, h->stream);
+    CKL();
+    return sync(h);
+}
+
+int64_t tosp::handle_ndof(const tosp_handle *h) { return h->fg.g.ndof; }
+int tosp::handle_device(const tosp_handle *h) { return h->device; }
+void tosp::set_handle_error(tosp_handle *h, const std::string &msg) { h->err = msg; }
+
 // =============================================================================
 // C ABI
 // =============================================================================

@@ -151,4 +151,11 @@ void launch_pcg_update(double *x, double *r, const double *d, const double *q, d
                        int64_t n, cudaStream_t st);
 void launch_set_scalar(double *dst, const double *src, cudaStream_t st);
 
+// Handle internals used by entry points that live outside solver.cpp.
+int kelem_prod_with_scratch(tosp_handle *h, const double *x, double *y, int64_t nfree, double *xfull,
+                            double *yfull);
+int64_t handle_ndof(const tosp_handle *h);
+int handle_device(const tosp_handle *h);
+void set_handle_error(tosp_handle *h, const std::string &msg);
+
 }  // namespace tosp

@@ -83,6 +83,7 @@ def _load():
         "tosp_elem_stiff_mr": (C.c_int, [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int32, d]),
         "tosp_kernel_launches": (C.c_int64, []),
         "tosp_time_operator": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, P(C.c_double)]),
+        "tosp_kelem_prod_noalloc": (C.c_int, [C.c_void_p, d, d, C.c_int64]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
