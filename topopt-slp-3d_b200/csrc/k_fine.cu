@@ -29,17 +29,6 @@ __device__ __forceinline__ float wval(float v) { return v; }
 __device__ __forceinline__ void atomic_add(double *p, double v) { atomicAdd(p, v); }
 __device__ __forceinline__ void atomic_add(float *p, float v) { atomicAdd(p, v); }
 
-// Row/column of packed upper-triangle entry t (row-major, i <= j).
-__host__ __device__ constexpr int pair_i(int t) {
-    int i = 0;
-    while (t >= 24 - i) {
-        t -= 24 - i;
-        ++i;
-    }
-    return i;
-}
-__host__ __device__ constexpr int pair_j(int t) { return pair_i(t) + (t - (pair_i(t) * 24 - pair_i(t) * (pair_i(t) - 1) / 2)); }
-
 template <typename T> struct Vec;
 template <> struct Vec<float> { using type = float4; static constexpr int W = 4; };
 template <> struct Vec<double> { using type = double2; static constexpr int W = 2; };
@@ -48,7 +37,9 @@ __device__ __forceinline__ float dot_vec(const float4 v, const float *w) { retur
 __device__ __forceinline__ double dot_vec(const double2 v, const double *w) { return w[0] * v.x + w[1] * v.y; }
 
 // One packed entry t of the element matrix: k = sum_s w_s KE_s[i][j], then
-// y_i += k u_j and (for i != j) y_j += k u_i.
+// y_i += k u_j and (for i != j) y_j += k u_i.  Entries are visited diagonal
+// by diagonal (pair_i/pair_j) so consecutive updates hit different
+// accumulators.
 template <typename T, int NSP, int t>
 __device__ __forceinline__ void pair_step(const T *__restrict__ kt, const T (&w)[NSP], const T (&u)[24],
                                           T (&acc)[24]) {
@@ -57,11 +48,21 @@ __device__ __forceinline__ void pair_step(const T *__restrict__ kt, const T (&w)
     if constexpr (NSP == 1) {
         k = w[0] * kt[t];
     } else {
-        constexpr int W = Vec<T>::W;
+        // two independent partial sums halve the dependent FMA chain
+        constexpr int W = Vec<T>::W, NV = NSP / W;
         const typename Vec<T>::type *kv = reinterpret_cast<const typename Vec<T>::type *>(kt + t * NSP);
-        k = dot_vec(kv[0], w);
+        T k0 = dot_vec(kv[0], w);
+        if constexpr (NV > 1) {
+            T k1 = dot_vec(kv[1], w + W);
 #pragma unroll
-        for (int q = 1; q < NSP / W; ++q) k += dot_vec(kv[q], w + q * W);
+            for (int q = 2; q < NV; ++q) {
+                if (q % 2 == 0) k0 += dot_vec(kv[q], w + q * W);
+                else k1 += dot_vec(kv[q], w + q * W);
+            }
+            k = k0 + k1;
+        } else {
+            k = k0;
+        }
     }
     if constexpr (i == j) {
         acc[i] += k * u[i];
@@ -179,7 +180,7 @@ __global__ void k_fine_diag(double *__restrict__ y, const double *__restrict__ w
          e += (int64_t)gridDim.x * blockDim.x) {
         const int ey = (int)(e % g.nely), ex = (int)((e / g.nely) % g.nelx), ez = (int)(e / ((int64_t)g.nely * g.nelx));
         for (int i = 0; i < 24; ++i) {
-            const int t = i * 24 - i * (i - 1) / 2;
+            const int t = pair_index_diag(i);
             double d = 0.0;
             for (int s = 0; s < NS; ++s) {
                 const int sy = s % N, sx = (s / N) % N, sz = s / (N * N);

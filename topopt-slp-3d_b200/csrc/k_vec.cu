@@ -78,14 +78,19 @@ void launch_dot(const double *a, const double *b, int64_t n, double *partials, d
 
 // Scalar slots (see solver.cpp): 0 rho, 1 gamma2 (previous rho), 2 d'q, 3 r'r,
 // 5 r's_old.  mode 1: first iteration (d = s); 0: beta = rho/gamma2
-// (I/SolveMG.m:43-46); 2: flexible beta = (rho - r's_old)/gamma2.
-__global__ void k_pcg_direction(double *d, const double *s, const double *scal, int64_t n, int mode) {
+// (I/SolveMG.m:43-46); 2: flexible beta = (rho - r's_old)/gamma2.  When sold
+// is given it receives s (the next iteration's s_old).
+__global__ void k_pcg_direction(double *d, const double *s, double *sold, const double *scal, int64_t n, int mode) {
     const double beta = mode == 1 ? 0.0 : (mode == 2 ? (scal[0] - scal[5]) / scal[1] : scal[0] / scal[1]);
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        d[i] = mode == 1 ? s[i] : beta * d[i] + s[i];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double si = s[i];
+        d[i] = mode == 1 ? si : beta * d[i] + si;
+        if (sold) sold[i] = si;
+    }
 }
-void launch_pcg_direction(double *d, const double *s, const double *scal, int64_t n, int mode, cudaStream_t st) {
-    k_pcg_direction<<<gridv(n), 256, 0, st>>>(d, s, scal, n, mode); count_launch();
+void launch_pcg_direction(double *d, const double *s, double *sold, const double *scal, int64_t n, int mode,
+                          cudaStream_t st) {
+    k_pcg_direction<<<gridv(n), 256, 0, st>>>(d, s, sold, scal, n, mode); count_launch();
 }
 
 // x += alpha d ; r -= alpha q ; partial sums of r'r  (alpha = rho / d'q)

@@ -69,6 +69,8 @@ struct tosp_handle {
     int64_t ncoarse = 0, npad = 0;
     int *d_info = nullptr;
     bool setup_done = false;
+    cudaGraphExec_t iter_graph = nullptr;   // one CG iteration (it >= 2), captured once per handle
+    bool graph_failed = false;
     // CG (FP64, full-length vectors with zeros on fixed dofs)
     double *cx = nullptr, *cr = nullptr, *cd = nullptr, *cq = nullptr, *cs = nullptr, *cf = nullptr, *cso = nullptr;
     double *d_partials = nullptr, *d_scal = nullptr, *h_scal = nullptr;
@@ -441,11 +443,13 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
         const int nsp64 = fine_nsp(h->n, 8), nsp32 = fine_nsp(h->n, 4);
         std::vector<double> kt64((size_t)KE_PACK * nsp64, 0.0);
         std::vector<float> kt32((size_t)KE_PACK * nsp32, 0.0f);
-        for (int t = 0; t < KE_PACK; ++t)
+        for (int t = 0; t < KE_PACK; ++t) {
+            const int rm = pair_rowmajor(pair_i(t), pair_j(t));
             for (int s = 0; s < h->ns; ++s) {
-                kt64[(size_t)t * nsp64 + s] = packed[(size_t)s * KE_PACK + t];
-                kt32[(size_t)t * nsp32 + s] = (float)packed[(size_t)s * KE_PACK + t];
+                kt64[(size_t)t * nsp64 + s] = packed[(size_t)s * KE_PACK + rm];
+                kt32[(size_t)t * nsp32 + s] = (float)packed[(size_t)s * KE_PACK + rm];
             }
+        }
         TRY(dalloc(h, &h->d_kt64, (int64_t)kt64.size()));
         TRY(dalloc(h, &h->d_kt32, (int64_t)kt32.size()));
         CK(cudaMemcpy(h->d_kt64, kt64.data(), sizeof(double) * kt64.size(), cudaMemcpyHostToDevice));
@@ -624,6 +628,45 @@ int read_scalars(tosp_handle *h) {
     return sync(h);
 }
 
+// One iteration of I/SolveMG.m:31-52 from the current r, ending with an
+// asynchronous copy of the scalars to pinned host memory.  mode: 1 first
+// iteration, 0 reference beta, 2 flexible beta.
+int cg_iteration(tosp_handle *h, int mode) {
+    const int64_t nd = h->lev[0].g.ndof;
+    TRY(precondition(h, h->cr, h->cs));
+    launch_dot(h->cr, h->cs, nd, h->d_partials, h->d_scal + 0, h->stream);
+    if (mode == 2) launch_dot(h->cr, h->cso, nd, h->d_partials, h->d_scal + 5, h->stream);
+    launch_pcg_direction(h->cd, h->cs, h->mg.flexible ? h->cso : nullptr, h->d_scal, nd, mode, h->stream);
+    CKL();
+    TRY(fine_apply64(h, h->cd, h->cq));
+    launch_dot(h->cd, h->cq, nd, h->d_partials, h->d_scal + 2, h->stream);
+    launch_pcg_update(h->cx, h->cr, h->cd, h->cq, h->d_scal, h->d_partials, nd, h->stream);
+    CKL();
+    CK(cudaMemcpyAsync(h->h_scal, h->d_scal, sizeof(double) * 8, cudaMemcpyDeviceToHost, h->stream));
+    return TOSP_OK;
+}
+
+// Capture the generic iteration (it >= 2) into a CUDA graph: all buffers
+// are fixed per handle, so the graph is reused by every later solve.  On any
+// capture failure the solver keeps launching the same kernels one by one.
+void capture_iteration(tosp_handle *h) {
+    cudaGraph_t g = nullptr;
+    if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cudaGetLastError();
+        h->graph_failed = true;
+        return;
+    }
+    const int rc = cg_iteration(h, h->mg.flexible ? 2 : 0);
+    const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
+    if (rc != TOSP_OK || e != cudaSuccess || !g ||
+        cudaGraphInstantiate(&h->iter_graph, g, 0) != cudaSuccess) {
+        cudaGetLastError();
+        h->iter_graph = nullptr;
+        h->graph_failed = true;
+    }
+    if (g) cudaGraphDestroy(g);
+}
+
 int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
     const int64_t nd = h->lev[0].g.ndof;
     // r = f - K x
@@ -639,17 +682,17 @@ int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
     int it = 1;
     int rc = TOSP_OK;
     while (nr > h->mg.tolMG && it <= h->mg.maxiterMG) {
-        TRY(precondition(h, h->cr, h->cs));
-        launch_dot(h->cr, h->cs, nd, h->d_partials, h->d_scal + 0, h->stream);
-        const bool flex = h->mg.flexible && it > 1;
-        if (flex) launch_dot(h->cr, h->cso, nd, h->d_partials, h->d_scal + 5, h->stream);
-        launch_pcg_direction(h->cd, h->cs, h->d_scal, nd, it == 1 ? 1 : (flex ? 2 : 0), h->stream);
-        CKL();
-        TRY(fine_apply64(h, h->cd, h->cq));
-        launch_dot(h->cd, h->cq, nd, h->d_partials, h->d_scal + 2, h->stream);
-        launch_pcg_update(h->cx, h->cr, h->cd, h->cq, h->d_scal, h->d_partials, nd, h->stream);
-        CKL();
-        TRY(read_scalars(h));
+        if (it == 1) {
+            TRY(cg_iteration(h, 1));
+        } else {
+            if (!h->iter_graph && !h->graph_failed) capture_iteration(h);
+            if (h->iter_graph) {
+                CK(cudaGraphLaunch(h->iter_graph, h->stream));
+            } else {
+                TRY(cg_iteration(h, h->mg.flexible ? 2 : 0));
+            }
+        }
+        TRY(sync(h));
         const double dq = h->h_scal[2], rr = h->h_scal[3];
         if (!(dq > 0.0) || !std::isfinite(rr)) {
             h->err = "CG breakdown: d'q = " + std::to_string(dq) + ", r'r = " + std::to_string(rr);
@@ -658,7 +701,6 @@ int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
         }
         nr = std::sqrt(rr) / nf;
         ++it;
-        if (h->mg.flexible) std::swap(h->cs, h->cso);
     }
     if (rc == TOSP_OK && nr > h->mg.tolMG && it > h->mg.maxiterMG) rc = TOSP_NOT_CONVERGED;
     if (it_out) *it_out = it;
@@ -738,6 +780,7 @@ int tosp_create(const tosp_problem *prob, const tosp_mg_params *mg, int32_t prec
 int tosp_destroy(tosp_handle *h) {
     if (!h) return TOSP_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->iter_graph) cudaGraphExecDestroy(h->iter_graph);
     for (void *p : h->allocs) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
     if (h->ev0) cudaEventDestroy(h->ev0);

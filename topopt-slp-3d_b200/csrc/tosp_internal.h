@@ -44,6 +44,31 @@ constexpr int NBX = BX + 1, NBY = BY + 1, NBZ = BZ + 1;
 constexpr int BRICK_NODES = NBX * NBY * NBZ;         // 225
 constexpr int KE_PACK = 300;                          // upper triangle of a 24x24 block
 
+// Order of the 300 upper-triangle entries (i <= j) in the fine operator's
+// block layout: diagonal by diagonal (d = j - i = 0..23), and within a
+// diagonal even i first, then odd i, so that consecutive entries never update
+// the same output (the updates y_i += k u_j, y_j += k u_i are dependent
+// through y otherwise).
+__host__ __device__ constexpr int pair_d(int t) {
+    int d = 0;
+    while (t >= 24 - d) {
+        t -= 24 - d;
+        ++d;
+    }
+    return d;
+}
+__host__ __device__ constexpr int pair_i(int t) {
+    const int d = pair_d(t);
+    int r = t;
+    for (int e = 0; e < d; ++e) r -= 24 - e;
+    const int neven = (24 - d + 1) / 2;
+    return r < neven ? 2 * r : 2 * (r - neven) + 1;
+}
+__host__ __device__ constexpr int pair_j(int t) { return pair_i(t) + pair_d(t); }
+__host__ __device__ constexpr int pair_index_diag(int i) { return (i % 2 == 0) ? i / 2 : 12 + i / 2; }
+// Row-major packed index of (i, j), i <= j (Galerkin build, Grad).
+__host__ __device__ constexpr int pair_rowmajor(int i, int j) { return i * 24 - i * (i - 1) / 2 + (j - i); }
+
 struct FineGeom {
     Grid g;
     int nelx_d, nely_d;        // density mesh (n x finer)
@@ -145,7 +170,7 @@ void launch_convert(const TI *a, TO *b, int64_t n, cudaStream_t st);
 constexpr int RED_BLOCKS = 592;
 void launch_dot(const double *a, const double *b, int64_t n, double *partials, double *out, cudaStream_t st);
 // PCG pieces (scalars in device memory, see solver.cpp for the slots).
-void launch_pcg_direction(double *d, const double *s, const double *scal, int64_t n, int mode,
+void launch_pcg_direction(double *d, const double *s, double *sold, const double *scal, int64_t n, int mode,
                           cudaStream_t st);
 void launch_pcg_update(double *x, double *r, const double *d, const double *q, double *scal, double *partials,
                        int64_t n, cudaStream_t st);
