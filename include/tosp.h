@@ -190,6 +190,50 @@ int tosp_time_operator(tosp_handle *h, int32_t precision, int32_t reps, double *
  * the array: calls whose GPU work overlaps race. */
 int tosp_kelem_prod_noalloc(tosp_handle *h, const double *x, double *y, int64_t nfree);
 
+/* ---- serving loop ------------------------------------------------------
+ * A server runs many independent SetupGMG + SolveMG (zero start) + Grad
+ * requests on the current device.  No counterpart in the reference (which
+ * solves one problem per MATLAB process): requests are admitted in arrival
+ * order as soon as one of `max_slots` slots is free and the request's
+ * estimated device memory fits `hbm_budget_bytes`; each slot drives a solve
+ * handle on its own CUDA stream, so concurrent requests overlap on the GPU;
+ * handles are cached per problem shape and reused. */
+typedef struct tosp_server tosp_server;
+
+#define TOSP_REQ_QUEUED     0
+#define TOSP_REQ_RUNNING    1
+#define TOSP_REQ_DONE       2
+#define TOSP_REQ_FAILED     3
+#define TOSP_REQ_CANCELLED  4
+
+typedef struct tosp_request_stats {
+    int32_t it;            /* the reference's `it` of the solve                    */
+    double  relres;        /* final relative residual                              */
+    double  ms_latency;    /* submit -> results ready (host clock)                 */
+    double  ms_queue;      /* time spent waiting for a slot / memory                */
+    double  ms_run;        /* setup + solve + Grad                                 */
+} tosp_request_stats;
+
+int tosp_server_create(int32_t max_slots, int64_t hbm_budget_bytes, tosp_server **out);
+/* Copies the problem arrays, densities `xfil` (density mesh) and load `f`
+ * (free dofs); TOSP_ERR_OOM if the request can never fit the budget. */
+int tosp_server_submit(tosp_server *s, const tosp_problem *prob, const tosp_mg_params *mg, int32_t precision,
+                       const double *xfil, int64_t ndens, const double *f, int64_t nfree, int64_t *request_id);
+int tosp_server_poll(tosp_server *s, int64_t request_id, int32_t *state);
+/* Block until the request is done/failed/cancelled (TOSP_ERR_TIMEOUT otherwise). */
+int tosp_server_wait(tosp_server *s, int64_t request_id, double timeout_s);
+/* Copy results: u on the free dofs, the filtered sensitivities; returns the
+ * solve status (TOSP_OK / TOSP_NOT_CONVERGED / an error). */
+int tosp_server_result(tosp_server *s, int64_t request_id, double *u, int64_t nfree, double *fgrad, int64_t ndens,
+                       tosp_request_stats *st);
+/* Cancel a queued request (running requests complete). */
+int tosp_server_cancel(tosp_server *s, int64_t request_id);
+/* Forget a finished request and its results. */
+int tosp_server_release(tosp_server *s, int64_t request_id);
+int tosp_server_info(tosp_server *s, int32_t *active, int32_t *queued, int64_t *used_bytes, int64_t *cached_handles);
+/* Cancels queued requests, waits for running ones, frees every handle. */
+int tosp_server_destroy(tosp_server *s);
+
 /* Host-only: the n^3 sub-element stiffness blocks kv (576 x n^3, column s is
  * k{s}(:), column-major) of I/ElemStiffMatrixGQMR.m:1 for hex8 elements. */
 int tosp_elem_stiff_mr(double el, double eh, double ew, double nu, int32_t n, double *kv);

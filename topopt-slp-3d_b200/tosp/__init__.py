@@ -52,6 +52,11 @@ class MgParams(C.Structure):
                 ("maxiterMG", C.c_int32), ("nmaxchol", C.c_int32), ("flexible", C.c_int32)]
 
 
+class RequestStats(C.Structure):
+    _fields_ = [("it", C.c_int32), ("relres", C.c_double), ("ms_latency", C.c_double), ("ms_queue", C.c_double),
+                ("ms_run", C.c_double)]
+
+
 class SolveStats(C.Structure):
     _fields_ = [("it", C.c_int32), ("relres", C.c_double), ("ms_setup", C.c_double), ("ms_solve", C.c_double)]
 
@@ -84,6 +89,16 @@ def _load():
         "tosp_kernel_launches": (C.c_int64, []),
         "tosp_time_operator": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, P(C.c_double)]),
         "tosp_kelem_prod_noalloc": (C.c_int, [C.c_void_p, d, d, C.c_int64]),
+        "tosp_server_create": (C.c_int, [C.c_int32, C.c_int64, P(C.c_void_p)]),
+        "tosp_server_submit": (C.c_int, [C.c_void_p, P(_Problem), P(MgParams), C.c_int32, d, C.c_int64, d, C.c_int64,
+                                         P(C.c_int64)]),
+        "tosp_server_poll": (C.c_int, [C.c_void_p, C.c_int64, P(C.c_int32)]),
+        "tosp_server_wait": (C.c_int, [C.c_void_p, C.c_int64, C.c_double]),
+        "tosp_server_result": (C.c_int, [C.c_void_p, C.c_int64, d, C.c_int64, d, C.c_int64, P(RequestStats)]),
+        "tosp_server_cancel": (C.c_int, [C.c_void_p, C.c_int64]),
+        "tosp_server_release": (C.c_int, [C.c_void_p, C.c_int64]),
+        "tosp_server_info": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32), P(C.c_int64), P(C.c_int64)]),
+        "tosp_server_destroy": (C.c_int, [C.c_void_p]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -272,3 +287,93 @@ class Solver:
         fd1, fdp = _i64(np.asarray(freedofs) + 1)
         self._check(_lib.tosp_set_freedofs(self.h, fdp, fd1.size))
         self.nfree = fd1.size
+
+
+def _problem_struct(pb, mr_n, p, emin, opfilter, rmin, fixed_dens=None, free_dens_g=None):
+    """tosp_problem for `pb` plus the arrays it points to (keep them alive)."""
+    keep = []
+    fd1, fdp = _i64(np.asarray(pb.freedofs) + 1)
+    keep.append(fd1)
+    prob = _Problem(pb.nelx, pb.nely, pb.nelz, pb.el, pb.eh, pb.ew, pb.E, pb.nu, p, emin, mr_n, opfilter, rmin,
+                    fdp, fd1.size, None, 0, None, 0)
+    if fixed_dens is not None and len(fixed_dens):
+        fx1, fxp = _i64(np.asarray(fixed_dens) + 1)
+        keep.append(fx1)
+        prob.fixed_dens, prob.nfixed_dens = fxp, fx1.size
+    if free_dens_g is not None:
+        fg1, fgp = _i64(np.asarray(free_dens_g) + 1)
+        keep.append(fg1)
+        prob.free_dens_g, prob.nfree_dens_g = fgp, fg1.size
+    return prob, keep
+
+
+class Server:
+    """The serving loop of tosp.h: admission by slots and HBM budget,
+    concurrent requests on their own streams, handles cached per shape."""
+
+    def __init__(self, max_slots=4, hbm_budget_bytes=64 << 30):
+        h = C.c_void_p()
+        rc = _lib.tosp_server_create(max_slots, int(hbm_budget_bytes), C.byref(h))
+        if rc != TOSP_OK:
+            raise TospError(rc, "tosp_server_create")
+        self.h = h
+        self.meta = {}
+
+    def submit(self, pb, xfil, f=None, mg=None, precision=PREC_MIXED, mr_n=1, p=3.0, emin=1e-9, opfilter=1,
+               rmin=1.5):
+        mg = mg if mg is not None else default_mg()
+        prob, keep = _problem_struct(pb, mr_n, p, emin, opfilter, rmin)
+        xfil = np.ascontiguousarray(xfil, dtype=np.float64)
+        f = np.ascontiguousarray(pb.f if f is None else f, dtype=np.float64)
+        rid = C.c_int64()
+        rc = _lib.tosp_server_submit(self.h, C.byref(prob), C.byref(mg), precision, xfil.ctypes.data, xfil.size,
+                                     f.ctypes.data, f.size, C.byref(rid))
+        if rc != TOSP_OK:
+            raise TospError(rc, "tosp_server_submit")
+        self.meta[rid.value] = (f.size, xfil.size)
+        return rid.value
+
+    def state(self, rid):
+        st = C.c_int32()
+        rc = _lib.tosp_server_poll(self.h, rid, C.byref(st))
+        if rc != TOSP_OK:
+            raise TospError(rc, "tosp_server_poll")
+        return st.value
+
+    def wait(self, rid, timeout=600.0):
+        rc = _lib.tosp_server_wait(self.h, rid, timeout)
+        if rc != TOSP_OK:
+            raise TospError(rc, "tosp_server_wait")
+
+    def result(self, rid, release=True):
+        nfree, ndens = self.meta[rid]
+        u = np.empty(nfree)
+        g = np.empty(ndens)
+        st = RequestStats()
+        rc = _lib.tosp_server_result(self.h, rid, u.ctypes.data, nfree, g.ctypes.data, ndens, C.byref(st))
+        if rc < 0:
+            raise TospError(rc, "request failed")
+        if release:
+            _lib.tosp_server_release(self.h, rid)
+            self.meta.pop(rid, None)
+        return u, g, {"it": st.it, "relres": st.relres, "ms_latency": st.ms_latency, "ms_queue": st.ms_queue,
+                      "ms_run": st.ms_run, "status": rc}
+
+    def cancel(self, rid):
+        return _lib.tosp_server_cancel(self.h, rid)
+
+    def info(self):
+        a, q, b, c = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int64()
+        _lib.tosp_server_info(self.h, C.byref(a), C.byref(q), C.byref(b), C.byref(c))
+        return {"active": a.value, "queued": q.value, "used_bytes": b.value, "cached_handles": c.value}
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.tosp_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

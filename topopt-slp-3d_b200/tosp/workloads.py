@@ -67,3 +67,63 @@ def build_workload(name, filter_fn=None):
     else:
         xfil = np.full(nd, 0.3)
     return pb, n, xfil, spec
+
+
+# ---------------------------------------------------------------------------
+# Serving stream: seed-7 requests with Poisson arrivals.
+# ---------------------------------------------------------------------------
+SERVING_NX = (32, 64, 96, 128)
+SERVING_BC = ("cantilever", "bridge", "torsion")
+
+
+def serving_levels(nx):
+    """Grids for an nx x nx/2 x nx/2 mesh: coarsest grid of 8 (or 12) x 4 x 4
+    elements, within the reference's level rule."""
+    ng = 1
+    while nx // (2 ** ng) >= 8 and (nx // 2) % (2 ** ng) == 0:
+        ng += 1
+    return ng
+
+
+def serving_requests(count=512, seed=7, pool=3):
+    """Request descriptors: (nx, n, bc, field index, eta).  Density fields are
+    drawn from a small pool of seeded Gaussian random fields per shape (each
+    request shifts the Heaviside threshold), so generating the stream stays
+    cheap."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        nx = int(rng.choice(SERVING_NX))
+        n = int(rng.choice((1, 2)))
+        bc = str(rng.choice(SERVING_BC))
+        out.append((nx, n, bc, int(rng.integers(pool)), float(rng.uniform(0.4, 0.6))))
+    return out
+
+
+def serving_problem(nx, bc):
+    builder = {"cantilever": problems.cantilever, "bridge": problems.bridge, "torsion": problems.torsion}[bc]
+    return builder(nx, nx // 2, nx // 2)
+
+
+class FieldPool:
+    """Seeded GRF fields per (nx, n, index), generated on first use."""
+
+    def __init__(self, seed=7):
+        self.seed = seed
+        self.cache = {}
+
+    def field(self, nx, n, idx, eta):
+        key = (nx, n, idx)
+        if key not in self.cache:
+            from scipy.special import ndtr
+            rng = np.random.default_rng((self.seed, nx, n, idx))
+            shape = (nx // 2 * n, nx * n, nx // 2 * n)     # (z, x, y) of the density mesh
+            noise = rng.standard_normal(shape)
+            F = np.fft.rfftn(noise)
+            kz = np.fft.fftfreq(shape[0])[:, None, None]
+            kx = np.fft.fftfreq(shape[1])[None, :, None]
+            ky = np.fft.rfftfreq(shape[2])[None, None, :]
+            F *= np.exp(-2.0 * (math.pi * 4.0 * n) ** 2 * (kx ** 2 + ky ** 2 + kz ** 2))
+            fld = np.fft.irfftn(F, s=shape)
+            self.cache[key] = ndtr((fld - fld.mean()) / fld.std()).ravel()
+        return 0.001 + 0.999 * heaviside(self.cache[key], 4.0, eta)
