@@ -178,6 +178,111 @@ def cpu_baseline(args, pb, n, xfil, spec, it_fp64):
                        f"{t3 - t0:.1f} s timed; full solve projected as setup + {it_fp64} x iteration + Grad")}
 
 
+class _Timed:
+    """Wraps a solve path and accumulates wall time per entry point (each
+    call is synchronous)."""
+
+    def __init__(self, inner):
+        self.inner = inner
+        self.t = {"filter": 0.0, "setup": 0.0, "solve": 0.0, "grad": 0.0}
+
+    def _run(self, key, fn, *a, **k):
+        t0 = time.perf_counter()
+        out = fn(*a, **k)
+        self.t[key] += time.perf_counter() - t0
+        return out
+
+    def ApplyFilter(self, x, trans=False):
+        return self._run("filter", self.inner.ApplyFilter, x, trans=trans)
+
+    def SetupGMG(self, x):
+        return self._run("setup", self.inner.SetupGMG, x)
+
+    def SolveMG(self, x, f):
+        return self._run("solve", self.inner.SolveMG, x, f)
+
+    def Grad(self, u):
+        return self._run("grad", self.inner.Grad, u)
+
+
+def run_slp(args):
+    """Full SLP loop (host LP) on the GPU solve path: config 0 (FP64) or
+    config 3 (mixed precision, MR factor 3, GradProj at the end)."""
+    import torch
+    import tosp
+    from tosp import problems as P
+    from tosp import slp
+    torch.cuda.set_device(0)
+    if args.slp == "config0":
+        pb = P.cantilever(48, 24, 24)
+        n, prec, ngr, rmin, volfrac, iters, lp = 1, tosp.PREC_FP64, 3, 1.5, 0.3, 20, "highs"
+        prj = slp.PrjParams(op=False)
+    else:
+        pb = P.bridge(160, 80, 40)
+        n, prec, ngr, rmin, volfrac, iters, lp = 3, tosp.PREC_MIXED, 4, 2.5 / 3, 0.2, 100, "knapsack"
+        prj = slp.PrjParams(op=True)
+    iters = args.slp_iters or iters
+    mg = tosp.default_mg(ngrids=ngr, cycle=0, omega=0.6, smoothiter1=1, smoothiter2=1, tolMG=1e-8, maxiterMG=2000,
+                         flexible=1 if prec == tosp.PREC_MIXED else 0)
+    solver = tosp.Solver(pb, mg, precision=prec, mr_n=n, p=3.0, emin=1e-9, opfilter=1, rmin=rmin)
+    timed = _Timed(solver)
+    x0 = np.full(pb.nelem * n ** 3, volfrac)
+    per_it = []
+    last = [time.perf_counter()]
+
+    def on_iter(h):
+        now = time.perf_counter()
+        per_it.append(now - last[0])
+        last[0] = now
+    t0 = time.perf_counter()
+    res = slp.str_slp(timed, pb, volfrac, x0, slp.SlpParams(maxiter=iters, lp=lp), prj=prj, on_iter=on_iter)
+    wall = time.perf_counter() - t0
+    steps = len(res.history)
+    line = {"metric": f"SLP loop ({args.slp}): seconds per SLP iteration", "value": round(wall / max(steps, 1), 4),
+            "unit": "s/iteration", "higher_is_better": False, "n_gpus": 1, "data": "synthetic",
+            "dtype": "f64" if prec == tosp.PREC_FP64 else "f64 outer CG / f32+bf16 V-cycle",
+            "config": {"workload": args.slp, "mesh": [pb.nelx, pb.nely, pb.nelz], "mr_n": n, "volfrac": volfrac,
+                       "rmin": rmin, "lp": lp, "ngrids": ngr},
+            "slp": {"accepted": res.iters, "rejected": res.rejected, "opstop": res.opstop, "F_final": res.F,
+                    "F_first": res.history[0]["F"] if res.history else None,
+                    "pcg_iterations_total": int(sum(res.pcgit)), "wall_s": round(wall, 3)},
+            "time_s": {k: round(v, 3) for k, v in timed.t.items()},
+            "time_per_iteration_s": {k: round(v / max(steps, 1), 4) for k, v in timed.t.items()}}
+    if prj.op:
+        line["slp"]["volume_rounded"] = float(res.xstar.mean())
+        line["slp"]["rounded_fraction_0_1"] = float(np.mean((res.xstar == 0) | (res.xstar == 1)))
+    if args.slp == "config3":
+        # final displacement checked with the CPU restatement of KelemProd
+        from oracle.cpu_wok import CpuWok
+        cw = CpuWok(pb, n, ngr, 0.6, nthreads=os.cpu_count())
+        xf_final = solver.ApplyFilter(res.x)
+        solver.SetupGMG(xf_final)
+        u_final = solver.SolveMG(res.u, pb.f)[0]
+        res.u = u_final
+        cw.w = np.ascontiguousarray(1e-9 + (1 - 1e-9) * np.power(xf_final, 3))
+        uf = np.zeros(3 * pb.nnodes)
+        uf[pb.freedofs] = u_final
+        r = pb.f_full() - cw.kelem(uf)
+        line["cpu_check"] = {"relres_cpu_operator": float(np.linalg.norm(r[pb.freedofs]) / np.linalg.norm(pb.f)),
+                             "compliance": float(pb.f @ res.u)}
+    if args.check_cpu and args.slp == "config0":
+        sys.path.insert(0, os.path.join(ROOT, "tests"))
+        from oracle_solver import OracleSolver
+        orc = OracleSolver(pb, n=n, ngrids=ngr, cycle=0, omega=0.6, rmin=rmin)
+        t1 = time.perf_counter()
+        ro = slp.str_slp(orc, pb, volfrac, x0, slp.SlpParams(maxiter=iters, lp=lp), prj=prj)
+        tcpu = time.perf_counter() - t1
+        line["cpu_baseline"] = {"value": round(tcpu / max(len(ro.history), 1), 4), "unit": "s/iteration",
+                                "cores": os.cpu_count(), "kind": "port",
+                                "sample": f"the same {iters}-iteration SLP loop on the NumPy/SciPy oracle "
+                                          "(assembled K, SetupGMG, SolveMG, Grad)"}
+        line["parity"] = {"F_rel_diff": abs(ro.F - res.F) / abs(ro.F),
+                          "design_max_abs_diff": float(np.abs(ro.x - res.x).max()),
+                          "same_accept_reject": [h["it"] for h in ro.history] == [h["it"] for h in res.history]}
+    print(json.dumps(line))
+    return 0
+
+
 def run_serving(args):
     """Serving stream: 512 seeded requests (mesh nx x nx/2 x nx/2, nx in
     {32, 64, 96, 128}, MR factor 1 or 2, cantilever/bridge/torsion, GRF
@@ -279,6 +384,11 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--ngrids", type=int, default=0, help="override the workload's grid count")
     ap.add_argument("--flexible", type=int, default=1, help="flexible (Polak-Ribiere) CG beta in both arms")
+    ap.add_argument("--slp", default="", choices=["", "config0", "config3"],
+                    help="full SLP loop: config0 = 48x24x24 cantilever, FP64, 20 iterations; config3 = 160x80x40 "
+                         "bridge (reference axes), MR 3, mixed precision, 100 iterations + GradProj")
+    ap.add_argument("--slp-iters", type=int, default=0)
+    ap.add_argument("--check-cpu", action="store_true", help="config0: run the same SLP loop on the oracle")
     ap.add_argument("--serving", action="store_true",
                     help="serving stream (seed 7): Poisson arrivals at --rates, p50/p99 latency and solves/s")
     ap.add_argument("--rates", default="10,20,50,100,200,500")
@@ -296,6 +406,8 @@ def main():
         return profile_kernels(args)
     if args.serving:
         return run_serving(args)
+    if args.slp:
+        return run_slp(args)
 
     import torch
     import torch.distributed as dist

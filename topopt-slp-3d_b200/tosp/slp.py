@@ -1,0 +1,309 @@
+"""Sequential linear programming driver (host) on top of the GPU solve path.
+
+Restates the trust-region SLP loop of ``I/StrSLP.m:46-560`` (``I/`` =
+``Implementation/``) for the configuration the solve path serves
+(matrix-free geometric MG, ``mr.n = mr.d``, ``elem.fix = 0``): per step it
+solves the LP subproblem on the host, filters the new design, rebuilds K(rho)
+and the hierarchy, solves K u = f with the previous u as warm start
+(``pcgp.opu0``), and on acceptance recomputes the sensitivities.  The final
+optional rounding is ``GradProj`` (``I/GradProj.m``).
+
+The solve path is any object with ``ApplyFilter(x, trans)``, ``SetupGMG(xfil)``,
+``SolveMG(x0, f) -> (u, it, relres, status)`` and ``Grad(u_full)`` -
+:class:`tosp.Solver` on the GPU.
+
+LP solvers: ``"highs"`` - ``scipy.optimize.linprog(method="highs-ds")``, the
+dual simplex like the reference's ``linprog`` (``I/StrSLP.m:239-245,267-290``);
+``"knapsack"`` - the exact solution of this LP (one inequality with positive
+coefficients plus bounds) by sorting the cost/coefficient ratios, O(N log N).
+"""
+from dataclasses import dataclass, field
+
+import numpy as np
+
+
+@dataclass
+class SlpParams:
+    """``slp.*`` of I/TopOpt3D.m:61-72."""
+    tolS: float = 1e-4
+    tolG: float = 1e-3
+    tolF: float = 5e-2
+    maxcount: int = 3
+    maxiter: int = 500
+    delta0: float = 0.1
+    eta: float = 0.1
+    rho: float = 0.5
+    alphaR: float = 0.25
+    alphaA: float = 2.0
+    lp: str = "highs"
+
+
+@dataclass
+class PrjParams:
+    """``prj.*`` of I/TopOpt3D.m:73-92 used by GradProj."""
+    op: bool = False
+    nearlim: bool = True
+    maxang: float = 89.9
+    gthresh: float = 1e-4
+    ut: float = 0.95
+    lt: float = 0.05
+    vumin: float = 0.7
+    vlmax: float = 0.3
+
+
+@dataclass
+class SlpResult:
+    xstar: np.ndarray
+    x: np.ndarray
+    u: np.ndarray
+    F: float
+    iters: int
+    rejected: int
+    opstop: int
+    pcgit: list = field(default_factory=list)
+    history: list = field(default_factory=list)
+
+
+def lp_knapsack(g, a, c, lo, hi):
+    """min g's  s.t.  a's <= c, lo <= s <= hi  with a > 0.
+
+    Returns (s, fval, lam, ok): start from the unconstrained minimiser
+    (hi where g < 0, lo elsewhere); if a's > c, lower the variables that cost
+    least per unit of constraint (smallest |g|/a among g < 0) until a's = c.
+    lam is the multiplier of the inequality (>= 0, MATLAB's lambda.ineqlin).
+    """
+    s = np.where(g < 0, hi, lo).astype(np.float64)
+    excess = a @ s - c
+    if excess <= 0:
+        return s, float(g @ s), 0.0, True
+    cand = np.nonzero((g < 0) & (hi > lo))[0]
+    ratio = -g[cand] / a[cand]
+    order = cand[np.argsort(ratio, kind="stable")]
+    red = a[order] * (hi[order] - lo[order])        # constraint reduction if moved fully to lo
+    cum = np.cumsum(red)
+    k = int(np.searchsorted(cum, excess))
+    if k >= order.size:
+        return None, None, None, False                # infeasible within the box
+    s[order[:k]] = lo[order[:k]]
+    prev = cum[k - 1] if k > 0 else 0.0
+    j = order[k]
+    s[j] = hi[j] - (excess - prev) / a[j]
+    lam = float(-g[j] / a[j])
+    return s, float(g @ s), lam, True
+
+
+def lp_highs(g, a, c, lo, hi):
+    from scipy.optimize import linprog
+    res = linprog(g, A_ub=a[None, :], b_ub=[c], bounds=np.stack([lo, hi], axis=1), method="highs-ds")
+    if res.status != 0:
+        return None, None, None, False, 0
+    lam = float(-res.ineqlin.marginals[0]) if res.ineqlin is not None else 0.0
+    return res.x, float(res.fun), lam, True, int(res.nit)
+
+
+def grad_proj(x, g, prj, Vmax, velem):
+    """Rounding of the densities to 0/1 along -grad(Lag) (I/GradProj.m:1-124)."""
+    g = -np.asarray(g, dtype=np.float64)
+    gnorm = np.linalg.norm(g)
+    coslim = np.cos(np.deg2rad(prj.maxang))
+    gt = prj.gthresh * np.abs(g).max()
+    volfrac = (velem @ x) / velem.sum()
+    xtop = np.nonzero(x >= prj.ut)[0]
+    ntop = xtop.size
+    done = int(np.round(Vmax / velem[0]))
+    nup = done - ntop
+    xnew = np.zeros(x.size)
+    if nup <= 0:
+        su = np.argsort(-x[xtop], kind="stable")
+        xnew[xtop[su[:done]]] = 1.0
+        return xnew
+    xnew[xtop] = 1.0
+    xvar = np.nonzero((x > prj.lt) & (x < prj.ut))[0]
+    nvar = xvar.size
+    if nvar == 0:
+        return xnew
+    dvol = min(nvar, nup, int(np.round(volfrac * x.size)) - ntop)
+
+    def cos_of(xn):
+        d = xn - x
+        nd = np.linalg.norm(d)
+        return (d @ g) / (gnorm * nd) if nd > 0 else -1.0
+
+    if prj.nearlim:
+        ivol = np.argsort(-x[xvar], kind="stable")
+        xnew[xvar[ivol[:max(dvol, 0)]]] = 1.0
+        cosang = cos_of(xnew)
+    else:
+        cosang = -1.0
+    if cosang < coslim:
+        gv = g[xvar].copy()
+        iup = np.nonzero(gv > 0.0)[0]
+        iup2 = np.nonzero((gv == 0.0) & (x[xvar] >= prj.vumin))[0]
+        g[xvar[iup2]] = 1e16
+        gv = g[xvar]
+        iup = np.concatenate([iup, iup2])
+        niup = iup.size
+        idown = np.nonzero(gv < -gt)[0]
+        nidown = idown.size
+        alphau = (1 - x[xvar[iup]]) / gv[iup]
+        alphad = -x[xvar[idown]] / gv[idown]
+        su = np.argsort(alphau, kind="stable")
+        sd = np.argsort(alphad, kind="stable")
+        alphau, alphad = alphau[su], alphad[sd]
+        xup = x[xvar[iup[su]]]
+        xdown = x[xvar[idown[sd]]]
+        ku = np.nonzero(xup < prj.vumin)[0]
+        kup = niup if ku.size == 0 else int(ku[0])
+        kd = np.nonzero(xdown > prj.vlmax)[0]
+        kdown = nidown if kd.size == 0 else int(kd[0])
+        if niup == 0:
+            if nidown == 0:
+                return xnew
+            alpha = alphad[:kdown]
+        else:
+            imax = min(dvol, kup)
+            if nidown == 0:
+                alpha = alphau[:imax]
+            elif imax == 0:
+                alpha = alphad[:kdown]
+            else:
+                i2 = np.nonzero(alphad > alphau[imax - 1])[0]
+                imax2 = kdown if i2.size == 0 else min(kdown, int(i2[0]))
+                alpha = np.sort(np.concatenate([alphau[:imax], alphad[:imax2]]))
+        pos = alpha.size - 1
+        while pos >= 0 and cosang < coslim:
+            xnew[xvar] = np.maximum(0.0, np.minimum(1.0, x[xvar] + alpha[pos] * g[xvar]))
+            cosang = cos_of(xnew)
+            pos -= 1
+        if cosang < coslim:
+            xnew[xvar] = x[xvar]
+    return xnew
+
+
+def str_slp(solver, pb, volfrac, x0, slp=None, prj=None, fixed=None, on_iter=None):
+    """Trust-region SLP of I/StrSLP.m with ``volineq = true`` and MG solves.
+
+    ``solver``: the solve path (see the module docstring); ``pb`` the problem
+    (free dofs and loads); ``x0`` the initial design variables on the
+    density (= design) mesh; ``fixed``: 0-based fixed design variables.
+    """
+    slp = slp or SlpParams()
+    prj = prj or PrjParams()
+    x = np.asarray(x0, dtype=np.float64).copy()
+    nelem = x.size
+    V = pb.l * pb.h * pb.w
+    velem = np.full(nelem, V / nelem)
+    Vmax = volfrac * V
+    fixed = np.zeros(0, dtype=np.int64) if fixed is None else np.asarray(fixed, dtype=np.int64)
+    free = np.setdiff1d(np.arange(nelem), fixed)
+    theta1 = theta2 = thetaMax = 1.0
+    countS = countG = countF = 0
+    it_acc = itrej = 0
+    delta = slp.delta0
+    res = SlpResult(None, None, None, 0.0, 0, 0, 2)
+
+    xfil = solver.ApplyFilter(x)
+    solver.SetupGMG(xfil)
+    u, pit, _, _ = solver.SolveMG(np.zeros(pb.f.size), pb.f)
+    res.pcgit.append(pit)
+    Fold = float(pb.f @ u)
+    F = Fold
+    ufull = np.zeros(3 * pb.nnodes)
+    ufull[pb.freedofs] = u
+    Fgrad = solver.Grad(ufull)
+    A = solver.ApplyFilter(velem, trans=True) / Vmax          # I/StrSLP.m:222-228
+    b = (velem @ xfil - Vmax) / Vmax
+    sL = np.maximum(-delta, -x)
+    sU = np.minimum(delta, 1 - x)
+    sL[fixed] = 0.0
+    sU[fixed] = 0.0
+    lam = 0.0
+    gp = np.minimum(1, np.maximum(0.0, x[free] - Fgrad[free])) - x[free]
+    gpnorm = np.abs(gp).max() if gp.size else 0.0
+    if gpnorm < 1e-12 and b < 1e-12 and (x - 1.0).max() < 1e-12 and x.min() > -1e-12:
+        countG = countF = slp.maxcount
+
+    while (countG < slp.maxcount or countF < slp.maxcount) and countS < slp.maxcount and it_acc < slp.maxiter:
+        if slp.lp == "knapsack":
+            s, fval, lam_new, ok = lp_knapsack(Fgrad, A, -b, sL, sU)
+            nit = 1
+        else:
+            s, fval, lam_new, ok, nit = lp_highs(Fgrad, A, -b, sL, sU)
+        if not ok:
+            # infeasible step box: minimise the infeasibility (I/StrSLP.m:272-286)
+            from scipy.optimize import linprog
+            A2 = np.concatenate([A, [-1.0, 1.0]])
+            c2 = np.concatenate([np.zeros(nelem), [1.0, 1.0]])
+            lo2 = np.concatenate([np.maximum(-0.8 * delta, -x), [0.0, 0.0]])
+            hi2 = np.concatenate([np.minimum(0.8 * delta, 1 - x), [np.inf, np.inf]])
+            lo2[fixed] = 0.0
+            hi2[fixed] = 0.0
+            r2 = linprog(c2, A_ub=A2[None, :], b_ub=[-b], bounds=np.stack([lo2, hi2], axis=1), method="highs-ds")
+            s = r2.x[:nelem]
+            fval = float(Fgrad @ s)
+            lam_new = float(-r2.ineqlin.marginals[0])
+        elif nit == 0:
+            s = np.zeros(nelem)
+        lam = lam_new
+        snorm = np.abs(s).max()
+        xold, bold, deltaold = x, b, delta
+        x = x + s
+        xfil = solver.ApplyFilter(x)
+        b = (velem @ xfil - Vmax) / Vmax
+        solver.SetupGMG(xfil)
+        u, pit, _, _ = solver.SolveMG(u, pb.f)                # warm start, pcgp.opu0
+        res.pcgit.append(pit)
+        F = float(pb.f @ u)
+        predopt = -fval
+        predfsb = abs(bold) - abs(A @ s + bold)
+        aredopt = Fold - F
+        aredfsb = abs(bold) - abs(b)
+        thetaMin = min(theta1, theta2)
+        thetaLarge = (1 + 1e6 / ((it_acc + 1) ** 1.1)) * thetaMin
+        thetaSup = 1.0 if predopt > 0.5 * predfsb else (0.5 * predfsb) / (predfsb - predopt)
+        theta = min(thetaLarge, thetaSup, thetaMax)
+        theta2, theta1 = theta1, theta
+        pred = theta * predopt + (1 - theta) * predfsb
+        ared = theta * aredopt + (1 - theta) * aredfsb
+        if ared < slp.eta * pred:                               # rejected
+            itrej += 1
+            delta = max(slp.alphaR * snorm, 0.1 * deltaold)
+            thetaMax = theta
+            x, b, F = xold, bold, Fold
+        else:                                                   # accepted
+            if ared >= slp.rho * pred:
+                delta = min(slp.alphaA * deltaold, 1.0)
+            delta = max(delta, 0.0001)
+            thetaMax = 1.0
+            Fold = F
+            ufull = np.zeros(3 * pb.nnodes)
+            ufull[pb.freedofs] = u
+            Fgrad = solver.Grad(ufull)
+            Lgrad = Fgrad[free] + lam * A[free]
+            gp = np.minimum(1, np.maximum(0.0, x[free] - Lgrad)) - x[free]
+            gpnorm = np.abs(gp).max() if gp.size else 0.0
+            it_acc += 1
+            countG = countG + 1 if gpnorm <= slp.tolG else 0
+            countF = countF + 1 if ared <= slp.tolF else 0
+        countS = countS + 1 if snorm <= slp.tolS else 0
+        sL = np.maximum(-delta, -x)
+        sU = np.minimum(delta, 1 - x)
+        sL[fixed] = 0.0
+        sU[fixed] = 0.0
+        res.history.append({"it": it_acc, "F": F, "ared": ared, "pred": pred, "snorm": snorm, "delta": deltaold,
+                            "gpnorm": gpnorm, "pcgit": pit})
+        if on_iter:
+            on_iter(res.history[-1])
+
+    if countG >= slp.maxcount and countF >= slp.maxcount:
+        res.opstop = 0
+    elif countS >= slp.maxcount:
+        res.opstop = 1
+    else:
+        res.opstop = 2
+    if prj.op:
+        res.xstar = grad_proj(xfil, Fgrad + lam * A, prj, Vmax, velem)
+    else:
+        res.xstar = xfil
+    res.x, res.u, res.F, res.iters, res.rejected = x, u, F, it_acc, itrej
+    return res

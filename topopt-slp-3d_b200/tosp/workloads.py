@@ -124,6 +124,6 @@ class FieldPool:
             kx = np.fft.fftfreq(shape[1])[None, :, None]
             ky = np.fft.rfftfreq(shape[2])[None, None, :]
             F *= np.exp(-2.0 * (math.pi * 4.0 * n) ** 2 * (kx ** 2 + ky ** 2 + kz ** 2))
-            fld = np.fft.irfftn(F, s=shape)
+            fld = np.fft.irfftn(F, s=shape, axes=(0, 1, 2))
             self.cache[key] = ndtr((fld - fld.mean()) / fld.std()).ravel()
         return 0.001 + 0.999 * heaviside(self.cache[key], 4.0, eta)
