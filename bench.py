@@ -222,6 +222,7 @@ def run_slp(args):
         n, prec, ngr, rmin, volfrac, iters, lp = 3, tosp.PREC_MIXED, 4, 2.5 / 3, 0.2, 100, "knapsack"
         prj = slp.PrjParams(op=True)
     iters = args.slp_iters or iters
+    lp = args.lp or lp
     mg = tosp.default_mg(ngrids=ngr, cycle=0, omega=0.6, smoothiter1=1, smoothiter2=1, tolMG=1e-8, maxiterMG=2000,
                          flexible=1 if prec == tosp.PREC_MIXED else 0)
     solver = tosp.Solver(pb, mg, precision=prec, mr_n=n, p=3.0, emin=1e-9, opfilter=1, rmin=rmin)
@@ -333,6 +334,11 @@ def run_serving(args):
             srv.wait(rid)
             stats.append(srv.result(rid)[2])
         t1 = time.perf_counter()
+        for k, st in enumerate(stats):
+            if st["relres"] > 1e-8 or st["status"] != 0:
+                nx, n, bc, idx, eta = reqs[k]
+                print(json.dumps({"unconverged": [nx, n, bc, idx, round(eta, 4)], "it": st["it"],
+                                  "relres": st["relres"], "status": st["status"]}), file=sys.stderr)
         lat = np.array([st["ms_latency"] for st in stats])
         out.append({"rate_per_s": lam, "solves_per_s": round(len(ids) / (t1 - t0), 3),
                     "p50_ms": round(float(np.percentile(lat, 50)), 2), "p99_ms": round(float(np.percentile(lat, 99)), 2),
@@ -389,6 +395,7 @@ def main():
                          "bridge (reference axes), MR 3, mixed precision, 100 iterations + GradProj")
     ap.add_argument("--slp-iters", type=int, default=0)
     ap.add_argument("--check-cpu", action="store_true", help="config0: run the same SLP loop on the oracle")
+    ap.add_argument("--lp", default="", choices=["", "highs", "knapsack"], help="LP solver of the SLP loop")
     ap.add_argument("--serving", action="store_true",
                     help="serving stream (seed 7): Poisson arrivals at --rates, p50/p99 latency and solves/s")
     ap.add_argument("--rates", default="10,20,50,100,200,500")

@@ -18,6 +18,7 @@
 
 #include <utility>
 
+#include "mr2_pattern.h"
 #include "tosp_internal.h"
 
 namespace tosp {
@@ -78,9 +79,71 @@ __device__ __forceinline__ void all_pairs(const T *__restrict__ kt, const T (&w)
     (pair_step<T, NSP, Ts>(kt, w, u, acc), ...);
 }
 
+// --- MR factor 2: Walsh-Hadamard form -------------------------------------
+// K_e = sum_b what_b Khat_b with what = H w (8-point Walsh-Hadamard transform
+// of the sub-cube factors) and Khat = H KE / 8; mr2_mask marks the non-zero
+// modes of each entry (mr2_mask; structural zeros skipped at compile time: 1548 instead
+// of 2400 FMAs).  Entry t's non-zero values are contiguous in shared memory,
+// padded to the vector width.
+__host__ __device__ constexpr int mr2_nz(int t) {
+    int c = 0;
+    for (int m = 0; m < 8; ++m) c += (mr2_mask(t) >> m) & 1;
+    return c;
+}
+__host__ __device__ constexpr int mr2_off(int t, int w) {
+    int o = 0;
+    for (int q = 0; q < t; ++q) o += (mr2_nz(q) + w - 1) / w * w;
+    return o;
+}
+
+template <typename T, int t>
+__device__ __forceinline__ void pair_step_mr2(const T *__restrict__ kt, const T (&wh)[8], const T (&u)[24],
+                                              T (&acc)[24]) {
+    constexpr int i = pair_i(t), j = pair_j(t);
+    constexpr int W = Vec<T>::W, NZ = mr2_nz(t), NV = (NZ + W - 1) / W;
+    constexpr unsigned MASK = mr2_mask(t);
+    const typename Vec<T>::type *kv = reinterpret_cast<const typename Vec<T>::type *>(kt + mr2_off(t, W));
+    T vals[NV * W];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) {
+        const typename Vec<T>::type v = kv[q];
+        if constexpr (W == 4) {
+            vals[4 * q] = v.x; vals[4 * q + 1] = v.y; vals[4 * q + 2] = v.z; vals[4 * q + 3] = v.w;
+        } else {
+            vals[2 * q] = v.x; vals[2 * q + 1] = v.y;
+        }
+    }
+    // two partial sums over the set modes (shorter dependent chains)
+    T k0 = T(0), k1 = T(0);
+    int idx = 0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        if ((MASK >> m) & 1) {
+            if (idx & 1) k1 += wh[m] * vals[idx];
+            else k0 += wh[m] * vals[idx];
+            ++idx;
+        }
+    }
+    const T k = k0 + k1;
+    if constexpr (i == j) {
+        acc[i] += k * u[i];
+    } else {
+        acc[i] += k * u[j];
+        acc[j] += k * u[i];
+    }
+}
+
+template <typename T, int... Ts>
+__device__ __forceinline__ void all_pairs_mr2(const T *__restrict__ kt, const T (&wh)[8], const T (&u)[24],
+                                              T (&acc)[24], std::integer_sequence<int, Ts...>) {
+    (pair_step_mr2<T, Ts>(kt, wh, u, acc), ...);
+}
+
 template <typename T, int N> struct FineShape {
     static constexpr int NS = N * N * N;
     static constexpr int NSP = (N == 1) ? 1 : (NS + Vec<T>::W - 1) / Vec<T>::W * Vec<T>::W;
+    // shared-memory length of the block table
+    static constexpr int KT_LEN = (N == 2) ? mr2_off(KE_PACK, Vec<T>::W) : KE_PACK * NSP;
 };
 
 // Operator: persistent CTAs over element bricks; see the file header.
@@ -91,10 +154,10 @@ k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ 
     constexpr int NS = FineShape<T, N>::NS, NSP = FineShape<T, N>::NSP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *kt = reinterpret_cast<T *>(smem_raw);               // KE_PACK * NSP (pair-major)
-    T *xs = kt + KE_PACK * NSP;                             // BRICK_NODES * 3
+    T *xs = kt + FineShape<T, N>::KT_LEN;                   // BRICK_NODES * 3
     T *eo = xs + BRICK_NODES * 3;                           // 24 * BRICK_ELEMS element outputs
     const int tid = threadIdx.x;
-    for (int i = tid; i < KE_PACK * NSP; i += BRICK_ELEMS) kt[i] = ktg[i];
+    for (int i = tid; i < FineShape<T, N>::KT_LEN; i += BRICK_ELEMS) kt[i] = ktg[i];
 
     const Grid &g = fg.g;
     const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
@@ -139,7 +202,26 @@ k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ 
                     wv[s] = T(0);
                 }
             }
-            all_pairs<T, NSP>(kt, wv, u, acc, std::make_integer_sequence<int, KE_PACK>{});
+            if constexpr (N == 2) {
+                // 8-point Walsh-Hadamard transform of the sub-cube factors
+                T wh[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) wh[q] = wv[q];
+#pragma unroll
+                for (int bit = 1; bit < 8; bit <<= 1) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        if (!(q & bit)) {
+                            const T a = wh[q], b = wh[q | bit];
+                            wh[q] = a + b;
+                            wh[q | bit] = a - b;
+                        }
+                    }
+                }
+                all_pairs_mr2<T>(kt, wh, u, acc, std::make_integer_sequence<int, KE_PACK>{});
+            } else {
+                all_pairs<T, NSP>(kt, wv, u, acc, std::make_integer_sequence<int, KE_PACK>{});
+            }
         }
         // element outputs -> per-element slots, then every node gathers the
         // (up to 8) contributions of the brick's elements around it
@@ -170,22 +252,23 @@ k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ 
     }
 }
 
-// Diagonal of K(w): one thread per element, atomics (setup only).
+// Diagonal of K(w): one thread per element, atomics (setup only).  Reads the
+// row-major packed blocks ke[s*300 + rowmajor(i,i)].
 template <int N>
 __global__ void k_fine_diag(double *__restrict__ y, const double *__restrict__ w, const uint8_t *__restrict__ freemask,
-                            const double *__restrict__ ktg, FineGeom fg) {
-    constexpr int NS = N * N * N, NSP = FineShape<double, N>::NSP;
+                            const double *__restrict__ ke, FineGeom fg) {
+    constexpr int NS = N * N * N;
     const Grid &g = fg.g;
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < g.nelem;
          e += (int64_t)gridDim.x * blockDim.x) {
         const int ey = (int)(e % g.nely), ex = (int)((e / g.nely) % g.nelx), ez = (int)(e / ((int64_t)g.nely * g.nelx));
         for (int i = 0; i < 24; ++i) {
-            const int t = pair_index_diag(i);
+            const int t = pair_rowmajor(i, i);
             double d = 0.0;
             for (int s = 0; s < NS; ++s) {
                 const int sy = s % N, sx = (s / N) % N, sz = s / (N * N);
                 d += w[((int64_t)(ez * N + sz) * fg.nelx_d + (ex * N + sx)) * fg.nely_d + (ey * N + sy)] *
-                     ktg[t * NSP + s];
+                     ke[s * KE_PACK + t];
             }
             const int a = i / 3, c = i % 3;
             const int64_t node = ((int64_t)(ez + ((a >> 2) & 1)) * g.nx + (ex + ((a >> 1) & 1))) * g.ny + (ey + (a & 1));
@@ -210,11 +293,39 @@ int fine_nsp(int n, int elem_bytes) {
     return (ns + vw - 1) / vw * vw;
 }
 
+// Host layout of the operator's block table (see FineShape::KT_LEN).
+void fine_block_table(const std::vector<double> &packed_rowmajor, int n, int elem_bytes, std::vector<double> &kt) {
+    const int ns = n * n * n;
+    if (n == 2) {
+        const int w = elem_bytes == 8 ? 2 : 4;
+        kt.assign((size_t)mr2_off(KE_PACK, w), 0.0);
+        for (int t = 0; t < KE_PACK; ++t) {
+            const int rm = pair_rowmajor(pair_i(t), pair_j(t));
+            int o = mr2_off(t, w);
+            for (int m = 0; m < 8; ++m) {
+                if (!((mr2_mask(t) >> m) & 1)) continue;
+                double v = 0.0;
+                for (int q = 0; q < 8; ++q) {
+                    const int sign = (__builtin_popcount(m & q) & 1) ? -1 : 1;
+                    v += sign * packed_rowmajor[(size_t)q * KE_PACK + rm];
+                }
+                kt[o++] = v / 8.0;
+            }
+        }
+        return;
+    }
+    const int nsp = fine_nsp(n, elem_bytes);
+    kt.assign((size_t)KE_PACK * nsp, 0.0);
+    for (int t = 0; t < KE_PACK; ++t) {
+        const int rm = pair_rowmajor(pair_i(t), pair_j(t));
+        for (int s = 0; s < ns; ++s) kt[(size_t)t * nsp + s] = packed_rowmajor[(size_t)s * KE_PACK + rm];
+    }
+}
+
 template <typename T, typename TW, int N>
 static void launch_fine_t(const T *x, T *y, const TW *w, const uint8_t *fm, const T *kt, const FineGeom &fg,
                           cudaStream_t st) {
-    constexpr int NSP = FineShape<T, N>::NSP;
-    const size_t smem = sizeof(T) * (KE_PACK * NSP + BRICK_NODES * 3 + 24 * BRICK_ELEMS);
+    const size_t smem = sizeof(T) * (FineShape<T, N>::KT_LEN + BRICK_NODES * 3 + 24 * BRICK_ELEMS);
     auto kern = k_fine_apply<T, TW, N>;
     static int attr_dev = -1;
     int dev = 0;
@@ -247,14 +358,14 @@ template void launch_fine_apply<double, double>(const double *, double *, const 
 template void launch_fine_apply<float, __nv_bfloat16>(const float *, float *, const __nv_bfloat16 *, const uint8_t *,
                                                       const float *, const FineGeom &, int, cudaStream_t);
 
-void launch_fine_diag(double *y, const double *w, const uint8_t *freemask, const double *kt64, const FineGeom &fg,
+void launch_fine_diag(double *y, const double *w, const uint8_t *freemask, const double *ke64, const FineGeom &fg,
                       int n, cudaStream_t st) {
     int64_t blocks = (fg.g.nelem + 255) / 256;
     if (blocks > 16 * num_sms()) blocks = 16 * num_sms();
     if (blocks < 1) blocks = 1;
-    if (n == 1) { k_fine_diag<1><<<(unsigned)blocks, 256, 0, st>>>(y, w, freemask, kt64, fg); count_launch(); }
-    else if (n == 2) { k_fine_diag<2><<<(unsigned)blocks, 256, 0, st>>>(y, w, freemask, kt64, fg); count_launch(); }
-    else { k_fine_diag<3><<<(unsigned)blocks, 256, 0, st>>>(y, w, freemask, kt64, fg); count_launch(); }
+    if (n == 1) { k_fine_diag<1><<<(unsigned)blocks, 256, 0, st>>>(y, w, freemask, ke64, fg); count_launch(); }
+    else if (n == 2) { k_fine_diag<2><<<(unsigned)blocks, 256, 0, st>>>(y, w, freemask, ke64, fg); count_launch(); }
+    else { k_fine_diag<3><<<(unsigned)blocks, 256, 0, st>>>(y, w, freemask, ke64, fg); count_launch(); }
 }
 
 // ---------------------------------------------------------------------------

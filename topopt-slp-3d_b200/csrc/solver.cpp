@@ -440,16 +440,10 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
     TRY(dalloc(h, &h->d_ke64, (int64_t)packed.size()));
     CK(cudaMemcpy(h->d_ke64, packed.data(), sizeof(double) * packed.size(), cudaMemcpyHostToDevice));
     {
-        const int nsp64 = fine_nsp(h->n, 8), nsp32 = fine_nsp(h->n, 4);
-        std::vector<double> kt64((size_t)KE_PACK * nsp64, 0.0);
-        std::vector<float> kt32((size_t)KE_PACK * nsp32, 0.0f);
-        for (int t = 0; t < KE_PACK; ++t) {
-            const int rm = pair_rowmajor(pair_i(t), pair_j(t));
-            for (int s = 0; s < h->ns; ++s) {
-                kt64[(size_t)t * nsp64 + s] = packed[(size_t)s * KE_PACK + rm];
-                kt32[(size_t)t * nsp32 + s] = (float)packed[(size_t)s * KE_PACK + rm];
-            }
-        }
+        std::vector<double> kt64, kt32d;
+        fine_block_table(packed, h->n, 8, kt64);
+        fine_block_table(packed, h->n, 4, kt32d);
+        std::vector<float> kt32(kt32d.begin(), kt32d.end());
         TRY(dalloc(h, &h->d_kt64, (int64_t)kt64.size()));
         TRY(dalloc(h, &h->d_kt32, (int64_t)kt32.size()));
         CK(cudaMemcpy(h->d_kt64, kt64.data(), sizeof(double) * kt64.size(), cudaMemcpyHostToDevice));
@@ -567,7 +561,7 @@ int setup_levels(tosp_handle *h) {
     // the V-cycle hierarchy is Galerkin-consistent with the V-cycle's finest
     // operator: FP64 factors for the FP64 path, the BF16-rounded ones for mixed
     const double *wh = h->d_wq ? h->d_wq : h->d_w64;
-    launch_fine_diag(h->d_diag64, wh, h->lev[0].fm, h->d_kt64, h->fg, h->n, h->stream);
+    launch_fine_diag(h->d_diag64, wh, h->lev[0].fm, h->d_ke64, h->fg, h->n, h->stream);
     CKL();
     if constexpr (sizeof(T) == 8) {
         launch_invert_diag<double>(h->d_diag64, h->lev[0].fm, (double *)h->lev[0].invd, h->mg.omega, nd0, h->stream);

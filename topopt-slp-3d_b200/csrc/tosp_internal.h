@@ -105,11 +105,14 @@ void launch_simp(const double *rho, double *w64, __nv_bfloat16 *wbf, double *wq,
 template <typename T, typename TW>
 void launch_fine_apply(const T *x, T *y, const TW *w, const uint8_t *freemask, const T *kt, const FineGeom &fg,
                        int n, cudaStream_t st);
-// y += diag(K(w)) (y zeroed by the caller).
-void launch_fine_diag(double *y, const double *w, const uint8_t *freemask, const double *kt64, const FineGeom &fg,
+// y += diag(K(w)) (y zeroed by the caller); ke64: row-major packed blocks.
+void launch_fine_diag(double *y, const double *w, const uint8_t *freemask, const double *ke64, const FineGeom &fg,
                       int n, cudaStream_t st);
 // Stride of the pair-major block layout: entry t of block s at kt[t*nsp + s].
 int fine_nsp(int n, int elem_bytes);
+// The operator's block table from the row-major packed blocks (n = 2: the
+// Walsh-Hadamard modes; otherwise pair-major with stride fine_nsp).
+void fine_block_table(const std::vector<double> &packed_rowmajor, int n, int elem_bytes, std::vector<double> &kt);
 
 // Sensitivities g0 (I/Grad.m:24-49), zero for elements not in freeDensG.
 void launch_grad(const double *u, const double *rho, const uint8_t *free_elem, const double *kepack,
