@@ -304,7 +304,7 @@ def run_serving(args):
 
     def submit(srv, item):
         pb, n, x, ng = item
-        mg = tosp.default_mg(ngrids=ng, cycle=0, omega=0.6, tolMG=1e-8, maxiterMG=1000, flexible=1)
+        mg = tosp.default_mg(ngrids=ng, cycle=0, omega=0.6, tolMG=1e-8, maxiterMG=1000, flexible=1, maxstall=60)
         return srv.submit(pb, x, mg=mg, precision=tosp.PREC_MIXED, mr_n=n, p=3.0, emin=1e-9, opfilter=1,
                           rmin=1.0 if n > 1 else 1.5)
 
@@ -344,6 +344,7 @@ def run_serving(args):
                     "p50_ms": round(float(np.percentile(lat, 50)), 2), "p99_ms": round(float(np.percentile(lat, 99)), 2),
                     "mean_run_ms": round(float(np.mean([st["ms_run"] for st in stats])), 2),
                     "max_it": int(max(st["it"] for st in stats)),
+                    "fp64_fallbacks": int(sum(1 for st in stats if st["precision"] == 0)),
                     "all_converged": bool(all(st["relres"] <= 1e-8 for st in stats))})
         print(json.dumps(out[-1]), file=sys.stderr)
     clk = clocks.stop()
@@ -425,16 +426,13 @@ def main():
     import tosp
     from tosp.workloads import build_workload
 
+    from tosp import replicas
+
     def barrier():
-        if world > 1:
-            dist.barrier()
+        replicas.barrier()
 
     def max_over_ranks(v):
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return replicas.max_over_ranks(v, device="cuda")
 
     # ---- workload -------------------------------------------------------------
     holder = {}

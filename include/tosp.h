@@ -84,6 +84,10 @@ typedef struct tosp_mg_params {
                               1: flexible (Polak-Ribiere) beta = r'(s - s_old)/rho_old,
                               robust to a preconditioner that varies between applications
                               (FP32 V-cycle with atomics)                                    */
+    int32_t maxstall;      /* 0: off (the reference runs to maxiterMG); k > 0: stop with
+                              TOSP_NOT_CONVERGED when the best relative residual has not
+                              halved within k iterations (used by the serving loop to fall
+                              back from a stalling mixed-precision solve)                    */
 } tosp_mg_params;
 
 /* Statistics of the last tosp_solve_mg call. */
@@ -212,6 +216,9 @@ typedef struct tosp_request_stats {
     double  ms_latency;    /* submit -> results ready (host clock)                 */
     double  ms_queue;      /* time spent waiting for a slot / memory                */
     double  ms_run;        /* setup + solve + Grad                                 */
+    int32_t precision;     /* precision that produced the result: a mixed-precision
+                              request whose solve stalls or breaks down is re-run once
+                              in FP64, warm-started from the mixed iterate            */
 } tosp_request_stats;
 
 int tosp_server_create(int32_t max_slots, int64_t hbm_budget_bytes, tosp_server **out);

@@ -45,3 +45,20 @@ def test_slp_mixed_precision_same_designs(tosp_mod):
     tmx = slp.grad_proj(rmx.xstar, np.ones(pb.nelem), prj, 0.3 * V, velem)
     assert np.abs(r64.x - rmx.x).max() <= 1e-5
     assert np.count_nonzero(t64 != tmx) <= 0.001 * t64.size
+
+
+def test_correct_function_value_matches_oracle(tosp_mod):
+    """CorrectFunctionValue (I/CorrectFunctionValue.m): re-solve the MR design
+    on the density mesh; against the oracle's assembled solve on that mesh."""
+    import scipy.sparse.linalg as spla
+    from oracle import fem
+    pb = P.cantilever(8, 4, 4)
+    n = 2
+    x = np.random.default_rng(2).uniform(0.2, 1.0, pb.nelem * n ** 3)
+    F, it, rr = slp.correct_function_value(pb, n, x, tosp_mod.default_mg(ngrids=3, cycle=1, omega=0.5))
+    strT = slp.density_mesh_problem(pb, n)
+    ks = fem.elem_stiff_gqmr(strT.el, strT.eh, strT.ew, strT.nu, 1)
+    K = fem.global_stiff_matrix(strT.nelx, strT.nely, strT.nelz, ks, x, 3.0, 1e-9, strT.freedofs)
+    u = spla.spsolve(K.tocsc(), strT.f)
+    assert rr <= 1e-8
+    assert abs(F - strT.f @ u) <= 1e-7 * abs(strT.f @ u)

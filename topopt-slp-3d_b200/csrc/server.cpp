@@ -10,6 +10,7 @@
 // problem shape and reused by later requests of the same shape (hierarchy
 // buffers, captured graph), and evicted when another shape needs the memory.
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -36,6 +37,8 @@ struct Request {
     tosp_mg_params mg{};
     int32_t precision = TOSP_PREC_MIXED;
     std::vector<double> xfil, f;
+    std::vector<double> u0;        // warm start (FP64 re-run after a stalled mixed solve)
+    int fallbacks = 0;
     // results
     std::vector<double> u, g;
     tosp_request_stats st{};
@@ -148,6 +151,7 @@ void run_request(tosp_server *s, Request &r, tosp_handle *h) {
     const auto t0 = Clock::now();
     int rc = tosp_setup_gmg(h, r.xfil.data(), (int64_t)r.xfil.size());
     std::vector<double> x(r.freedofs.size(), 0.0);
+    if (r.u0.size() == x.size()) x = r.u0;
     int32_t it = 0;
     double rr = 0;
     if (rc == TOSP_OK) rc = tosp_solve_mg(h, x.data(), r.f.data(), (int64_t)x.size(), &it, &rr);
@@ -170,6 +174,7 @@ void run_request(tosp_server *s, Request &r, tosp_handle *h) {
     r.st.ms_run = std::chrono::duration<double, std::milli>(t1 - t0).count();
     r.st.ms_latency = std::chrono::duration<double, std::milli>(t1 - r.t_submit).count();
     r.st.ms_queue = r.st.ms_latency - r.st.ms_run;
+    r.st.precision = r.precision;
     (void)s;
 }
 
@@ -211,8 +216,13 @@ void worker_main(tosp_server *s) {
                     h = nullptr;
                 }
             }
-            if (h) run_request(s, *r, h);
-            else r->status = rc;
+            if (h) {
+                // a breakdown leaves the handle's iterate unusable for a warm start
+                run_request(s, *r, h);
+                if (r->status == TOSP_ERR_BREAKDOWN) r->u.clear();
+            } else {
+                r->status = rc;
+            }
             lk.lock();
             for (auto it = s->cache.begin(); it != s->cache.end(); ++it) {
                 if (it->busy && it->key == key && (it->h == h || it->h == nullptr)) {
@@ -235,7 +245,26 @@ void worker_main(tosp_server *s) {
                     break;
                 }
             }
-            r->state = r->status < 0 ? TOSP_REQ_FAILED : TOSP_REQ_DONE;
+            const bool stalled = r->status == TOSP_NOT_CONVERGED || r->status == TOSP_ERR_BREAKDOWN;
+            if (stalled && r->precision == TOSP_PREC_MIXED && r->fallbacks == 0) {
+                // re-run once in FP64 (front of the queue), warm-started from
+                // the mixed iterate when it is finite
+                r->fallbacks = 1;
+                r->precision = TOSP_PREC_FP64;
+                r->mg.maxstall = 0;
+                r->u0.clear();
+                bool finite = !r->u.empty();
+                for (double v : r->u) finite = finite && std::isfinite(v);
+                if (finite) r->u0 = r->u;
+                r->key = shape_key(*r);
+                r->est_bytes = estimate_bytes(*r);
+                r->state = TOSP_REQ_QUEUED;
+                r->status = TOSP_OK;
+                r->err.clear();
+                s->queue.push_front(r);
+            } else {
+                r->state = r->status < 0 ? TOSP_REQ_FAILED : TOSP_REQ_DONE;
+            }
             s->active--;
             s->completed++;
         }

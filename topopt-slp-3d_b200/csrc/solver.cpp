@@ -675,6 +675,8 @@ int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
     double nr = std::sqrt(h->h_scal[3]) / nf;
     int it = 1;
     int rc = TOSP_OK;
+    double best = nr;
+    int best_it = 1;
     while (nr > h->mg.tolMG && it <= h->mg.maxiterMG) {
         if (it == 1) {
             TRY(cg_iteration(h, 1));
@@ -687,16 +689,29 @@ int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
             }
         }
         TRY(sync(h));
-        const double dq = h->h_scal[2], rr = h->h_scal[3];
-        if (!(dq > 0.0) || !std::isfinite(rr)) {
-            h->err = "CG breakdown: d'q = " + std::to_string(dq) + ", r'r = " + std::to_string(rr);
+        const double rho = h->h_scal[0], dq = h->h_scal[2], rr = h->h_scal[3];
+        if (!(dq > 0.0) || !(rho > 0.0) || !std::isfinite(rr)) {
+            h->err = "CG breakdown: r'M^{-1}r = " + std::to_string(rho) + ", d'q = " + std::to_string(dq) +
+                     ", r'r = " + std::to_string(rr);
             rc = TOSP_ERR_BREAKDOWN;
             break;
         }
         nr = std::sqrt(rr) / nf;
         ++it;
+        if (nr <= 0.5 * best) {
+            best = nr;
+            best_it = it;
+        }
+        if (h->mg.maxstall > 0 && nr > h->mg.tolMG && it - best_it >= h->mg.maxstall) {
+            h->err = "CG stalled: relative residual not halved in " + std::to_string(h->mg.maxstall) + " iterations";
+            rc = TOSP_NOT_CONVERGED;
+            break;
+        }
     }
     if (rc == TOSP_OK && nr > h->mg.tolMG && it > h->mg.maxiterMG) rc = TOSP_NOT_CONVERGED;
+    if (rc == TOSP_ERR_BREAKDOWN && h->precision == TOSP_PREC_MIXED) {
+        // keep the last iterate: a caller may continue from it in FP64
+    }
     if (it_out) *it_out = it;
     if (relres_out) *relres_out = nr;
     h->stats.it = it;
@@ -748,6 +763,7 @@ void tosp_default_mg_params(tosp_mg_params *mg) {
     mg->maxiterMG = 5000;
     mg->nmaxchol = 60000;
     mg->flexible = 0;
+    mg->maxstall = 0;
 }
 
 int tosp_create(const tosp_problem *prob, const tosp_mg_params *mg, int32_t precision, tosp_handle **out) {

@@ -49,12 +49,13 @@ class MgParams(C.Structure):
     """The ``mg.*`` struct of the reference (I/TopOpt3D.m:171-190)."""
     _fields_ = [("ngrids", C.c_int32), ("cycle", C.c_int32), ("smoother", C.c_int32), ("omega", C.c_double),
                 ("smoothiter1", C.c_int32), ("smoothiter2", C.c_int32), ("tolMG", C.c_double),
-                ("maxiterMG", C.c_int32), ("nmaxchol", C.c_int32), ("flexible", C.c_int32)]
+                ("maxiterMG", C.c_int32), ("nmaxchol", C.c_int32), ("flexible", C.c_int32),
+                ("maxstall", C.c_int32)]
 
 
 class RequestStats(C.Structure):
     _fields_ = [("it", C.c_int32), ("relres", C.c_double), ("ms_latency", C.c_double), ("ms_queue", C.c_double),
-                ("ms_run", C.c_double)]
+                ("ms_run", C.c_double), ("precision", C.c_int32)]
 
 
 class SolveStats(C.Structure):
@@ -357,7 +358,7 @@ class Server:
             _lib.tosp_server_release(self.h, rid)
             self.meta.pop(rid, None)
         return u, g, {"it": st.it, "relres": st.relres, "ms_latency": st.ms_latency, "ms_queue": st.ms_queue,
-                      "ms_run": st.ms_run, "status": rc}
+                      "ms_run": st.ms_run, "precision": st.precision, "status": rc}
 
     def cancel(self, rid):
         return _lib.tosp_server_cancel(self.h, rid)

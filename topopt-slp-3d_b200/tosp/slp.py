@@ -78,17 +78,26 @@ def lp_knapsack(g, a, c, lo, hi):
         return s, float(g @ s), 0.0, True
     cand = np.nonzero((g < 0) & (hi > lo))[0]
     ratio = -g[cand] / a[cand]
-    order = cand[np.argsort(ratio, kind="stable")]
+    srt = np.argsort(ratio, kind="stable")
+    order, ratio = cand[srt], ratio[srt]
     red = a[order] * (hi[order] - lo[order])        # constraint reduction if moved fully to lo
-    cum = np.cumsum(red)
-    k = int(np.searchsorted(cum, excess))
-    if k >= order.size:
+    # equal ratios (mirror-symmetric elements) form one group that moves by a
+    # common fraction, so the step does not depend on round-off between them
+    newgrp = np.ones(order.size, dtype=bool)
+    newgrp[1:] = ratio[1:] - ratio[:-1] > 1e-9 * np.abs(ratio[1:])
+    gid = np.cumsum(newgrp) - 1
+    gred = np.bincount(gid, weights=red)
+    gcum = np.cumsum(gred)
+    k = int(np.searchsorted(gcum, excess))
+    if k >= gred.size:
         return None, None, None, False                # infeasible within the box
-    s[order[:k]] = lo[order[:k]]
-    prev = cum[k - 1] if k > 0 else 0.0
-    j = order[k]
-    s[j] = hi[j] - (excess - prev) / a[j]
-    lam = float(-g[j] / a[j])
+    done = gid < k
+    s[order[done]] = lo[order[done]]
+    prev = gcum[k - 1] if k > 0 else 0.0
+    frac = (excess - prev) / gred[k]
+    grp = order[gid == k]
+    s[grp] = hi[grp] - frac * (hi[grp] - lo[grp])
+    lam = float(np.mean(ratio[gid == k]))
     return s, float(g @ s), lam, True
 
 
@@ -307,3 +316,28 @@ def str_slp(solver, pb, volfrac, x0, slp=None, prj=None, fixed=None, on_iter=Non
         res.xstar = xfil
     res.x, res.u, res.F, res.iters, res.rejected = x, u, F, it_acc, itrej
     return res
+
+
+def density_mesh_problem(pb, n):
+    """The problem on the density mesh (n times finer), built from the same
+    support/load rows (the ``strT`` of I/ExtraResults.m for CorrectFunctionValue)."""
+    from . import problems
+    if pb.supp is None or pb.loads is None:
+        raise ValueError("the problem needs its support/load rows to be rebuilt on the density mesh")
+    return problems.build(pb.nelx * n, pb.nely * n, pb.nelz * n, pb.supp, pb.loads, el=pb.el / n, eh=pb.eh / n,
+                          ew=pb.ew / n, E=pb.E, nu=pb.nu)
+
+
+def correct_function_value(pb, n, xstar, mg=None, precision=0, p=3.0, emin=1e-9):
+    """``Ftrue`` of I/CorrectFunctionValue.m:1-58: the compliance of the
+    multiresolution design re-solved with one displacement element per density
+    element (no multiresolution), on the GPU solve path."""
+    from . import Solver, default_mg
+    strT = density_mesh_problem(pb, n)
+    s = Solver(strT, mg if mg is not None else default_mg(), precision=precision, mr_n=1, p=p, emin=emin,
+               opfilter=0, rmin=1.0)
+    s.SetupGMG(np.asarray(xstar, dtype=np.float64))
+    u, it, rr, rc = s.SolveMG(np.zeros(strT.f.size), strT.f)
+    F = float(strT.f @ u)
+    s.close()
+    return F, it, rr
