@@ -373,6 +373,9 @@ def profile_kernels(args):
     r = np.random.default_rng(0).standard_normal(pb.freedofs.size)
     s.KelemProd(r)       # k_fine_apply<double,double>
     s.MGCycle(r)         # two k_fine_apply<float,bf16> launches
+    if args.profile_solve:
+        u, it, rr, rc = s.SolveMG(np.zeros(pb.f.size), pb.f)   # one full mixed solve
+        print("solve iterations", it)
     torch.cuda.synchronize()
     s.close()
     print("profile run done")
@@ -403,6 +406,8 @@ def main():
     ap.add_argument("--serving-count", type=int, default=512)
     ap.add_argument("--slots", type=int, default=4)
     ap.add_argument("--budget-gb", type=float, default=64.0)
+    ap.add_argument("--profile-solve", action="store_true",
+                    help="with --profile-kernels: also one full mixed-precision solve (launch lists)")
     ap.add_argument("--profile-kernels", action="store_true",
                     help="one mixed-precision handle: setup, one FP64 product and one V-cycle, then exit "
                          "(a short run for ncu captures of the operator kernels)")

@@ -690,7 +690,11 @@ int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
         }
         TRY(sync(h));
         const double rho = h->h_scal[0], dq = h->h_scal[2], rr = h->h_scal[3];
-        if (!(dq > 0.0) || !(rho > 0.0) || !std::isfinite(rr)) {
+        // r'M^{-1}r may turn negative when the smoother is not convergent for
+        // the chosen omega (the V-cycle is then indefinite); the reference
+        // PCG carries on in that case, so only d'Kd <= 0 and non-finite
+        // values stop the iteration.
+        if (!(dq > 0.0) || !std::isfinite(rho) || !std::isfinite(rr)) {
             h->err = "CG breakdown: r'M^{-1}r = " + std::to_string(rho) + ", d'q = " + std::to_string(dq) +
                      ", r'r = " + std::to_string(rr);
             rc = TOSP_ERR_BREAKDOWN;
@@ -709,9 +713,6 @@ int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
         }
     }
     if (rc == TOSP_OK && nr > h->mg.tolMG && it > h->mg.maxiterMG) rc = TOSP_NOT_CONVERGED;
-    if (rc == TOSP_ERR_BREAKDOWN && h->precision == TOSP_PREC_MIXED) {
-        // keep the last iterate: a caller may continue from it in FP64
-    }
     if (it_out) *it_out = it;
     if (relres_out) *relres_out = nr;
     h->stats.it = it;
