@@ -106,7 +106,7 @@ def run_reference(args, world, rank):
     spec = WORKLOADS[args.workload]
     pb, n, xfil, spec = build_workload(args.workload, filter_fn=_cpu_filter(args.workload))
     cores = os.cpu_count()
-    cw = CpuWok(pb, n, spec["ngrids"], 0.6, nthreads=cores)
+    cw = CpuWok(pb, n, spec["ngrids"], spec["omega"], nthreads=cores)
     f = pb.f_full()
     its = spec.get("pcg_iterations_fp64")
     samples = []
@@ -162,7 +162,7 @@ def cpu_baseline(args, pb, n, xfil, spec, it_fp64):
     """Bounded CPU sample of the same workload (oracle port, all host cores)."""
     from oracle.cpu_wok import CpuWok
     cores = os.cpu_count()
-    cw = CpuWok(pb, n, spec["ngrids"], 0.6, nthreads=cores)
+    cw = CpuWok(pb, n, spec["ngrids"], spec["omega"], nthreads=cores)
     f = pb.f_full()
     t0 = time.perf_counter()
     cw.setup(xfil)
@@ -215,16 +215,16 @@ def run_slp(args):
     torch.cuda.set_device(0)
     if args.slp == "config0":
         pb = P.cantilever(48, 24, 24)
-        n, prec, ngr, rmin, volfrac, iters, lp = 1, tosp.PREC_FP64, 3, 1.5, 0.3, 20, "highs"
+        n, prec, ngr, rmin, volfrac, iters, lp, omega = 1, tosp.PREC_FP64, 3, 1.5, 0.3, 20, "highs", 0.6
         prj = slp.PrjParams(op=False)
     else:
         pb = P.bridge(160, 80, 40)
-        n, prec, ngr, rmin, volfrac, iters, lp = 3, tosp.PREC_MIXED, 4, 2.5 / 3, 0.2, 100, "knapsack"
+        n, prec, ngr, rmin, volfrac, iters, lp, omega = 3, tosp.PREC_MIXED, 4, 2.5 / 3, 0.2, 100, "knapsack", 0.5
         prj = slp.PrjParams(op=True)
     iters = args.slp_iters or iters
     lp = args.lp or lp
-    mg = tosp.default_mg(ngrids=ngr, cycle=0, omega=0.6, smoothiter1=1, smoothiter2=1, tolMG=1e-8, maxiterMG=2000,
-                         flexible=1 if prec == tosp.PREC_MIXED else 0)
+    mg = tosp.default_mg(ngrids=ngr, cycle=0, omega=omega, smoothiter1=1, smoothiter2=1, tolMG=1e-8,
+                         maxiterMG=2000, flexible=1 if prec == tosp.PREC_MIXED else 0)
     solver = tosp.Solver(pb, mg, precision=prec, mr_n=n, p=3.0, emin=1e-9, opfilter=1, rmin=rmin)
     timed = _Timed(solver)
     x0 = np.full(pb.nelem * n ** 3, volfrac)
@@ -255,7 +255,7 @@ def run_slp(args):
     if args.slp == "config3":
         # final displacement checked with the CPU restatement of KelemProd
         from oracle.cpu_wok import CpuWok
-        cw = CpuWok(pb, n, ngr, 0.6, nthreads=os.cpu_count())
+        cw = CpuWok(pb, n, ngr, omega, nthreads=os.cpu_count())
         xf_final = solver.ApplyFilter(res.x)
         solver.SetupGMG(xf_final)
         u_final = solver.SolveMG(res.u, pb.f)[0]
@@ -269,7 +269,7 @@ def run_slp(args):
     if args.check_cpu and args.slp == "config0":
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         from oracle_solver import OracleSolver
-        orc = OracleSolver(pb, n=n, ngrids=ngr, cycle=0, omega=0.6, rmin=rmin)
+        orc = OracleSolver(pb, n=n, ngrids=ngr, cycle=0, omega=omega, rmin=rmin)
         t1 = time.perf_counter()
         ro = slp.str_slp(orc, pb, volfrac, x0, slp.SlpParams(maxiter=iters, lp=lp), prj=prj)
         tcpu = time.perf_counter() - t1
@@ -304,7 +304,8 @@ def run_serving(args):
 
     def submit(srv, item):
         pb, n, x, ng = item
-        mg = tosp.default_mg(ngrids=ng, cycle=0, omega=0.6, tolMG=1e-8, maxiterMG=1000, flexible=1, maxstall=60)
+        mg = tosp.default_mg(ngrids=ng, cycle=0, omega=W.REF_OMEGA, tolMG=1e-8, maxiterMG=1000, flexible=1,
+                             maxstall=60)
         return srv.submit(pb, x, mg=mg, precision=tosp.PREC_MIXED, mr_n=n, p=3.0, emin=1e-9, opfilter=1,
                           rmin=1.0 if n > 1 else 1.5)
 
@@ -367,7 +368,8 @@ def profile_kernels(args):
     from tosp.workloads import WORKLOADS, build_workload
     spec = WORKLOADS[args.workload]
     pb, n, xfil, spec = build_workload(args.workload)
-    mg = tosp.default_mg(ngrids=args.ngrids or spec["ngrids"], cycle=0, omega=0.6, tolMG=1e-8, maxiterMG=1000)
+    mg = tosp.default_mg(ngrids=args.ngrids or spec["ngrids"], cycle=0, omega=spec["omega"], tolMG=1e-8,
+                         maxiterMG=1000)
     s = tosp.Solver(pb, mg, precision=tosp.PREC_MIXED, mr_n=n, p=3.0, emin=1e-9, opfilter=1, rmin=spec["rmin"])
     s.SetupGMG(xfil)
     r = np.random.default_rng(0).standard_normal(pb.freedofs.size)
@@ -450,7 +452,7 @@ def main():
     nelx, nely, nelz = spec0["dims"]
     pb0 = tosp.problems.cantilever(nelx, nely, nelz)
     ngrids = args.ngrids or spec0["ngrids"]
-    mg = tosp.default_mg(ngrids=ngrids, cycle=0, omega=0.6, smoothiter1=1, smoothiter2=1, tolMG=1e-8,
+    mg = tosp.default_mg(ngrids=ngrids, cycle=0, omega=spec0["omega"], smoothiter1=1, smoothiter2=1, tolMG=1e-8,
                          maxiterMG=1000, flexible=args.flexible)
     n = spec0["n"]
     kw = dict(mr_n=n, p=3.0, emin=1e-9, opfilter=1, rmin=spec0["rmin"])
@@ -580,7 +582,7 @@ def main():
         "data": "synthetic",
         "config": {"workload": args.workload, "mesh": list(spec["dims"]), "mr_n": n, "ndof": ndof,
                    "nfree": int(pb.freedofs.size), "density_elements": int(nsub), "ngrids": ngrids, "cg_beta": "flexible" if args.flexible else "reference",
-                   "cycle": "V", "omega": 0.6, "smooth": "1+1 Jacobi", "tol": 1e-8,
+                   "cycle": "V", "omega": spec0["omega"], "smooth": "1+1 Jacobi", "tol": 1e-8,
                    "l2": "inputs larger than L2 (densities 113 MB, vectors 44 MB each)",
                    "parallelism": f"replicas x{world}"},
         "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3), "p99": round(float(np.percentile(lat, 99)), 3)},

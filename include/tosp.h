@@ -139,6 +139,13 @@ int tosp_setup_gmg(tosp_handle *h, const double *xfil, int64_t ndens);
 /* y = K(rho) x on the free dofs: KelemProd (I/WOK/KelemProd.m:1). */
 int tosp_kelem_prod(tosp_handle *h, const double *x, double *y, int64_t nfree);
 
+/* y = K(rho) x evaluated by the finest-level operator of the mixed V-cycle
+ * (FP32 vectors, BF16 SIMP factors; for MR factor 2 the element matrices are
+ * formed on the tensor cores).  No counterpart in the reference: it exposes
+ * the preconditioner's operator for inspection and tests.  TOSP_PREC_MIXED
+ * handles only (TOSP_ERR_STATE otherwise); x and y are FP64 on the free dofs. */
+int tosp_kelem_prod_mixed(tosp_handle *h, const double *x, double *y, int64_t nfree);
+
 /* One preconditioner application s = cycle(r) (VCycle/WCycle/FMVCycle,
  * I/VCycle.m:1, I/WCycle.m:1, I/FMVCycle.m:1) on free-dof vectors. */
 int tosp_mg_cycle(tosp_handle *h, const double *r, double *s, int64_t nfree);

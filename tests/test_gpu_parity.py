@@ -61,6 +61,42 @@ def test_kelem_prod_parity(tosp_mod, dims, n):
     assert rel(y, yo) <= 1e-12
 
 
+def bf16_round(a):
+    """Round FP64 values to the nearest BF16 (8 significant bits, ties to
+    even), as __double2bfloat16 does for the normal range used here."""
+    m, e = np.frexp(np.asarray(a, dtype=np.float64))
+    return np.ldexp(np.round(m * 256.0) / 256.0, e)
+
+
+@pytest.mark.parametrize("dims,n", [((8, 4, 4), 2), ((10, 9, 3), 2), ((12, 16, 6), 2), ((4, 8, 12), 2),
+                                    ((6, 10, 2), 1), ((4, 4, 4), 3)])
+def test_mixed_operator_parity(tosp_mod, dims, n):
+    """The V-cycle's FP32/BF16 finest operator (tensor-core element matrices
+    for MR factor 2) against the FP64 oracle product with the same
+    BF16-rounded SIMP factors: max error <= 1e-5 of max |y| (FP32 vectors and
+    accumulation).  Ragged meshes leave partially filled element bricks."""
+    pb = P.cantilever(*dims)
+    dens = make(pb, n, seed=sum(dims) + 1)
+    s = solver(tosp_mod, pb, n, prec=1)
+    s.SetupGMG(dens)
+    ks = fem.elem_stiff_gqmr(1, 1, 1, 0.3, n)
+    x = np.random.default_rng(3).standard_normal(pb.freedofs.size)
+    y = s.KelemProdMixed(x)
+    xc = np.zeros(3 * pb.nnodes)
+    xc[pb.freedofs] = x.astype(np.float32)
+    wq = bf16_round(fem.simp(dens, P_SIMP, EMIN))
+    yo = fem.kelem_prod_full(pb.nelx, pb.nely, pb.nelz, ks, wq, xc, n)[pb.freedofs]
+    assert rel(y, yo) <= 1e-5
+    # and against the FP64 operator: the BF16 factors differ by <= 2^-9
+    assert rel(y, s_fp64_product(tosp_mod, pb, n, dens, x)) <= 1e-2
+
+
+def s_fp64_product(tosp_mod, pb, n, dens, x):
+    s = solver(tosp_mod, pb, n)
+    s.SetupGMG(dens)
+    return s.KelemProd(x)
+
+
 @pytest.mark.parametrize("cycle", [0, 1, 2])
 @pytest.mark.parametrize("dims,n,ngrids", [((8, 4, 4), 2, 3), ((16, 8, 8), 1, 3), ((16, 8, 8), 1, 4),
                                            ((8, 8, 4), 3, 2)])

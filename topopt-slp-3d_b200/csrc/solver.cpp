@@ -52,6 +52,8 @@ struct tosp_handle {
     double *d_ke64 = nullptr;       // blocks packed per s (coarse build, Grad)
     double *d_kt64 = nullptr;       // pair-major layout of the fine operator
     float *d_kt32 = nullptr;
+    uint16_t *d_tcimg = nullptr;    // mixed, MR 2: tensor-core B operand image of the blocks
+    int *d_tcerr = nullptr;         // set by the tensor-core operator when an MMA wait times out
     // densities
     double *d_rho = nullptr, *d_w64 = nullptr;
     double *d_wq = nullptr;         // mixed: BF16-rounded factors in FP64 (V-cycle hierarchy)
@@ -187,6 +189,8 @@ int fine_apply(tosp_handle *h, const T *x, T *y) {
     CK(cudaMemsetAsync(y, 0, sizeof(T) * h->fg.g.ndof, h->stream));
     if constexpr (sizeof(T) == 8) {
         launch_fine_apply<double, double>(x, y, h->d_w64, h->lev[0].fm, h->d_kt64, h->fg, h->n, h->stream);
+    } else if (h->d_tcimg) {
+        launch_fine_apply_tc(x, y, h->d_wbf, h->lev[0].fm, h->d_tcimg, h->fg, h->d_tcerr, h->stream);
     } else {
         launch_fine_apply<float, __nv_bfloat16>(x, y, h->d_wbf, h->lev[0].fm, h->d_kt32, h->fg, h->n, h->stream);
     }
@@ -449,6 +453,14 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
         CK(cudaMemcpy(h->d_kt64, kt64.data(), sizeof(double) * kt64.size(), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(h->d_kt32, kt32.data(), sizeof(float) * kt32.size(), cudaMemcpyHostToDevice));
     }
+    if (precision == TOSP_PREC_MIXED && h->n == 2) {
+        std::vector<uint16_t> img;
+        fine_tc_image(packed, img);
+        TRY(dalloc(h, &h->d_tcimg, (int64_t)img.size()));
+        CK(cudaMemcpy(h->d_tcimg, img.data(), sizeof(uint16_t) * img.size(), cudaMemcpyHostToDevice));
+        TRY(dalloc(h, &h->d_tcerr, 1));
+        CK(cudaMemset(h->d_tcerr, 0, sizeof(int)));
+    }
 
     // levels
     const size_t tsz = precision == TOSP_PREC_FP64 ? 8 : 4;
@@ -609,6 +621,21 @@ int need_mg(tosp_handle *h) {
     return TOSP_OK;
 }
 
+// Reads (and clears) the tensor-core operator's timeout flag; call after a
+// stream synchronisation.
+int check_tc(tosp_handle *h) {
+    if (!h->d_tcerr) return TOSP_OK;
+    int e = 0;
+    CK(cudaMemcpy(&e, h->d_tcerr, sizeof(int), cudaMemcpyDeviceToHost));
+    if (e) {
+        CK(cudaMemset(h->d_tcerr, 0, sizeof(int)));
+        h->err = e == 2 ? "tensor-core operator: dynamic shared memory not 16-byte aligned"
+                        : "tensor-core operator: wait for MMA completion timed out";
+        return TOSP_ERR_TIMEOUT;
+    }
+    return TOSP_OK;
+}
+
 int need_setup(tosp_handle *h) {
     if (!h->setup_done) {
         h->err = "tosp_setup_gmg must be called first (densities/hierarchy missing)";
@@ -717,6 +744,7 @@ int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
     if (relres_out) *relres_out = nr;
     h->stats.it = it;
     h->stats.relres = nr;
+    TRY(check_tc(h));
     return rc;
 }
 
@@ -850,6 +878,28 @@ int tosp_kelem_prod(tosp_handle *h, const double *x, double *y, int64_t nfree) {
     return sync(h);
 }
 
+int tosp_kelem_prod_mixed(tosp_handle *h, const double *x, double *y, int64_t nfree) {
+    if (!h || !x || !y) return TOSP_ERR_BAD_ARG;
+    cudaSetDevice(h->device);
+    if (h->precision != TOSP_PREC_MIXED) {
+        h->err = "the FP32/BF16 operator exists only on TOSP_PREC_MIXED handles";
+        return TOSP_ERR_STATE;
+    }
+    TRY(check_len(h, nfree, h->nfree, "x"));
+    TRY(need_setup(h));
+    Level &F = h->lev[0];
+    const int64_t nd = F.g.ndof;
+    TRY(free_to_full(h, x, h->cd));
+    launch_convert<double, float>(h->cd, (float *)F.x, nd, h->stream);
+    CKL();
+    TRY(fine_apply<float>(h, (const float *)F.x, (float *)F.t));
+    launch_convert<float, double>((const float *)F.t, h->cq, nd, h->stream);
+    CKL();
+    TRY(full_to_free(h, h->cq, y));
+    TRY(sync(h));
+    return check_tc(h);
+}
+
 int tosp_mg_cycle(tosp_handle *h, const double *r, double *s, int64_t nfree) {
     if (!h || !r || !s) return TOSP_ERR_BAD_ARG;
     cudaSetDevice(h->device);
@@ -859,7 +909,8 @@ int tosp_mg_cycle(tosp_handle *h, const double *r, double *s, int64_t nfree) {
     TRY(free_to_full(h, r, h->cr));
     TRY(precondition(h, h->cr, h->cs));
     TRY(full_to_free(h, h->cs, s));
-    return sync(h);
+    TRY(sync(h));
+    return check_tc(h);
 }
 
 int tosp_solve_mg(tosp_handle *h, double *x, const double *f, int64_t nfree, int32_t *it, double *relres) {
@@ -989,8 +1040,12 @@ int tosp_time_operator(tosp_handle *h, int32_t precision, int32_t reps, double *
             Level &F = h->lev[0];
             CK(cudaMemsetAsync(F.t, 0, sizeof(float) * g0.ndof, h->stream));
             CK(cudaEventRecord(a, h->stream));
-            launch_fine_apply<float, __nv_bfloat16>((const float *)F.x, (float *)F.t, h->d_wbf, F.fm, h->d_kt32,
-                                                    h->fg, h->n, h->stream);
+            if (h->d_tcimg)
+                launch_fine_apply_tc((const float *)F.x, (float *)F.t, h->d_wbf, F.fm, h->d_tcimg, h->fg, h->d_tcerr,
+                                     h->stream);
+            else
+                launch_fine_apply<float, __nv_bfloat16>((const float *)F.x, (float *)F.t, h->d_wbf, F.fm, h->d_kt32,
+                                                        h->fg, h->n, h->stream);
         }
         CKL();
         CK(cudaEventRecord(b, h->stream));
@@ -1002,7 +1057,7 @@ int tosp_time_operator(tosp_handle *h, int32_t precision, int32_t reps, double *
     cudaEventDestroy(a);
     cudaEventDestroy(b);
     *ms_per_launch = total / reps;
-    return TOSP_OK;
+    return check_tc(h);
 }
 
 int tosp_elem_stiff_mr(double el, double eh, double ew, double nu, int32_t n, double *kv) {

@@ -113,6 +113,12 @@ int fine_nsp(int n, int elem_bytes);
 // The operator's block table from the row-major packed blocks (n = 2: the
 // Walsh-Hadamard modes; otherwise pair-major with stride fine_nsp).
 void fine_block_table(const std::vector<double> &packed_rowmajor, int n, int elem_bytes, std::vector<double> &kt);
+// Tensor-core finest operator of the mixed V-cycle (MR factor 2): B operand
+// image (BF16 pieces of the blocks, canonical shared-memory layout) and launch.
+void fine_tc_image(const std::vector<double> &packed_rowmajor, std::vector<uint16_t> &img);
+size_t fine_tc_image_bytes();
+void launch_fine_apply_tc(const float *x, float *y, const __nv_bfloat16 *w, const uint8_t *fm, const void *bimg,
+                          const FineGeom &fg, int *err, cudaStream_t st);
 
 // Sensitivities g0 (I/Grad.m:24-49), zero for elements not in freeDensG.
 void launch_grad(const double *u, const double *rho, const uint8_t *free_elem, const double *kepack,

@@ -79,6 +79,7 @@ def _load():
         "tosp_set_freedofs": (C.c_int, [C.c_void_p, P(C.c_int64), C.c_int64]),
         "tosp_setup_gmg": (C.c_int, [C.c_void_p, d, C.c_int64]),
         "tosp_kelem_prod": (C.c_int, [C.c_void_p, d, d, C.c_int64]),
+        "tosp_kelem_prod_mixed": (C.c_int, [C.c_void_p, d, d, C.c_int64]),
         "tosp_mg_cycle": (C.c_int, [C.c_void_p, d, d, C.c_int64]),
         "tosp_solve_mg": (C.c_int, [C.c_void_p, d, d, C.c_int64, P(C.c_int32), P(C.c_double)]),
         "tosp_grad": (C.c_int, [C.c_void_p, d, C.c_int64, d, d, C.c_int64]),
@@ -234,6 +235,14 @@ class Solver:
         x = np.ascontiguousarray(x, dtype=np.float64)
         y = np.empty_like(x)
         self._check(_lib.tosp_kelem_prod(self.h, _ptr(x), _ptr(y), x.size))
+        return y
+
+    def KelemProdMixed(self, x):
+        """K(rho) x by the mixed V-cycle's finest operator (FP32 vectors, BF16
+        SIMP factors; tensor-core element matrices for MR factor 2)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty_like(x)
+        self._check(_lib.tosp_kelem_prod_mixed(self.h, _ptr(x), _ptr(y), x.size))
         return y
 
     def MGCycle(self, r):
