@@ -10,14 +10,15 @@
 // 300 (n^3 + 2) FMAs per element instead of 600 n^3 for block-by-block
 // products.  A persistent CTA walks
 // element bricks of BX x BY x BZ: it stages the brick's nodal values in
-// shared memory, each thread forms one element's 24 outputs into shared slots,
-// every brick node then gathers the contributions of its (up to 8) elements,
-// and the result is written with plain stores for nodes only this brick
-// touches and atomics on the brick faces.
+// shared memory, each thread forms one element's 24 outputs, the outputs are
+// summed into the brick's nodes corner by corner (brick.cuh), and the result
+// is written with plain stores for nodes only this brick touches and atomics
+// on the brick faces.
 #include <cuda_bf16.h>
 
 #include <utility>
 
+#include "brick.cuh"
 #include "mr2_pattern.h"
 #include "tosp_internal.h"
 
@@ -26,9 +27,6 @@ namespace tosp {
 __device__ __forceinline__ float wval(__nv_bfloat16 v) { return __bfloat162float(v); }
 __device__ __forceinline__ double wval(double v) { return v; }
 __device__ __forceinline__ float wval(float v) { return v; }
-
-__device__ __forceinline__ void atomic_add(double *p, double v) { atomicAdd(p, v); }
-__device__ __forceinline__ void atomic_add(float *p, float v) { atomicAdd(p, v); }
 
 template <typename T> struct Vec;
 template <> struct Vec<float> { using type = float4; static constexpr int W = 4; };
@@ -146,16 +144,17 @@ template <typename T, int N> struct FineShape {
     static constexpr int KT_LEN = (N == 2) ? mr2_off(KE_PACK, Vec<T>::W) : KE_PACK * NSP;
 };
 
-// Operator: persistent CTAs over element bricks; see the file header.
+// Operator: persistent CTAs over element bricks; see the file header.  The
+// FP64 MR-2 instance is held to 168 registers so that three CTAs fit an SM.
 template <typename T, typename TW, int N>
-__global__ void __launch_bounds__(BRICK_ELEMS)
+__global__ void __launch_bounds__(BRICK_ELEMS, (sizeof(T) == 8 && N == 2) ? 3 : 1)
 k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ w,
              const uint8_t *__restrict__ freemask, const T *__restrict__ ktg, FineGeom fg) {
     constexpr int NS = FineShape<T, N>::NS, NSP = FineShape<T, N>::NSP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     T *kt = reinterpret_cast<T *>(smem_raw);               // KE_PACK * NSP (pair-major)
     T *xs = kt + FineShape<T, N>::KT_LEN;                   // BRICK_NODES * 3
-    T *eo = xs + BRICK_NODES * 3;                           // 24 * BRICK_ELEMS element outputs
+    T *ys = xs + BRICK_NODES * 3;                           // BRICK_NODES * 3 node sums
     const int tid = threadIdx.x;
     for (int i = tid; i < FineShape<T, N>::KT_LEN; i += BRICK_ELEMS) kt[i] = ktg[i];
 
@@ -167,7 +166,7 @@ k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ 
         const int bbx = (int)((brick / fg.nby) % fg.nbx);
         const int bbz = (int)(brick / ((int64_t)fg.nby * fg.nbx));
         const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
-        __syncthreads();   // previous brick done with xs/eo (and kt loaded)
+        __syncthreads();   // previous brick done with xs/ys (and kt loaded)
         for (int i = tid; i < BRICK_NODES * 3; i += BRICK_ELEMS) {
             const int ln = i / 3, c = i - 3 * ln;
             const int ny_ = ln % NBY, nx_ = (ln / NBY) % NBX, nz_ = ln / (NBY * NBX);
@@ -175,6 +174,7 @@ k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ 
             T v = T(0);
             if (gx < g.nx && gy < g.ny && gz < g.nz) v = x[3 * (((int64_t)gz * g.nx + gx) * g.ny + gy) + c];
             xs[i] = v;
+            ys[i] = T(0);
         }
         __syncthreads();
 
@@ -223,32 +223,8 @@ k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ 
                 all_pairs<T, NSP>(kt, wv, u, acc, std::make_integer_sequence<int, KE_PACK>{});
             }
         }
-        // element outputs -> per-element slots, then every node gathers the
-        // (up to 8) contributions of the brick's elements around it
-#pragma unroll
-        for (int k = 0; k < 24; ++k) eo[k * BRICK_ELEMS + tid] = acc[k];
-        __syncthreads();
-        for (int i = tid; i < BRICK_NODES * 3; i += BRICK_ELEMS) {
-            const int ln = i / 3, c = i - 3 * ln;
-            const int ny_ = ln % NBY, nx_ = (ln / NBY) % NBX, nz_ = ln / (NBY * NBX);
-            const int gx = ex0 + nx_, gy = ey0 + ny_, gz = ez0 + nz_;
-            if (gx < g.nx && gy < g.ny && gz < g.nz) {
-                const int64_t dof = 3 * (((int64_t)gz * g.nx + gx) * g.ny + gy) + c;
-                if (freemask[dof]) {
-                    T v = T(0);
-#pragma unroll
-                    for (int a = 0; a < 8; ++a) {
-                        const int dx = (a >> 1) & 1, dy = a & 1, dz = (a >> 2) & 1;
-                        const int ex_ = nx_ - dx, ey_ = ny_ - dy, ez_ = nz_ - dz;
-                        if (ex_ >= 0 && ex_ < BX && ey_ >= 0 && ey_ < BY && ez_ >= 0 && ez_ < BZ)
-                            v += eo[(3 * a + c) * BRICK_ELEMS + (ez_ * BX + ex_) * BY + ey_];
-                    }
-                    const bool inner = nx_ > 0 && nx_ < BX && ny_ > 0 && ny_ < BY && nz_ > 0 && nz_ < BZ;
-                    if (inner) y[dof] = v;
-                    else atomic_add(&y[dof], v);
-                }
-            }
-        }
+        brick_accumulate(ys, acc, valid, brick_base_node(tid));
+        brick_writeout(ys, y, freemask, g, ex0, ey0, ez0, tid);
     }
 }
 
@@ -325,7 +301,7 @@ void fine_block_table(const std::vector<double> &packed_rowmajor, int n, int ele
 template <typename T, typename TW, int N>
 static void launch_fine_t(const T *x, T *y, const TW *w, const uint8_t *fm, const T *kt, const FineGeom &fg,
                           cudaStream_t st) {
-    const size_t smem = sizeof(T) * (FineShape<T, N>::KT_LEN + BRICK_NODES * 3 + 24 * BRICK_ELEMS);
+    const size_t smem = sizeof(T) * (FineShape<T, N>::KT_LEN + 2 * BRICK_NODES * 3);
     auto kern = k_fine_apply<T, TW, N>;
     static int attr_dev = -1;
     int dev = 0;

@@ -2,27 +2,30 @@
 // element-matrix formation on the 5th-generation tensor cores.
 //
 // y_e = K_e u_e with K_e = sum_s w_s KE_s (I/WOK/KelemProd.m:57-100).  For a
-// brick of 128 elements the 300 packed entries of every K_e form one GEMM,
+// brick of 128 elements the 300 packed entries of every K_e form one GEMM
+// (M = 128 elements, N = 300 entries, kind::f16, FP32 accumulator):
 //
-//     D[e][t] = sum_k A[e][k] B[t][k],   A[e][8q+s] = w_s(e),
-//                                        B[t][8q+s] = piece q of KE_s[t],
+//     D[e][t] = sum_k A[e][k] B1[t][k] + sum_k A[e][k] B2[t][k],
+//     A[e][.] = (w_0..w_7, w_0..w_7),  B1[t][.] = (hi_s, mid_s),  B2[t][.] = (lo_s, 0)
 //
-// with q = 0..2 the three BF16 pieces of each FP64 block value (hi, mid, lo;
-// their sum carries 24 significant bits) and k = 24..31 zero.  The BF16 SIMP
-// factors are exact in the A operand and every product of two BF16 values is
-// exact, so D equals the FP32 formation of the CUDA-core kernel up to the
-// order of the FP32 accumulation.  D lands in tensor memory (one lane per
-// element, one column per entry); each thread reads its lane back in 32-column
-// slices and applies y_i += k u_j, y_j += k u_i on the CUDA cores (576 FMAs per
-// element instead of the 2148 of the Walsh-Hadamard CUDA-core formation).
+// where hi/mid/lo are the three BF16 pieces of the FP64 block value KE_s[t]
+// (their sum carries 24 significant bits).  The BF16 SIMP factors are exact
+// in A and every product of two BF16 values is exact, so D is the FP32
+// formation of K_e up to the order of the FP32 accumulation.  D lands in
+// tensor memory (one lane per element, one column per entry); each thread
+// reads its lane back in 32-column slices and applies y_i += k u_j,
+// y_j += k u_i on the CUDA cores (576 FMAs per element instead of the 2148 of
+// the Walsh-Hadamard CUDA-core formation).
 //
-// The entries are formed in three column chunks (128, 128, 48) through a
-// 128-column tensor-memory allocation, so four CTAs share an SM's 512 columns;
-// the dynamic shared memory per CTA is padded so that no fifth CTA can become
-// resident and wait for columns.  Brick staging, the per-element output slots
-// and the node gather with face atomics are those of the CUDA-core kernel.
-// Every wait on the MMA-completion barrier is bounded; a timeout sets *err,
-// leaves the brick loop and still frees the tensor memory.
+// Pipelining inside a CTA: the next brick's nodal values and factors are
+// staged with cp.async while the current brick computes; the entries are
+// formed in 64-column chunks through two tensor-memory buffers, so the MMA of
+// chunk c+1 runs while the threads consume chunk c.  Each CTA allocates 128
+// tensor-memory columns; the dynamic shared memory per CTA is padded so that
+// at most four CTAs (512 columns) are resident on an SM.  Every wait on an
+// MMA-completion barrier is bounded; a timeout sets *err, leaves the brick
+// loop and still frees the tensor memory.  Node sums and the write-out are
+// those of the CUDA-core kernel (brick.cuh).
 #include <cuda_bf16.h>
 
 #include <cstdint>
@@ -30,26 +33,31 @@
 #include <utility>
 #include <vector>
 
+#include "brick.cuh"
 #include "tosp_internal.h"
 
 namespace tosp {
 
 namespace {
 
-constexpr int TC_K = 32;                      // 3 BF16 pieces x 8 sub-cubes + 8 zero columns
-constexpr int TC_ROWS_B = 304;                // 300 entries padded to a multiple of 16
-constexpr int TC_ROW_BYTES = TC_K * 2;        // 64 B per K-major row
-constexpr int TC_B_BYTES = TC_ROWS_B * TC_ROW_BYTES;          // 19456
-constexpr int TC_A_BYTES = BRICK_ELEMS * TC_ROW_BYTES;        // 8192
-constexpr int TC_COLS = 128;                  // tensor-memory columns per CTA
-constexpr int TC_CTAS_PER_SM = 4;             // 4 x 128 = 512 columns
-constexpr uint32_t TC_WAIT_LIMIT = 1u << 22;  // try_wait rounds before giving up
+constexpr int TC_K = 16;                              // K of every MMA (kind::f16)
+constexpr int TC_ROWS_B = 304;                        // 300 entries padded to a multiple of 16
+constexpr int TC_GROUP = 8 * TC_K * 2;                // bytes of one 8-row group (256)
+constexpr int TC_B_TILE = TC_ROWS_B / 8 * TC_GROUP;   // 9728 per B tile
+constexpr int TC_B_BYTES = 2 * TC_B_TILE;             // B1 then B2
+constexpr int TC_A_BYTES = BRICK_ELEMS / 8 * TC_GROUP;        // 4096 per A buffer
+constexpr int TC_XS_FLOATS = (BRICK_NODES * 3 + 3) / 4 * 4;   // 676
+constexpr int TC_COLS = 128;                          // tensor-memory columns per CTA (2 x 64)
+constexpr int TC_CHUNK = 64;
+constexpr int TC_NCHUNK = 5;                          // 4 x 64 + 48 columns
+constexpr int TC_CTAS_PER_SM = 4;                     // 4 x 128 = 512 columns
+constexpr uint32_t TC_WAIT_LIMIT = 1u << 22;          // try_wait rounds before giving up
 
-// Canonical no-swizzle K-major layout: 8-row x 16-byte core matrices, core
-// matrices adjacent in K 128 B apart (leading byte offset), 8-row groups
-// 512 B apart (stride byte offset).
+// Canonical no-swizzle K-major layout with K = 16: 8-row x 16-byte core
+// matrices, the two core matrices of a row group 128 B apart (leading byte
+// offset), 8-row groups 256 B apart (stride byte offset).
 __host__ __device__ constexpr int tc_offset(int row, int k) {
-    return (row >> 3) * 512 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
+    return (row >> 3) * TC_GROUP + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
 }
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -58,11 +66,11 @@ __device__ __forceinline__ uint32_t smem_u32(const void *p) {
 
 __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
     uint64_t d = 0;
-    d |= (uint64_t)((addr >> 4) & 0x3FFF);          // start address
-    d |= (uint64_t)((128 >> 4) & 0x3FFF) << 16;     // leading byte offset (K direction)
-    d |= (uint64_t)((512 >> 4) & 0x3FFF) << 32;     // stride byte offset (M/N direction)
-    d |= (uint64_t)1 << 46;                         // descriptor version for sm_100
-    return d;                                       // base offset 0, no swizzle
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);               // start address
+    d |= (uint64_t)((128 >> 4) & 0x3FFF) << 16;          // leading byte offset (K direction)
+    d |= (uint64_t)((TC_GROUP >> 4) & 0x3FFF) << 32;     // stride byte offset (M/N direction)
+    d |= (uint64_t)1 << 46;                              // descriptor version for sm_100
+    return d;                                            // base offset 0, no swizzle
 }
 
 // kind::f16 instruction descriptor: FP32 accumulator, BF16 A and B, both
@@ -102,6 +110,16 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
 
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 4-byte asynchronous global -> shared copy; nbytes = 0 zero-fills.
+__device__ __forceinline__ void cp_async4(void *dst, const void *src, int nbytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(nbytes)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
     asm volatile(
@@ -146,126 +164,161 @@ __device__ __forceinline__ void slice_steps(const uint32_t (&r)[32], const float
     (entry_step<T0 + J>(__uint_as_float(r[J]), u, acc), ...);
 }
 
-// Read the chunk's columns of this thread's lane and apply them.
+// Read NC columns of this thread's lane (entries T0..T0+NC-1) and apply them.
 template <int T0, int NC>
-__device__ __forceinline__ void consume_chunk(uint32_t tlane, const float (&u)[24], float (&acc)[24]) {
+__device__ __forceinline__ void consume(uint32_t taddr, const float (&u)[24], float (&acc)[24]) {
     uint32_t r[32];
     if constexpr (NC >= 32) {
-        tmem_ld32(tlane, r);
+        tmem_ld32(taddr, r);
         slice_steps<T0>(r, u, acc, std::make_integer_sequence<int, 32>{});
-        if constexpr (NC > 32) consume_chunk<T0 + 32, NC - 32>(tlane + 32, u, acc);
+        if constexpr (NC > 32) consume<T0 + 32, NC - 32>(taddr + 32, u, acc);
     } else {
         static_assert(NC == 16, "chunk tails are 16 columns");
-        tmem_ld16(tlane, r);
+        tmem_ld16(taddr, r);
         slice_steps<T0>(r, u, acc, std::make_integer_sequence<int, 16>{});
     }
 }
 
+template <int C>
+__device__ __forceinline__ void consume_chunk(uint32_t taddr, const float (&u)[24], float (&acc)[24]) {
+    consume<C * TC_CHUNK, (C < TC_NCHUNK - 1) ? TC_CHUNK : TC_ROWS_B - C * TC_CHUNK>(taddr, u, acc);
+}
+
+// MMAs of chunk c into tensor-memory buffer (c & 1), then commit to its barrier.
+__device__ __forceinline__ void issue_chunk(int c, uint32_t tmem, uint32_t a_addr, uint32_t b_addr, uint32_t mbar) {
+    const int row0 = c * TC_CHUNK;
+    const int nc = (c < TC_NCHUNK - 1) ? TC_CHUNK : TC_ROWS_B - row0;
+    const uint32_t d = tmem + (uint32_t)((c & 1) * TC_CHUNK);
+    const uint64_t ad = smem_desc(a_addr);
+    const uint32_t boff = (uint32_t)((row0 >> 3) * TC_GROUP);
+    mma_bf16(d, ad, smem_desc(b_addr + boff), idesc_bf16(nc), 0u);
+    mma_bf16(d, ad, smem_desc(b_addr + TC_B_TILE + boff), idesc_bf16(nc), 1u);
+    mma_commit(mbar);
+}
+
 }  // namespace
 
-// Dynamic shared memory: B image, A tile, brick nodes, element output slots;
-// padded so that at most four CTAs fit on an SM (228 KB, 1 KB reserved per
-// CTA): 4 x 53.1 KB fit, 5 do not.  The MMA operands need 16-byte aligned
-// starts; the barrier and the tensor-memory address are static (8-byte
-// aligned) shared variables.
+// Dynamic shared memory: B image, two A buffers, two node-input buffers, the
+// node sums; padded so that at most four CTAs fit on an SM (228 KB with 1 KB
+// reserved per CTA: 4 x 53.1 KB fit, 5 do not).  The MMA operands need
+// 16-byte aligned starts; the barriers and the tensor-memory address are
+// static (8-byte aligned) shared variables.
 constexpr size_t TC_OFF_A = TC_B_BYTES;
-constexpr size_t TC_OFF_XS = TC_OFF_A + TC_A_BYTES;
-constexpr size_t TC_OFF_EO = TC_OFF_XS + sizeof(float) * ((BRICK_NODES * 3 + 3) / 4 * 4);
-constexpr size_t TC_SMEM_USED = TC_OFF_EO + sizeof(float) * 24 * BRICK_ELEMS;
+constexpr size_t TC_OFF_XS = TC_OFF_A + 2 * TC_A_BYTES;
+constexpr size_t TC_OFF_YS = TC_OFF_XS + sizeof(float) * 2 * TC_XS_FLOATS;
+constexpr size_t TC_SMEM_USED = TC_OFF_YS + sizeof(float) * TC_XS_FLOATS;
 constexpr size_t TC_SMEM = 52 * 1024;
-static_assert(TC_OFF_A % 16 == 0 && TC_OFF_XS % 16 == 0 && TC_OFF_EO % 16 == 0, "operand alignment");
+static_assert(TC_OFF_A % 16 == 0 && TC_OFF_XS % 16 == 0 && TC_OFF_YS % 16 == 0, "operand alignment");
 static_assert(TC_SMEM_USED <= TC_SMEM, "tensor-core operator shared memory");
+static_assert(TC_ROWS_B - (TC_NCHUNK - 1) * TC_CHUNK == 48, "last chunk");
+
+// Stage brick `brick` (nodal values, A rows) into buffer `buf` with cp.async.
+__device__ __forceinline__ void stage_brick(int64_t brick, int buf, const float *__restrict__ x,
+                                            const __nv_bfloat16 *__restrict__ w, const FineGeom &fg,
+                                            unsigned char *smem, int tid) {
+    const Grid &g = fg.g;
+    const int bby = (int)(brick % fg.nby);
+    const int bbx = (int)((brick / fg.nby) % fg.nbx);
+    const int bbz = (int)(brick / ((int64_t)fg.nby * fg.nbx));
+    const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
+    float *xs = reinterpret_cast<float *>(smem + TC_OFF_XS) + buf * TC_XS_FLOATS;
+    for (int i = tid; i < BRICK_NODES * 3; i += BRICK_ELEMS) {
+        const int ln = i / 3, c = i - 3 * ln;
+        const int ny_ = ln % NBY, nx_ = (ln / NBY) % NBX, nz_ = ln / (NBY * NBX);
+        const int gx = ex0 + nx_, gy = ey0 + ny_, gz = ez0 + nz_;
+        const bool in = gx < g.nx && gy < g.ny && gz < g.nz;
+        const float *src = in ? x + 3 * (((int64_t)gz * g.nx + gx) * g.ny + gy) + c : x;
+        cp_async4(xs + i, src, in ? 4 : 0);
+    }
+    const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
+    const int ex = ex0 + lx, ey = ey0 + ly, ez = ez0 + lz;
+    const bool valid = ex < g.nelx && ey < g.nely && ez < g.nelz;
+    unsigned char *ar = smem + TC_OFF_A + buf * TC_A_BYTES + tc_offset(tid, 0);
+#pragma unroll
+    for (int s = 0; s < 8; s += 2) {
+        // sub-cubes s and s+1 differ in y only: adjacent in the density mesh
+        const int sx = (s >> 1) & 1, sz = s >> 2;
+        const __nv_bfloat16 *src =
+            valid ? w + ((int64_t)(ez * 2 + sz) * fg.nelx_d + (ex * 2 + sx)) * fg.nely_d + ey * 2 : w;
+        cp_async4(ar + 2 * s, src, valid ? 4 : 0);
+        cp_async4(ar + 128 + 2 * s, src, valid ? 4 : 0);
+    }
+}
 
 __global__ void __launch_bounds__(BRICK_ELEMS, TC_CTAS_PER_SM)
 k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_bfloat16 *__restrict__ w,
                  const uint8_t *__restrict__ freemask, const uint4 *__restrict__ bimg, FineGeom fg,
                  int *__restrict__ err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char *bs = smem_raw;                                   // B image (canonical layout)
-    unsigned char *as = smem_raw + TC_OFF_A;                        // A tile (canonical layout)
-    float *xs = reinterpret_cast<float *>(smem_raw + TC_OFF_XS);    // BRICK_NODES * 3
-    float *eo = reinterpret_cast<float *>(smem_raw + TC_OFF_EO);    // 24 * BRICK_ELEMS
-    __shared__ __align__(8) uint64_t s_mbar;
+    float *ys = reinterpret_cast<float *>(smem_raw + TC_OFF_YS);    // BRICK_NODES * 3 node sums
+    __shared__ __align__(8) uint64_t s_mbar[2];
     __shared__ __align__(8) uint32_t s_tmem;
     __shared__ int s_fail;
-    uint64_t *mbar = &s_mbar;
-    uint32_t *tmem_holder = &s_tmem;
 
     const int tid = threadIdx.x, warp = tid >> 5;
     if (smem_u32(smem_raw) & 15u) {   // operand tiles need 16-byte aligned starts
         if (tid == 0) atomicExch(err, 2);
         return;
     }
-    for (int i = tid; i < TC_B_BYTES / 16; i += BRICK_ELEMS) reinterpret_cast<uint4 *>(bs)[i] = bimg[i];
+    for (int i = tid; i < TC_B_BYTES / 16; i += BRICK_ELEMS) reinterpret_cast<uint4 *>(smem_raw)[i] = bimg[i];
     if (tid == 0) {
         s_fail = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(mbar)) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar[0])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar[1])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_holder)),
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
                      "r"(TC_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    fence_async_smem();
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tmem = *tmem_holder;
-    const uint32_t tlane = tmem + ((uint32_t)(warp * 32) << 16);    // this warp's 32 lanes, column 0
-    const uint32_t mbar_a = smem_u32(mbar);
-    const uint32_t a_base = smem_u32(as), b_base = smem_u32(bs);
-    uint32_t phase = 0;
+    const uint32_t tmem = s_tmem;
+    const uint32_t tlane = tmem + ((uint32_t)(warp * 32) << 16);    // this warp's 32 lanes
+    const uint32_t mbar0 = smem_u32(&s_mbar[0]), mbar1 = smem_u32(&s_mbar[1]);
+    const uint32_t b_addr = smem_u32(smem_raw);
+    uint32_t ph0 = 0, ph1 = 0;
 
     const Grid &g = fg.g;
     const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
+    const int ln0 = brick_base_node(tid);
 
-    for (int64_t brick = blockIdx.x; brick < fg.nbricks; brick += gridDim.x) {
+    int buf = 0;
+    if (blockIdx.x < fg.nbricks) stage_brick(blockIdx.x, 0, x, w, fg, smem_raw, tid);
+    cp_async_commit();
+    for (int64_t brick = blockIdx.x; brick < fg.nbricks; brick += gridDim.x, buf ^= 1) {
+        // the other buffers were last read by the previous brick, whose
+        // threads have all passed its chunk barriers
+        const int64_t next = brick + gridDim.x;
+        if (next < fg.nbricks) stage_brick(next, buf ^ 1, x, w, fg, smem_raw, tid);
+        cp_async_commit();
+        cp_async_wait_1();   // this brick's copies are complete
+        fence_async_smem();
+        __syncthreads();     // also: every thread is done with the previous write-out
+
         const int bby = (int)(brick % fg.nby);
         const int bbx = (int)((brick / fg.nby) % fg.nbx);
         const int bbz = (int)(brick / ((int64_t)fg.nby * fg.nbx));
         const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
-        __syncthreads();   // previous brick done with xs / eo / A
-        for (int i = tid; i < BRICK_NODES * 3; i += BRICK_ELEMS) {
-            const int ln = i / 3, c = i - 3 * ln;
-            const int ny_ = ln % NBY, nx_ = (ln / NBY) % NBX, nz_ = ln / (NBY * NBX);
-            const int gx = ex0 + nx_, gy = ey0 + ny_, gz = ez0 + nz_;
-            float v = 0.f;
-            if (gx < g.nx && gy < g.ny && gz < g.nz) v = x[3 * (((int64_t)gz * g.nx + gx) * g.ny + gy) + c];
-            xs[i] = v;
-        }
-        const int ex = ex0 + lx, ey = ey0 + ly, ez = ez0 + lz;
-        const bool valid = ex < g.nelx && ey < g.nely && ez < g.nelz;
-        // A row of this element: the 8 sub-cube factors three times, then zeros
-        {
-            uint32_t wp[4] = {0u, 0u, 0u, 0u};
-            if (valid) {
-#pragma unroll
-                for (int s = 0; s < 8; s += 2) {
-                    const int sx = (s >> 1) & 1, sz = s >> 2;
-                    // sub-cubes s and s+1 differ in y only: adjacent in the density mesh
-                    const int64_t di = ((int64_t)(ez * 2 + sz) * fg.nelx_d + (ex * 2 + sx)) * fg.nely_d + ey * 2;
-                    const unsigned short lo = __bfloat16_as_ushort(w[di]);
-                    const unsigned short hi = __bfloat16_as_ushort(w[di + 1]);
-                    wp[s >> 1] = (uint32_t)lo | ((uint32_t)hi << 16);
-                }
-            }
-            const uint4 row = make_uint4(wp[0], wp[1], wp[2], wp[3]);
-            unsigned char *ar = as + tc_offset(tid, 0);
-            *reinterpret_cast<uint4 *>(ar) = row;
-            *reinterpret_cast<uint4 *>(ar + 128) = row;
-            *reinterpret_cast<uint4 *>(ar + 256) = row;
-            *reinterpret_cast<uint4 *>(ar + 384) = make_uint4(0u, 0u, 0u, 0u);
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
+        const bool valid = ex0 + lx < g.nelx && ey0 + ly < g.nely && ez0 + lz < g.nelz;
+        const uint32_t a_addr = smem_u32(smem_raw + TC_OFF_A + buf * TC_A_BYTES);
+        const float *xs = reinterpret_cast<const float *>(smem_raw + TC_OFF_XS) + buf * TC_XS_FLOATS;
 
+        if (tid == 0) {
+            fence_after();
+            issue_chunk(0, tmem, a_addr, b_addr, mbar0);
+            issue_chunk(1, tmem, a_addr, b_addr, mbar1);
+        }
+        for (int i = tid; i < BRICK_NODES * 3; i += BRICK_ELEMS) ys[i] = 0.f;
         float u[24], acc[24];
 #pragma unroll
         for (int a = 0; a < 8; ++a) {
             const int dx = (a >> 1) & 1, dy = a & 1, dz = (a >> 2) & 1;
-            const int ln = ((lz + dz) * NBX + (lx + dx)) * NBY + (ly + dy);
+            const int ln = ln0 + (dz * NBX + dx) * NBY + dy;
 #pragma unroll
             for (int c = 0; c < 3; ++c) u[3 * a + c] = xs[3 * ln + c];
         }
@@ -274,31 +327,27 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
 
         bool ok = true;
 #pragma unroll
-        for (int chunk = 0; chunk < 3; ++chunk) {
-            const int row0 = chunk * 128;
-            const int nc = chunk < 2 ? 128 : 48;
-            if (tid == 0) {
-                fence_after();
-#pragma unroll
-                for (int ks = 0; ks < 2; ++ks) {
-                    const uint64_t ad = smem_desc(a_base + ks * 256);
-                    const uint64_t bd = smem_desc(b_base + (row0 >> 3) * 512 + ks * 256);
-                    mma_bf16(tmem, ad, bd, idesc_bf16(nc), ks);
-                }
-                mma_commit(mbar_a);
-            }
-            const bool got = mbar_wait(mbar_a, phase);
-            phase ^= 1u;
+        for (int c = 0; c < TC_NCHUNK; ++c) {
+            const bool got = (c & 1) ? mbar_wait(mbar1, ph1) : mbar_wait(mbar0, ph0);
+            if (c & 1) ph1 ^= 1u;
+            else ph0 ^= 1u;
             if (__syncthreads_or(!got)) {
                 ok = false;
                 break;
             }
             fence_after();
-            if (chunk == 0) consume_chunk<0, 128>(tlane, u, acc);
-            else if (chunk == 1) consume_chunk<128, 128>(tlane, u, acc);
-            else consume_chunk<256, 48>(tlane, u, acc);
+            const uint32_t taddr = tlane + (uint32_t)((c & 1) * TC_CHUNK);
+            if (c == 0) consume_chunk<0>(taddr, u, acc);
+            else if (c == 1) consume_chunk<1>(taddr, u, acc);
+            else if (c == 2) consume_chunk<2>(taddr, u, acc);
+            else if (c == 3) consume_chunk<3>(taddr, u, acc);
+            else consume_chunk<4>(taddr, u, acc);
             fence_before();
-            __syncthreads();   // all lanes read before the next chunk overwrites the columns
+            __syncthreads();   // buffer (c & 1) fully read
+            if (tid == 0 && c + 2 < TC_NCHUNK) {
+                fence_after();
+                issue_chunk(c + 2, tmem, a_addr, b_addr, (c & 1) ? mbar1 : mbar0);
+            }
         }
         if (!ok) {
             if (tid == 0) {
@@ -307,36 +356,17 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
             }
             break;
         }
-
-#pragma unroll
-        for (int k = 0; k < 24; ++k) eo[k * BRICK_ELEMS + tid] = valid ? acc[k] : 0.f;
-        __syncthreads();
-        for (int i = tid; i < BRICK_NODES * 3; i += BRICK_ELEMS) {
-            const int ln = i / 3, c = i - 3 * ln;
-            const int ny_ = ln % NBY, nx_ = (ln / NBY) % NBX, nz_ = ln / (NBY * NBX);
-            const int gx = ex0 + nx_, gy = ey0 + ny_, gz = ez0 + nz_;
-            if (gx < g.nx && gy < g.ny && gz < g.nz) {
-                const int64_t dof = 3 * (((int64_t)gz * g.nx + gx) * g.ny + gy) + c;
-                if (freemask[dof]) {
-                    float v = 0.f;
-#pragma unroll
-                    for (int a = 0; a < 8; ++a) {
-                        const int dx = (a >> 1) & 1, dy = a & 1, dz = (a >> 2) & 1;
-                        const int ex_ = nx_ - dx, ey_ = ny_ - dy, ez_ = nz_ - dz;
-                        if (ex_ >= 0 && ex_ < BX && ey_ >= 0 && ey_ < BY && ez_ >= 0 && ez_ < BZ)
-                            v += eo[(3 * a + c) * BRICK_ELEMS + (ez_ * BX + ex_) * BY + ey_];
-                    }
-                    const bool inner = nx_ > 0 && nx_ < BX && ny_ > 0 && ny_ < BY && nz_ > 0 && nz_ < BZ;
-                    if (inner) y[dof] = v;
-                    else atomicAdd(&y[dof], v);
-                }
-            }
-        }
+        brick_accumulate(ys, acc, valid, ln0);
+        brick_writeout(ys, y, freemask, g, ex0, ey0, ez0, tid);
     }
+    cp_async_wait_0();
 
-    // An MMA still in flight after a timeout gets one more bounded wait
-    // before its columns are released.
-    if (s_fail && tid == 0) mbar_wait(mbar_a, phase ^ 1u);
+    // MMAs still in flight after a timeout get one more bounded wait each
+    // before their columns are released.
+    if (s_fail && tid == 0) {
+        mbar_wait(mbar0, ph0);
+        mbar_wait(mbar1, ph1);
+    }
     fence_before();
     __syncthreads();
     fence_after();
@@ -344,9 +374,9 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_COLS) : "memory");
 }
 
-// B operand image for MR factor 2: row t (diagonal-major entry order) holds
-// the hi / mid / lo BF16 pieces of KE_s[t] for s = 0..7; rows 300..303 and
-// columns 24..31 are zero.
+// B operand image for MR factor 2: tile B1 row t (diagonal-major entry order)
+// holds the hi and mid BF16 pieces of KE_s[t] for s = 0..7, tile B2 the lo
+// pieces and zeros; rows 300..303 are zero.
 static uint16_t bf16_bits(double v) {
     const float f = (float)v;
     uint32_t u;
@@ -369,7 +399,8 @@ void fine_tc_image(const std::vector<double> &packed_rowmajor, std::vector<uint1
             double r = packed_rowmajor[(size_t)s * KE_PACK + rm];
             for (int q = 0; q < 3; ++q) {
                 const uint16_t b = bf16_bits(r);
-                img[tc_offset(t, 8 * q + s) / 2] = b;
+                const int off = q < 2 ? tc_offset(t, 8 * q + s) : TC_B_TILE + tc_offset(t, s);
+                img[off / 2] = b;
                 r -= bf16_value(b);
             }
         }
@@ -377,6 +408,29 @@ void fine_tc_image(const std::vector<double> &packed_rowmajor, std::vector<uint1
 }
 
 size_t fine_tc_image_bytes() { return TC_B_BYTES; }
+
+// Resident CTAs per SM from the device limits (shared memory with the
+// per-CTA reservation, registers at warp allocation granularity), capped by
+// the 512 tensor-memory columns.
+static int tc_ctas_per_sm() {
+    int dev = 0, smem_sm = 0, smem_res = 0, regs_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&smem_res, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, k_fine_apply_tc2) != cudaSuccess) {
+        cudaGetLastError();
+        return 1;
+    }
+    const size_t per_cta = TC_SMEM + fa.sharedSizeBytes + (size_t)smem_res;
+    const int by_smem = (int)(smem_sm / per_cta);
+    const int regs_warp = (fa.numRegs * 32 + 255) / 256 * 256;
+    const int by_regs = regs_sm / (regs_warp * (BRICK_ELEMS / 32));
+    int n = by_smem < by_regs ? by_smem : by_regs;
+    if (n > TC_CTAS_PER_SM) n = TC_CTAS_PER_SM;
+    return n < 1 ? 1 : n;
+}
 
 static int num_sms_tc() {
     static int n = 0;
@@ -390,18 +444,15 @@ static int num_sms_tc() {
 
 void launch_fine_apply_tc(const float *x, float *y, const __nv_bfloat16 *w, const uint8_t *fm, const void *bimg,
                           const FineGeom &fg, int *err, cudaStream_t st) {
-    static int attr_dev = -1;
+    static int attr_dev = -1, per_sm = 1;
     int dev = 0;
     cudaGetDevice(&dev);
     if (attr_dev != dev) {
         cudaFuncSetAttribute(k_fine_apply_tc2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+        cudaFuncSetAttribute(k_fine_apply_tc2, cudaFuncAttributePreferredSharedMemoryCarveout,
+                             (int)cudaSharedmemCarveoutMaxShared);
+        per_sm = tc_ctas_per_sm();
         attr_dev = dev;
-    }
-    static int per_sm = 0;
-    if (!per_sm) {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fine_apply_tc2, BRICK_ELEMS, TC_SMEM);
-        if (per_sm < 1) per_sm = 1;
-        if (per_sm > TC_CTAS_PER_SM) per_sm = TC_CTAS_PER_SM;   // 4 x 128 tensor-memory columns
     }
     int64_t grid = (int64_t)per_sm * num_sms_tc();
     if (grid > fg.nbricks) grid = fg.nbricks;
