@@ -215,15 +215,17 @@ def run_slp(args):
     torch.cuda.set_device(0)
     if args.slp == "config0":
         pb = P.cantilever(48, 24, 24)
-        n, prec, ngr, rmin, volfrac, iters, lp, omega = 1, tosp.PREC_FP64, 3, 1.5, 0.3, 20, "highs", 0.6
+        n, prec, ngr, rmin, volfrac, iters, lp, omega, cycle = 1, tosp.PREC_FP64, 3, 1.5, 0.3, 20, "highs", 0.6, 0
         prj = slp.PrjParams(op=False)
     else:
         pb = P.bridge(160, 80, 40)
-        n, prec, ngr, rmin, volfrac, iters, lp, omega = 3, tosp.PREC_MIXED, 4, 2.5 / 3, 0.2, 100, "knapsack", 0.5
+        # cycle and omega unspecified for this loop: the reference defaults
+        # (W-cycle, omega 0.5; I/TopOpt3D.m:172-174)
+        n, prec, ngr, rmin, volfrac, iters, lp, omega, cycle = 3, tosp.PREC_MIXED, 4, 2.5 / 3, 0.2, 100, "knapsack", 0.5, 1
         prj = slp.PrjParams(op=True)
     iters = args.slp_iters or iters
     lp = args.lp or lp
-    mg = tosp.default_mg(ngrids=ngr, cycle=0, omega=omega, smoothiter1=1, smoothiter2=1, tolMG=1e-8,
+    mg = tosp.default_mg(ngrids=ngr, cycle=cycle, omega=omega, smoothiter1=1, smoothiter2=1, tolMG=1e-8,
                          maxiterMG=2000, flexible=1 if prec == tosp.PREC_MIXED else 0)
     solver = tosp.Solver(pb, mg, precision=prec, mr_n=n, p=3.0, emin=1e-9, opfilter=1, rmin=rmin)
     timed = _Timed(solver)
@@ -243,7 +245,7 @@ def run_slp(args):
             "unit": "s/iteration", "higher_is_better": False, "n_gpus": 1, "data": "synthetic",
             "dtype": "f64" if prec == tosp.PREC_FP64 else "f64 outer CG / f32+bf16 V-cycle",
             "config": {"workload": args.slp, "mesh": [pb.nelx, pb.nely, pb.nelz], "mr_n": n, "volfrac": volfrac,
-                       "rmin": rmin, "lp": lp, "ngrids": ngr},
+                       "rmin": rmin, "lp": lp, "ngrids": ngr, "cycle": "VW"[cycle], "omega": omega},
             "slp": {"accepted": res.iters, "rejected": res.rejected, "opstop": res.opstop, "F_final": res.F,
                     "F_first": res.history[0]["F"] if res.history else None,
                     "pcg_iterations_total": int(sum(res.pcgit)), "wall_s": round(wall, 3)},
@@ -258,18 +260,19 @@ def run_slp(args):
         cw = CpuWok(pb, n, ngr, omega, nthreads=os.cpu_count())
         xf_final = solver.ApplyFilter(res.x)
         solver.SetupGMG(xf_final)
-        u_final = solver.SolveMG(res.u, pb.f)[0]
+        u_final, it_final, rr_final, rc_final = solver.SolveMG(res.u, pb.f)
         res.u = u_final
         cw.w = np.ascontiguousarray(1e-9 + (1 - 1e-9) * np.power(xf_final, 3))
         uf = np.zeros(3 * pb.nnodes)
         uf[pb.freedofs] = u_final
         r = pb.f_full() - cw.kelem(uf)
         line["cpu_check"] = {"relres_cpu_operator": float(np.linalg.norm(r[pb.freedofs]) / np.linalg.norm(pb.f)),
-                             "compliance": float(pb.f @ res.u)}
+                             "compliance": float(pb.f @ res.u), "final_solve_it": int(it_final),
+                             "final_solve_relres": float(rr_final), "final_solve_status": int(rc_final)}
     if args.check_cpu and args.slp == "config0":
         sys.path.insert(0, os.path.join(ROOT, "tests"))
         from oracle_solver import OracleSolver
-        orc = OracleSolver(pb, n=n, ngrids=ngr, cycle=0, omega=omega, rmin=rmin)
+        orc = OracleSolver(pb, n=n, ngrids=ngr, cycle=cycle, omega=omega, rmin=rmin)
         t1 = time.perf_counter()
         ro = slp.str_slp(orc, pb, volfrac, x0, slp.SlpParams(maxiter=iters, lp=lp), prj=prj)
         tcpu = time.perf_counter() - t1
@@ -304,7 +307,8 @@ def run_serving(args):
 
     def submit(srv, item):
         pb, n, x, ng = item
-        mg = tosp.default_mg(ngrids=ng, cycle=0, omega=W.REF_OMEGA, tolMG=1e-8, maxiterMG=1000, flexible=1,
+        # cycle and omega unspecified for the stream: the reference defaults
+        mg = tosp.default_mg(ngrids=ng, cycle=1, omega=W.REF_OMEGA, tolMG=1e-8, maxiterMG=1000, flexible=1,
                              maxstall=60)
         return srv.submit(pb, x, mg=mg, precision=tosp.PREC_MIXED, mr_n=n, p=3.0, emin=1e-9, opfilter=1,
                           rmin=1.0 if n > 1 else 1.5)
@@ -356,6 +360,7 @@ def run_serving(args):
             "data": "synthetic", "dtype": "f64 outer CG / f32+bf16 V-cycle",
             "config": {"workload": "serving stream seed 7", "requests": len(items), "slots": args.slots,
                        "hbm_budget_gb": args.budget_gb, "mesh_nx": list(W.SERVING_NX), "mr_n": [1, 2],
+                       "cycle": "W", "omega": W.REF_OMEGA,
                        "bc": list(W.SERVING_BC)},
             "rates": out, "clocks": clk}
     print(json.dumps(line))

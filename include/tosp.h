@@ -88,6 +88,10 @@ typedef struct tosp_mg_params {
                               TOSP_NOT_CONVERGED when the best relative residual has not
                               halved within k iterations (used by the serving loop to fall
                               back from a stalling mixed-precision solve)                    */
+    int32_t warp_stencil_max; /* coarse levels with at most this many nodes store their 27-point
+                              stencil node-major and apply it with one warp per node (small
+                              levels are latency-bound with one thread per node); 0: 65536,
+                              -1: never.  A tuning knob with no reference counterpart.       */
 } tosp_mg_params;
 
 /* Statistics of the last tosp_solve_mg call. */

@@ -97,14 +97,17 @@ def s_fp64_product(tosp_mod, pb, n, dens, x):
     return s.KelemProd(x)
 
 
+@pytest.mark.parametrize("wsm", [0, -1])
 @pytest.mark.parametrize("cycle", [0, 1, 2])
 @pytest.mark.parametrize("dims,n,ngrids", [((8, 4, 4), 2, 3), ((16, 8, 8), 1, 3), ((16, 8, 8), 1, 4),
                                            ((8, 8, 4), 3, 2)])
-def test_cycle_parity(tosp_mod, cycle, dims, n, ngrids):
+def test_cycle_parity(tosp_mod, cycle, dims, n, ngrids, wsm):
+    """One cycle against the oracle; wsm 0 applies these small coarse levels
+    warp per node (node-major stencils), -1 thread per node."""
     pb = P.cantilever(*dims)
     dens = make(pb, n, seed=7)
     ks, K, H = oracle_hier(pb, n, dens, ngrids, 0.6)
-    s = solver(tosp_mod, pb, n, ngrids=ngrids, cycle=cycle)
+    s = solver(tosp_mod, pb, n, ngrids=ngrids, cycle=cycle, warp_stencil_max=wsm)
     s.SetupGMG(dens)
     r = np.random.default_rng(2).standard_normal(pb.freedofs.size)
     z = s.MGCycle(r)

@@ -42,6 +42,53 @@ __device__ __forceinline__ void brick_accumulate(T *ys, const T (&acc)[24], bool
     }
 }
 
+constexpr int BRICK_SLOTS = BRICK_NODES * 3;
+
+// Per-CTA table of the brick's node-value slots (i = 3 * local node + c):
+// offset of slot i from the brick's first dof, and its local node coordinates
+// packed as bits 0-2 x, 3-6 y, 7-9 z, bit 10 set when only this brick touches
+// the node.  Built once per CTA; valid for every brick of the grid.
+__device__ __forceinline__ void brick_slots_init(int32_t *rel, uint16_t *pk, const Grid &g, int tid) {
+    for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) {
+        const int ln = i / 3, c = i - 3 * ln;
+        const int ny_ = ln % NBY, nx_ = (ln / NBY) % NBX, nz_ = ln / (NBY * NBX);
+        rel[i] = 3 * ((nz_ * g.nx + nx_) * g.ny + ny_) + c;
+        const bool inner = nx_ > 0 && nx_ < BX && ny_ > 0 && ny_ < BY && nz_ > 0 && nz_ < BZ;
+        pk[i] = (uint16_t)(nx_ | (ny_ << 3) | (nz_ << 7) | (inner ? 1 << 10 : 0));
+    }
+}
+
+// All nodes of the brick with first element (ex0, ey0, ez0) lie in the mesh.
+__device__ __forceinline__ bool brick_interior(int ex0, int ey0, int ez0, const Grid &g) {
+    return ex0 + BX < g.nx && ey0 + BY < g.ny && ez0 + BZ < g.nz;
+}
+
+__device__ __forceinline__ bool brick_slot_in(uint16_t p, int ex0, int ey0, int ez0, const Grid &g) {
+    return ex0 + (p & 7) < g.nx && ey0 + ((p >> 3) & 15) < g.ny && ez0 + ((p >> 7) & 7) < g.nz;
+}
+
+__device__ __forceinline__ int64_t brick_base_dof(int ex0, int ey0, int ez0, const Grid &g) {
+    return 3 * (((int64_t)ez0 * g.nx + ex0) * g.ny + ey0);
+}
+
+// Write-out through the slot table.
+template <typename T>
+__device__ __forceinline__ void brick_writeout_tab(const T *ys, T *__restrict__ y, const uint8_t *__restrict__ freemask,
+                                                   const Grid &g, int ex0, int ey0, int ez0, const int32_t *rel,
+                                                   const uint16_t *pk, int tid) {
+    const int64_t base = brick_base_dof(ex0, ey0, ez0, g);
+    const bool interior = brick_interior(ex0, ey0, ez0, g);
+    for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) {
+        const uint16_t p = pk[i];
+        if (!interior && !brick_slot_in(p, ex0, ey0, ez0, g)) continue;
+        const int64_t dof = base + rel[i];
+        if (freemask[dof]) {
+            if (p >> 10) y[dof] = ys[i];
+            else brick_atomic_add(&y[dof], ys[i]);
+        }
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void brick_writeout(const T *ys, T *__restrict__ y, const uint8_t *__restrict__ freemask,
                                                const Grid &g, int ex0, int ey0, int ez0, int tid) {

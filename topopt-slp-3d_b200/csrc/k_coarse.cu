@@ -167,7 +167,7 @@ void launch_coarse_from_coarse(const double *Af, const uint8_t *freemask_f, cons
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void k_assemble_stencil(const double *__restrict__ Ae, const uint8_t *__restrict__ fmask, Grid g,
-                                   T *__restrict__ stv, T *__restrict__ invdiag, double omega) {
+                                   T *__restrict__ stv, T *__restrict__ invdiag, double omega, int node_major) {
     for (int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; I < g.nnodes;
          I += (int64_t)gridDim.x * blockDim.x) {
         const int y = (int)(I % g.ny), x = (int)((I / g.ny) % g.nx), z = (int)(I / ((int64_t)g.ny * g.nx));
@@ -198,7 +198,8 @@ __global__ void k_assemble_stencil(const double *__restrict__ Ae, const uint8_t 
             for (int ci = 0; ci < 3; ++ci)
                 for (int cj = 0; cj < 3; ++cj) {
                     const double v = (fi[ci] && fj[cj]) ? blk[ci * 3 + cj] : 0.0;
-                    stv[(int64_t)(o * 9 + ci * 3 + cj) * g.nnodes + I] = (T)v;
+                    const int k = o * 9 + ci * 3 + cj;
+                    stv[node_major ? I * STENCIL_VALS + k : (int64_t)k * g.nnodes + I] = (T)v;
                     if (o == 13 && ci == cj) invdiag[3 * I + ci] = (T)((fi[ci] && v != 0.0) ? omega / v : 0.0);
                 }
         }
@@ -207,13 +208,15 @@ __global__ void k_assemble_stencil(const double *__restrict__ Ae, const uint8_t 
 
 template <typename T>
 void launch_assemble_stencil(const double *Ae, const uint8_t *freemask, const Grid &g, T *stencil, T *invdiag,
-                             double omega, cudaStream_t st) {
-    k_assemble_stencil<T><<<grid_for(g.nnodes, 128), 128, 0, st>>>(Ae, freemask, g, stencil, invdiag, omega); count_launch();
+                             double omega, bool node_major, cudaStream_t st) {
+    k_assemble_stencil<T><<<grid_for(g.nnodes, 128), 128, 0, st>>>(Ae, freemask, g, stencil, invdiag, omega,
+                                                                    node_major ? 1 : 0);
+    count_launch();
 }
 template void launch_assemble_stencil<double>(const double *, const uint8_t *, const Grid &, double *, double *,
-                                              double, cudaStream_t);
+                                              double, bool, cudaStream_t);
 template void launch_assemble_stencil<float>(const double *, const uint8_t *, const Grid &, float *, float *,
-                                             double, cudaStream_t);
+                                             double, bool, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // Stencil products.  One thread per node, 3 dofs.
@@ -250,15 +253,63 @@ k_stencil(const T *__restrict__ stv, const T *__restrict__ x, const T *__restric
     }
 }
 
+// Small levels: one warp per node over the node-major stencil.  Lane o < 27
+// applies offset o's 3x3 block (nine contiguous values: the warp reads the
+// node's 243 values as one contiguous run), then the warp sums the three
+// partial rows.
+template <typename T>
+__global__ void __launch_bounds__(256)
+k_stencil_warp(const T *__restrict__ stv, const T *__restrict__ x, const T *__restrict__ b,
+               const T *__restrict__ invdiag, T *__restrict__ y, Grid g, int mode) {
+    const int lane = threadIdx.x & 31;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t I = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; I < g.nnodes; I += nw) {
+        T a0 = 0, a1 = 0, a2 = 0;
+        if (lane < 27) {
+            const int yy = (int)(I % g.ny), xx = (int)((I / g.ny) % g.nx), zz = (int)(I / ((int64_t)g.ny * g.nx));
+            const int oy = lane % 3 - 1, ox = (lane / 3) % 3 - 1, oz = lane / 9 - 1;
+            const int jx = xx + ox, jy = yy + oy, jz = zz + oz;
+            if (jx >= 0 && jx < g.nx && jy >= 0 && jy < g.ny && jz >= 0 && jz < g.nz) {
+                const int64_t J = I + ((int64_t)oz * g.nx + ox) * g.ny + oy;
+                const T x0 = x[3 * J], x1 = x[3 * J + 1], x2 = x[3 * J + 2];
+                const T *s = stv + I * STENCIL_VALS + lane * 9;
+                a0 = s[0] * x0 + s[1] * x1 + s[2] * x2;
+                a1 = s[3] * x0 + s[4] * x1 + s[5] * x2;
+                a2 = s[6] * x0 + s[7] * x1 + s[8] * x2;
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+            a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+            a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+        }
+        if (lane < 3) {
+            const T a = lane == 0 ? a0 : (lane == 1 ? a1 : a2);
+            const int64_t d = 3 * I + lane;
+            if (mode == 0) y[d] = a;
+            else if (mode == 1) y[d] = b[d] - a;
+            else y[d] = x[d] + invdiag[d] * (b[d] - a);
+        }
+    }
+}
+
 template <typename T>
 void launch_stencil(const T *st_vals, const T *x, const T *b, const T *invdiag, T *y, const Grid &g, int mode,
-                    cudaStream_t st) {
-    k_stencil<T><<<grid_for(g.nnodes, 128), 128, 0, st>>>(st_vals, x, b, invdiag, y, g, mode); count_launch();
+                    bool node_major, cudaStream_t st) {
+    if (node_major) {
+        int64_t blocks = (g.nnodes + 7) / 8;   // 8 warps per block
+        if (blocks > 65535) blocks = 65535;
+        k_stencil_warp<T><<<(unsigned)blocks, 256, 0, st>>>(st_vals, x, b, invdiag, y, g, mode);
+    } else {
+        k_stencil<T><<<grid_for(g.nnodes, 128), 128, 0, st>>>(st_vals, x, b, invdiag, y, g, mode);
+    }
+    count_launch();
 }
 template void launch_stencil<double>(const double *, const double *, const double *, const double *, double *,
-                                     const Grid &, int, cudaStream_t);
+                                     const Grid &, int, bool, cudaStream_t);
 template void launch_stencil<float>(const float *, const float *, const float *, const float *, float *,
-                                    const Grid &, int, cudaStream_t);
+                                    const Grid &, int, bool, cudaStream_t);
 
 // ---------------------------------------------------------------------------
 // Elementwise smoother pieces for the matrix-free finest level.

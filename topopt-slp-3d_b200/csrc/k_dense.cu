@@ -148,8 +148,17 @@ __global__ void k_dense_gemv(const double *__restrict__ X, const T *__restrict__
     const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
     for (int64_t row = warp; row < n; row += nwarps) {
         const double *xr = X + row * npad;
-        double s = 0.0;
-        for (int64_t j = lane; j < n; j += 32) s += xr[j] * (double)b[j];
+        // four independent partial sums keep four loads per lane in flight
+        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+        int64_t j = lane;
+        for (; j + 96 < n; j += 128) {
+            s0 += xr[j] * (double)b[j];
+            s1 += xr[j + 32] * (double)b[j + 32];
+            s2 += xr[j + 64] * (double)b[j + 64];
+            s3 += xr[j + 96] * (double)b[j + 96];
+        }
+        for (; j < n; j += 32) s0 += xr[j] * (double)b[j];
+        double s = (s0 + s1) + (s2 + s3);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
         if (lane == 0) x[row] = (T)s;

@@ -144,10 +144,10 @@ template <typename T, int N> struct FineShape {
     static constexpr int KT_LEN = (N == 2) ? mr2_off(KE_PACK, Vec<T>::W) : KE_PACK * NSP;
 };
 
-// Operator: persistent CTAs over element bricks; see the file header.  The
-// FP64 MR-2 instance is held to 168 registers so that three CTAs fit an SM.
+// Operator: persistent CTAs over element bricks; see the file header.  Used
+// for the FP32/BF16 V-cycle operator (MR 1 and 3) and FP64 with MR 3.
 template <typename T, typename TW, int N>
-__global__ void __launch_bounds__(BRICK_ELEMS, (sizeof(T) == 8 && N == 2) ? 3 : 1)
+__global__ void __launch_bounds__(BRICK_ELEMS)
 k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ w,
              const uint8_t *__restrict__ freemask, const T *__restrict__ ktg, FineGeom fg) {
     constexpr int NS = FineShape<T, N>::NS, NSP = FineShape<T, N>::NSP;
@@ -226,6 +226,144 @@ k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ 
         brick_accumulate(ys, acc, valid, brick_base_node(tid));
         brick_writeout(ys, y, freemask, g, ex0, ey0, ez0, tid);
     }
+}
+
+// FP64 operator for MR factor 1 and 2 with staged inputs: the next brick's
+// nodal values and SIMP factors are copied into the second half of double
+// buffers with cp.async while the current brick computes, so the global-load
+// latency is hidden behind the element-matrix arithmetic (three CTAs per SM
+// leave too few warps to hide it otherwise).  Factors are stored s-major
+// (ws[s * BRICK_ELEMS + element]) so that both the copies and the reads are
+// conflict-free.  Node offsets come from the per-CTA slot table.
+__device__ __forceinline__ void cp_async8(void *dst, const void *src, int nbytes) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)),
+                 "l"(src), "r"(nbytes)
+                 : "memory");
+}
+
+template <int N>
+struct StagedLayout {
+    static constexpr int NS = N * N * N;
+    static constexpr int KT = (FineShape<double, N>::KT_LEN + 1) / 2 * 2;   // doubles, 16-byte multiple
+    static constexpr int XS = (BRICK_SLOTS + 1) / 2 * 2;                     // 676
+    static constexpr size_t OFF_XS = sizeof(double) * KT;
+    static constexpr size_t OFF_YS = OFF_XS + sizeof(double) * 2 * XS;
+    static constexpr size_t OFF_WS = OFF_YS + sizeof(double) * XS;
+    static constexpr size_t OFF_REL = OFF_WS + sizeof(double) * 2 * NS * BRICK_ELEMS;
+    static constexpr size_t OFF_PK = OFF_REL + sizeof(int32_t) * XS;
+    static constexpr size_t BYTES = OFF_PK + sizeof(uint16_t) * XS;
+};
+
+template <int N>
+__device__ __forceinline__ void stage_brick64(int64_t brick, int buf, const double *__restrict__ x,
+                                              const double *__restrict__ w, const FineGeom &fg, unsigned char *smem,
+                                              const int32_t *rel, const uint16_t *pk, int tid) {
+    using L = StagedLayout<N>;
+    const Grid &g = fg.g;
+    const int bby = (int)(brick % fg.nby);
+    const int bbx = (int)((brick / fg.nby) % fg.nbx);
+    const int bbz = (int)(brick / ((int64_t)fg.nby * fg.nbx));
+    const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
+    double *xs = reinterpret_cast<double *>(smem + L::OFF_XS) + buf * L::XS;
+    const double *xb = x + brick_base_dof(ex0, ey0, ez0, g);
+    if (brick_interior(ex0, ey0, ez0, g)) {
+        for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) cp_async8(xs + i, xb + rel[i], 8);
+    } else {
+        for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) {
+            const bool in = brick_slot_in(pk[i], ex0, ey0, ez0, g);
+            cp_async8(xs + i, in ? xb + rel[i] : x, in ? 8 : 0);
+        }
+    }
+    const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
+    const int ex = ex0 + lx, ey = ey0 + ly, ez = ez0 + lz;
+    const bool valid = ex < g.nelx && ey < g.nely && ez < g.nelz;
+    double *ws = reinterpret_cast<double *>(smem + L::OFF_WS) + buf * L::NS * BRICK_ELEMS;
+#pragma unroll
+    for (int s = 0; s < L::NS; ++s) {
+        const int sy = s % N, sx = (s / N) % N, sz = s / (N * N);
+        const double *src =
+            valid ? w + ((int64_t)(ez * N + sz) * fg.nelx_d + (ex * N + sx)) * fg.nely_d + (ey * N + sy) : w;
+        cp_async8(ws + s * BRICK_ELEMS + tid, src, valid ? 8 : 0);
+    }
+}
+
+template <int N>
+__global__ void __launch_bounds__(BRICK_ELEMS, N == 2 ? 3 : 1)
+k_fine_apply64(const double *__restrict__ x, double *__restrict__ y, const double *__restrict__ w,
+               const uint8_t *__restrict__ freemask, const double *__restrict__ ktg, FineGeom fg) {
+    using L = StagedLayout<N>;
+    constexpr int NS = L::NS, NSP = FineShape<double, N>::NSP;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *kt = reinterpret_cast<double *>(smem_raw);
+    double *ys = reinterpret_cast<double *>(smem_raw + L::OFF_YS);
+    int32_t *rel = reinterpret_cast<int32_t *>(smem_raw + L::OFF_REL);
+    uint16_t *pk = reinterpret_cast<uint16_t *>(smem_raw + L::OFF_PK);
+    const int tid = threadIdx.x;
+    const Grid &g = fg.g;
+    for (int i = tid; i < FineShape<double, N>::KT_LEN; i += BRICK_ELEMS) kt[i] = ktg[i];
+    brick_slots_init(rel, pk, g, tid);
+    __syncthreads();
+
+    const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
+    const int ln0 = brick_base_node(tid);
+    int buf = 0;
+    if (blockIdx.x < fg.nbricks) stage_brick64<N>(blockIdx.x, 0, x, w, fg, smem_raw, rel, pk, tid);
+    asm volatile("cp.async.commit_group;" ::: "memory");
+    for (int64_t brick = blockIdx.x; brick < fg.nbricks; brick += gridDim.x, buf ^= 1) {
+        const int64_t next = brick + gridDim.x;
+        if (next < fg.nbricks) stage_brick64<N>(next, buf ^ 1, x, w, fg, smem_raw, rel, pk, tid);
+        asm volatile("cp.async.commit_group;" ::: "memory");
+        asm volatile("cp.async.wait_group 1;" ::: "memory");
+        __syncthreads();   // this brick's inputs landed; the previous write-out is done
+        for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) ys[i] = 0.0;
+
+        const int bby = (int)(brick % fg.nby);
+        const int bbx = (int)((brick / fg.nby) % fg.nbx);
+        const int bbz = (int)(brick / ((int64_t)fg.nby * fg.nbx));
+        const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
+        const bool valid = ex0 + lx < g.nelx && ey0 + ly < g.nely && ez0 + lz < g.nelz;
+        const double *xs = reinterpret_cast<const double *>(smem_raw + L::OFF_XS) + buf * L::XS;
+        const double *ws = reinterpret_cast<const double *>(smem_raw + L::OFF_WS) + buf * NS * BRICK_ELEMS;
+        double acc[24];
+#pragma unroll
+        for (int i = 0; i < 24; ++i) acc[i] = 0.0;
+        if (valid) {
+            double u[24];
+#pragma unroll
+            for (int a = 0; a < 8; ++a) {
+                const int dx = (a >> 1) & 1, dy = a & 1, dz = (a >> 2) & 1;
+                const int ln = ln0 + (dz * NBX + dx) * NBY + dy;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) u[3 * a + c] = xs[3 * ln + c];
+            }
+            if constexpr (N == 2) {
+                double wh[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) wh[q] = ws[q * BRICK_ELEMS + tid];
+#pragma unroll
+                for (int bit = 1; bit < 8; bit <<= 1) {
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        if (!(q & bit)) {
+                            const double a = wh[q], b = wh[q | bit];
+                            wh[q] = a + b;
+                            wh[q | bit] = a - b;
+                        }
+                    }
+                }
+                all_pairs_mr2<double>(kt, wh, u, acc, std::make_integer_sequence<int, KE_PACK>{});
+            } else {
+                double wv[NSP];
+#pragma unroll
+                for (int q = 0; q < NSP; ++q) wv[q] = q < NS ? ws[q * BRICK_ELEMS + tid] : 0.0;
+                all_pairs<double, NSP>(kt, wv, u, acc, std::make_integer_sequence<int, KE_PACK>{});
+            }
+        }
+        __syncthreads();   // ys cleared by every thread
+        brick_accumulate(ys, acc, valid, ln0);
+        brick_writeout_tab(ys, y, freemask, g, ex0, ey0, ez0, rel, pk, tid);
+    }
+    asm volatile("cp.async.wait_group 0;" ::: "memory");
 }
 
 // Diagonal of K(w): one thread per element, atomics (setup only).  Reads the
@@ -321,9 +459,34 @@ static void launch_fine_t(const T *x, T *y, const TW *w, const uint8_t *fm, cons
     kern<<<(unsigned)grid, BRICK_ELEMS, smem, st>>>(x, y, w, fm, kt, fg); count_launch();
 }
 
+template <int N>
+static void launch_fine64_staged(const double *x, double *y, const double *w, const uint8_t *fm, const double *kt,
+                                 const FineGeom &fg, cudaStream_t st) {
+    const size_t smem = StagedLayout<N>::BYTES;
+    auto kern = k_fine_apply64<N>;
+    static int attr_dev = -1, per_sm = 0;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (attr_dev != dev) {
+        cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BRICK_ELEMS, smem);
+        if (per_sm < 1) per_sm = 1;
+        attr_dev = dev;
+    }
+    int64_t grid = (int64_t)per_sm * num_sms();
+    if (grid > fg.nbricks) grid = fg.nbricks;
+    if (grid < 1) grid = 1;
+    kern<<<(unsigned)grid, BRICK_ELEMS, smem, st>>>(x, y, w, fm, kt, fg); count_launch();
+}
+
 template <typename T, typename TW>
 void launch_fine_apply(const T *x, T *y, const TW *w, const uint8_t *freemask, const T *kt, const FineGeom &fg, int n,
                        cudaStream_t st) {
+    if constexpr (sizeof(T) == 8) {
+        if (n == 1) return launch_fine64_staged<1>(x, y, w, freemask, kt, fg, st);
+        if (n == 2) return launch_fine64_staged<2>(x, y, w, freemask, kt, fg, st);
+    }
     if (n == 1) launch_fine_t<T, TW, 1>(x, y, w, freemask, kt, fg, st);
     else if (n == 2) launch_fine_t<T, TW, 2>(x, y, w, freemask, kt, fg, st);
     else launch_fine_t<T, TW, 3>(x, y, w, freemask, kt, fg, st);

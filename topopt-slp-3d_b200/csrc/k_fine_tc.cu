@@ -20,7 +20,8 @@
 // Pipelining inside a CTA: the next brick's nodal values and factors are
 // staged with cp.async while the current brick computes; the entries are
 // formed in 64-column chunks through two tensor-memory buffers, so the MMA of
-// chunk c+1 runs while the threads consume chunk c.  Each CTA allocates 128
+// chunk c+1 runs while the threads consume chunk c, and the next brick's
+// first two chunks run during the current brick's node sums and write-out.  Each CTA allocates 128
 // tensor-memory columns; the dynamic shared memory per CTA is padded so that
 // at most four CTAs (512 columns) are resident on an SM.  Every wait on an
 // MMA-completion barrier is bounded; a timeout sets *err, leaves the brick
@@ -118,7 +119,6 @@ __device__ __forceinline__ void cp_async4(void *dst, const void *src, int nbytes
                  : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&r)[32]) {
@@ -199,47 +199,52 @@ __device__ __forceinline__ void issue_chunk(int c, uint32_t tmem, uint32_t a_add
 }  // namespace
 
 // Dynamic shared memory: B image, two A buffers, two node-input buffers, the
-// node sums; padded so that at most four CTAs fit on an SM (228 KB with 1 KB
-// reserved per CTA: 4 x 53.1 KB fit, 5 do not).  The MMA operands need
-// 16-byte aligned starts; the barriers and the tensor-memory address are
-// static (8-byte aligned) shared variables.
+// node sums and the brick slot table; padded so that at most four CTAs fit on
+// an SM (228 KB with 1 KB reserved per CTA: 4 x 53.1 KB fit, 5 do not).  The
+// MMA operands need 16-byte aligned starts; the barriers and the
+// tensor-memory address are static (8-byte aligned) shared variables.
 constexpr size_t TC_OFF_A = TC_B_BYTES;
 constexpr size_t TC_OFF_XS = TC_OFF_A + 2 * TC_A_BYTES;
 constexpr size_t TC_OFF_YS = TC_OFF_XS + sizeof(float) * 2 * TC_XS_FLOATS;
-constexpr size_t TC_SMEM_USED = TC_OFF_YS + sizeof(float) * TC_XS_FLOATS;
+constexpr size_t TC_OFF_REL = TC_OFF_YS + sizeof(float) * TC_XS_FLOATS;
+constexpr size_t TC_OFF_PK = TC_OFF_REL + sizeof(int32_t) * TC_XS_FLOATS;
+constexpr size_t TC_SMEM_USED = TC_OFF_PK + sizeof(uint16_t) * TC_XS_FLOATS;
 constexpr size_t TC_SMEM = 52 * 1024;
 static_assert(TC_OFF_A % 16 == 0 && TC_OFF_XS % 16 == 0 && TC_OFF_YS % 16 == 0, "operand alignment");
+static_assert(TC_OFF_REL % 4 == 0 && TC_OFF_PK % 2 == 0, "slot table alignment");
 static_assert(TC_SMEM_USED <= TC_SMEM, "tensor-core operator shared memory");
 static_assert(TC_ROWS_B - (TC_NCHUNK - 1) * TC_CHUNK == 48, "last chunk");
 
 // Stage brick `brick` (nodal values, A rows) into buffer `buf` with cp.async.
 __device__ __forceinline__ void stage_brick(int64_t brick, int buf, const float *__restrict__ x,
                                             const __nv_bfloat16 *__restrict__ w, const FineGeom &fg,
-                                            unsigned char *smem, int tid) {
+                                            unsigned char *smem, const int32_t *rel, const uint16_t *pk,
+                                            int tid) {
     const Grid &g = fg.g;
     const int bby = (int)(brick % fg.nby);
     const int bbx = (int)((brick / fg.nby) % fg.nbx);
     const int bbz = (int)(brick / ((int64_t)fg.nby * fg.nbx));
     const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
     float *xs = reinterpret_cast<float *>(smem + TC_OFF_XS) + buf * TC_XS_FLOATS;
-    for (int i = tid; i < BRICK_NODES * 3; i += BRICK_ELEMS) {
-        const int ln = i / 3, c = i - 3 * ln;
-        const int ny_ = ln % NBY, nx_ = (ln / NBY) % NBX, nz_ = ln / (NBY * NBX);
-        const int gx = ex0 + nx_, gy = ey0 + ny_, gz = ez0 + nz_;
-        const bool in = gx < g.nx && gy < g.ny && gz < g.nz;
-        const float *src = in ? x + 3 * (((int64_t)gz * g.nx + gx) * g.ny + gy) + c : x;
-        cp_async4(xs + i, src, in ? 4 : 0);
+    const float *xb = x + brick_base_dof(ex0, ey0, ez0, g);
+    if (brick_interior(ex0, ey0, ez0, g)) {
+        for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) cp_async4(xs + i, xb + rel[i], 4);
+    } else {
+        for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) {
+            const bool in = brick_slot_in(pk[i], ex0, ey0, ez0, g);
+            cp_async4(xs + i, in ? xb + rel[i] : x, in ? 4 : 0);
+        }
     }
     const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
     const int ex = ex0 + lx, ey = ey0 + ly, ez = ez0 + lz;
     const bool valid = ex < g.nelx && ey < g.nely && ez < g.nelz;
     unsigned char *ar = smem + TC_OFF_A + buf * TC_A_BYTES + tc_offset(tid, 0);
+    const __nv_bfloat16 *wb = w + ((int64_t)(ez * 2) * fg.nelx_d + ex * 2) * fg.nely_d + ey * 2;
 #pragma unroll
     for (int s = 0; s < 8; s += 2) {
         // sub-cubes s and s+1 differ in y only: adjacent in the density mesh
         const int sx = (s >> 1) & 1, sz = s >> 2;
-        const __nv_bfloat16 *src =
-            valid ? w + ((int64_t)(ez * 2 + sz) * fg.nelx_d + (ex * 2 + sx)) * fg.nely_d + ey * 2 : w;
+        const __nv_bfloat16 *src = valid ? wb + ((int64_t)sz * fg.nelx_d + sx) * fg.nely_d : w;
         cp_async4(ar + 2 * s, src, valid ? 4 : 0);
         cp_async4(ar + 128 + 2 * s, src, valid ? 4 : 0);
     }
@@ -250,7 +255,9 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
                  const uint8_t *__restrict__ freemask, const uint4 *__restrict__ bimg, FineGeom fg,
                  int *__restrict__ err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    float *ys = reinterpret_cast<float *>(smem_raw + TC_OFF_YS);    // BRICK_NODES * 3 node sums
+    float *ys = reinterpret_cast<float *>(smem_raw + TC_OFF_YS);          // node sums
+    int32_t *rel = reinterpret_cast<int32_t *>(smem_raw + TC_OFF_REL);    // slot table
+    uint16_t *pk = reinterpret_cast<uint16_t *>(smem_raw + TC_OFF_PK);
     __shared__ __align__(8) uint64_t s_mbar[2];
     __shared__ __align__(8) uint32_t s_tmem;
     __shared__ int s_fail;
@@ -260,7 +267,9 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
         if (tid == 0) atomicExch(err, 2);
         return;
     }
+    const Grid &g = fg.g;
     for (int i = tid; i < TC_B_BYTES / 16; i += BRICK_ELEMS) reinterpret_cast<uint4 *>(smem_raw)[i] = bimg[i];
+    brick_slots_init(rel, pk, g, tid);
     if (tid == 0) {
         s_fail = 0;
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar[0])) : "memory");
@@ -281,39 +290,43 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
     const uint32_t tlane = tmem + ((uint32_t)(warp * 32) << 16);    // this warp's 32 lanes
     const uint32_t mbar0 = smem_u32(&s_mbar[0]), mbar1 = smem_u32(&s_mbar[1]);
     const uint32_t b_addr = smem_u32(smem_raw);
+    const uint32_t a_addr0 = smem_u32(smem_raw + TC_OFF_A);
     uint32_t ph0 = 0, ph1 = 0;
 
-    const Grid &g = fg.g;
     const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
     const int ln0 = brick_base_node(tid);
 
-    int buf = 0;
-    if (blockIdx.x < fg.nbricks) stage_brick(blockIdx.x, 0, x, w, fg, smem_raw, tid);
+    // Prologue: the first brick's inputs, then its first two chunks.  In the
+    // loop, brick b+1's inputs are staged while brick b computes, and its
+    // first two chunks are issued as soon as brick b's last chunk is read, so
+    // they run during brick b's node sums and write-out.
+    if (blockIdx.x < fg.nbricks) stage_brick(blockIdx.x, 0, x, w, fg, smem_raw, rel, pk, tid);
     cp_async_commit();
+    cp_async_wait_0();
+    fence_async_smem();
+    __syncthreads();
+    if (tid == 0 && blockIdx.x < fg.nbricks) {
+        fence_after();
+        issue_chunk(0, tmem, a_addr0, b_addr, mbar0);
+        issue_chunk(1, tmem, a_addr0, b_addr, mbar1);
+    }
+
+    int buf = 0;
     for (int64_t brick = blockIdx.x; brick < fg.nbricks; brick += gridDim.x, buf ^= 1) {
         // the other buffers were last read by the previous brick, whose
         // threads have all passed its chunk barriers
         const int64_t next = brick + gridDim.x;
-        if (next < fg.nbricks) stage_brick(next, buf ^ 1, x, w, fg, smem_raw, tid);
+        if (next < fg.nbricks) stage_brick(next, buf ^ 1, x, w, fg, smem_raw, rel, pk, tid);
         cp_async_commit();
-        cp_async_wait_1();   // this brick's copies are complete
-        fence_async_smem();
-        __syncthreads();     // also: every thread is done with the previous write-out
 
         const int bby = (int)(brick % fg.nby);
         const int bbx = (int)((brick / fg.nby) % fg.nbx);
         const int bbz = (int)(brick / ((int64_t)fg.nby * fg.nbx));
         const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
         const bool valid = ex0 + lx < g.nelx && ey0 + ly < g.nely && ez0 + lz < g.nelz;
-        const uint32_t a_addr = smem_u32(smem_raw + TC_OFF_A + buf * TC_A_BYTES);
+        const uint32_t a_addr = a_addr0 + (uint32_t)(buf * TC_A_BYTES);
         const float *xs = reinterpret_cast<const float *>(smem_raw + TC_OFF_XS) + buf * TC_XS_FLOATS;
 
-        if (tid == 0) {
-            fence_after();
-            issue_chunk(0, tmem, a_addr, b_addr, mbar0);
-            issue_chunk(1, tmem, a_addr, b_addr, mbar1);
-        }
-        for (int i = tid; i < BRICK_NODES * 3; i += BRICK_ELEMS) ys[i] = 0.f;
         float u[24], acc[24];
 #pragma unroll
         for (int a = 0; a < 8; ++a) {
@@ -334,6 +347,10 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
             if (__syncthreads_or(!got)) {
                 ok = false;
                 break;
+            }
+            if (c == 0) {
+                // every thread has finished the previous brick's write-out
+                for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) ys[i] = 0.f;
             }
             fence_after();
             const uint32_t taddr = tlane + (uint32_t)((c & 1) * TC_CHUNK);
@@ -356,8 +373,18 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
             }
             break;
         }
+        // next brick's inputs complete and visible to the tensor cores
+        cp_async_wait_0();
+        fence_async_smem();
+        __syncthreads();
+        if (tid == 0 && next < fg.nbricks) {
+            fence_after();
+            const uint32_t a_next = a_addr0 + (uint32_t)((buf ^ 1) * TC_A_BYTES);
+            issue_chunk(0, tmem, a_next, b_addr, mbar0);
+            issue_chunk(1, tmem, a_next, b_addr, mbar1);
+        }
         brick_accumulate(ys, acc, valid, ln0);
-        brick_writeout(ys, y, freemask, g, ex0, ey0, ez0, tid);
+        brick_writeout_tab(ys, y, freemask, g, ex0, ey0, ez0, rel, pk, tid);
     }
     cp_async_wait_0();
 

@@ -24,6 +24,7 @@ thread_local std::string g_create_error;
 struct Level {
     Grid g;
     uint8_t *fm = nullptr;     // free flag per dof
+    bool nm = false;           // stencil stored node-major, applied warp per node
     double *Ae = nullptr;      // Galerkin element matrices (levels >= 1), FP64
     void *st = nullptr;        // 27-point stencil (levels 1..L-2), cycle precision
     void *invd = nullptr;      // omega / diag(A), 0 on fixed dofs, cycle precision
@@ -214,7 +215,8 @@ int smooth(tosp_handle *h, int l, int niter, bool x_zero) {
             TRY(fine_apply<T>(h, (const T *)L.x, (T *)L.t));
             launch_jacobi_update<T>((T *)L.x, b, (const T *)L.t, (const T *)L.invd, nd, 0, h->stream);
         } else {
-            launch_stencil<T>((const T *)L.st, (const T *)L.x, b, (const T *)L.invd, (T *)L.t, L.g, 2, h->stream);
+            launch_stencil<T>((const T *)L.st, (const T *)L.x, b, (const T *)L.invd, (T *)L.t, L.g, 2, L.nm,
+                              h->stream);
             std::swap(L.x, L.t);
         }
         CKL();
@@ -229,7 +231,8 @@ int residual(tosp_handle *h, int l) {
         TRY(fine_apply<T>(h, (const T *)L.x, (T *)L.t));
         launch_residual<T>((const T *)L.b, (const T *)L.t, (T *)L.r, L.g.ndof, h->stream);
     } else {
-        launch_stencil<T>((const T *)L.st, (const T *)L.x, (const T *)L.b, nullptr, (T *)L.r, L.g, 1, h->stream);
+        launch_stencil<T>((const T *)L.st, (const T *)L.x, (const T *)L.b, nullptr, (T *)L.r, L.g, 1, L.nm,
+                          h->stream);
     }
     CKL();
     return TOSP_OK;
@@ -586,7 +589,9 @@ int setup_levels(tosp_handle *h) {
     CKL();
     for (int l = 1; l < ng - 1; ++l) {
         Level &L = h->lev[l];
-        launch_assemble_stencil<T>(L.Ae, L.fm, L.g, (T *)L.st, (T *)L.invd, h->mg.omega, h->stream);
+        const int64_t wmax = h->mg.warp_stencil_max == 0 ? 65536 : h->mg.warp_stencil_max;
+        L.nm = L.g.nnodes <= wmax;
+        launch_assemble_stencil<T>(L.Ae, L.fm, L.g, (T *)L.st, (T *)L.invd, h->mg.omega, L.nm, h->stream);
         launch_coarse_from_coarse(L.Ae, L.fm, L.g, h->lev[l + 1].Ae, h->lev[l + 1].g, h->stream);
         CKL();
     }
@@ -793,6 +798,7 @@ void tosp_default_mg_params(tosp_mg_params *mg) {
     mg->nmaxchol = 60000;
     mg->flexible = 0;
     mg->maxstall = 0;
+    mg->warp_stencil_max = 0;
 }
 
 int tosp_create(const tosp_problem *prob, const tosp_mg_params *mg, int32_t precision, tosp_handle **out) {

@@ -132,11 +132,13 @@ void launch_coarse_from_coarse(const double *Af, const uint8_t *freemask_f, cons
 // Node stencil from element matrices (masked), plus omega/diag.
 template <typename T>
 void launch_assemble_stencil(const double *Ae, const uint8_t *freemask, const Grid &g, T *stencil,
-                             T *invdiag, double omega, cudaStream_t st);
+                             T *invdiag, double omega, bool node_major, cudaStream_t st);
 // Stencil products: mode 0: y = A x; 1: y = b - A x; 2: y = x + invD (b - A x).
+// node_major: layout [node][27 offsets][3x3], one warp per node; otherwise
+// [27 offsets][3x3][node], one thread per node.
 template <typename T>
 void launch_stencil(const T *st_vals, const T *x, const T *b, const T *invdiag, T *y, const Grid &g,
-                    int mode, cudaStream_t st);
+                    int mode, bool node_major, cudaStream_t st);
 // Fine-level helpers: y = b - t ; x = x + invD (b - t) ; x = invD b
 template <typename T>
 void launch_residual(const T *b, const T *t, T *r, int64_t n, cudaStream_t st);
