@@ -58,7 +58,7 @@ template <bool FROM_FINE, int N>
 __global__ void __launch_bounds__(CB_THREADS)
 k_coarse_build(const double *__restrict__ w, const double *__restrict__ kepack, const double *__restrict__ Af,
                const uint8_t *__restrict__ fmask, Grid gf, int nelx_d, int nely_d, double *__restrict__ Ac,
-               Grid gc) {
+               Grid gc, int only_fixed) {
     constexpr int NS = N * N * N;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double *ke = reinterpret_cast<double *>(smem_raw);          // NS*300 (FROM_FINE only)
@@ -74,6 +74,17 @@ k_coarse_build(const double *__restrict__ w, const double *__restrict__ kepack, 
     for (int64_t E = blockIdx.x; E < gc.nelem; E += gridDim.x) {
         const int cy = (int)(E % gc.nely), cx = (int)((E / gc.nely) % gc.nelx),
                   cz = (int)(E / ((int64_t)gc.nely * gc.nelx));
+        if (only_fixed) {
+            // elements whose 27 fine nodes are all free were built from the table
+            bool fixed = false;
+            if (tid < 81) {
+                const int nd = tid / 3, comp = tid % 3;
+                const int64_t node = ((int64_t)(2 * cz + nd / 9) * gf.nx + (2 * cx + (nd / 3) % 3)) * gf.ny +
+                                     (2 * cy + nd % 3);
+                fixed = !fmask[3 * node + comp];
+            }
+            if (!__syncthreads_or(fixed)) continue;
+        }
         double acc[3] = {0.0, 0.0, 0.0};
 #pragma unroll 1
         for (int c = 0; c < 8; ++c) {
@@ -136,7 +147,7 @@ k_coarse_build(const double *__restrict__ w, const double *__restrict__ kepack, 
 
 template <bool FROM_FINE, int N>
 static void launch_cb(const double *w, const double *kepack, const double *Af, const uint8_t *fm, const Grid &gf,
-                      int nelx_d, int nely_d, double *Ac, const Grid &gc, cudaStream_t st) {
+                      int nelx_d, int nely_d, double *Ac, const Grid &gc, cudaStream_t st, int only_fixed = 0) {
     constexpr int NS = N * N * N;
     const size_t smem = sizeof(double) * ((FROM_FINE ? NS * KE_PACK : 0) + 576 * 2 + 64 + NS) + 32;
     auto kern = k_coarse_build<FROM_FINE, N>;
@@ -146,14 +157,109 @@ static void launch_cb(const double *w, const double *kepack, const double *Af, c
     if (per_sm < 1) per_sm = 1;
     int64_t grid = (int64_t)per_sm * num_sms_c();
     if (grid > gc.nelem) grid = gc.nelem;
-    kern<<<(unsigned)grid, CB_THREADS, smem, st>>>(w, kepack, Af, fm, gf, nelx_d, nely_d, Ac, gc); count_launch();
+    kern<<<(unsigned)grid, CB_THREADS, smem, st>>>(w, kepack, Af, fm, gf, nelx_d, nely_d, Ac, gc, only_fixed);
+    count_launch();
 }
 
-void launch_coarse_from_fine(const double *w, const uint8_t *freemask_f, const double *kepack, double *Ac,
-                             const FineGeom &fg, const Grid &gc, int n, cudaStream_t st) {
-    if (n == 1) launch_cb<true, 1>(w, kepack, nullptr, freemask_f, fg.g, fg.nelx_d, fg.nely_d, Ac, gc, st);
-    else if (n == 2) launch_cb<true, 2>(w, kepack, nullptr, freemask_f, fg.g, fg.nelx_d, fg.nely_d, Ac, gc, st);
-    else launch_cb<true, 3>(w, kepack, nullptr, freemask_f, fg.g, fg.nelx_d, fg.nely_d, Ac, gc, st);
+// Finest coarsening from the sub-cell table: Abar_E = sum_q w_q S_q over the
+// 8 n^3 density cells q of coarse element E, valid when none of E's 27 fine
+// nodes has a fixed dof (then M_c = I in every triple product).  A CTA of
+// TB_THREADS threads takes TB_ELEMS coarse elements at a time; thread t owns
+// packed entry t for all of them, reading S_q[t] once per cell.  Elements with
+// a fixed fine dof are left for the masked kernel.
+constexpr int TB_THREADS = 320;
+constexpr int TB_ELEMS = 8;
+
+template <int N>
+__global__ void __launch_bounds__(TB_THREADS, 2)
+k_coarse_table(const double *__restrict__ w, const uint8_t *__restrict__ fmask, const double *__restrict__ S,
+               Grid gf, int nelx_d, int nely_d, double *__restrict__ Ac, Grid gc) {
+    constexpr int Q = 8 * N * N * N;
+    __shared__ double ws[TB_ELEMS * Q];
+    __shared__ int fixed[TB_ELEMS];
+    const int tid = threadIdx.x;
+    int ti = 0, tj = 0;
+    if (tid < KE_PACK) {   // packed upper index -> (i, j), row-major
+        int t = tid;
+        while (t >= 24 - ti) {
+            t -= 24 - ti;
+            ++ti;
+        }
+        tj = ti + t;
+    }
+    for (int64_t E0 = (int64_t)blockIdx.x * TB_ELEMS; E0 < gc.nelem; E0 += (int64_t)gridDim.x * TB_ELEMS) {
+        __syncthreads();
+        if (tid < TB_ELEMS) fixed[tid] = 0;
+        __syncthreads();
+        for (int k = tid; k < TB_ELEMS * Q; k += TB_THREADS) {
+            const int e = k / Q, q = k - e * Q;
+            const int64_t E = E0 + e;
+            double v = 0.0;
+            if (E < gc.nelem) {
+                const int cy = (int)(E % gc.nely), cx = (int)((E / gc.nely) % gc.nelx),
+                          cz = (int)(E / ((int64_t)gc.nely * gc.nelx));
+                const int c = q / (N * N * N), sidx = q - c * N * N * N;
+                const int fx = 2 * cx + ((c >> 1) & 1), fy = 2 * cy + (c & 1), fz = 2 * cz + ((c >> 2) & 1);
+                const int sy = sidx % N, sx = (sidx / N) % N, sz = sidx / (N * N);
+                v = w[((int64_t)(fz * N + sz) * nelx_d + (fx * N + sx)) * nely_d + (fy * N + sy)];
+            }
+            ws[k] = v;
+        }
+        for (int k = tid; k < TB_ELEMS * 81; k += TB_THREADS) {
+            const int e = k / 81, r = k - e * 81, nd = r / 3, comp = r % 3;
+            const int64_t E = E0 + e;
+            if (E >= gc.nelem) continue;
+            const int cy = (int)(E % gc.nely), cx = (int)((E / gc.nely) % gc.nelx),
+                      cz = (int)(E / ((int64_t)gc.nely * gc.nelx));
+            const int64_t node = ((int64_t)(2 * cz + nd / 9) * gf.nx + (2 * cx + (nd / 3) % 3)) * gf.ny +
+                                 (2 * cy + nd % 3);
+            if (!fmask[3 * node + comp]) fixed[e] = 1;
+        }
+        __syncthreads();
+        if (tid < KE_PACK) {
+            double acc[TB_ELEMS];
+#pragma unroll
+            for (int e = 0; e < TB_ELEMS; ++e) acc[e] = 0.0;
+#pragma unroll 4
+            for (int q = 0; q < Q; ++q) {
+                const double sq = S[(size_t)q * KE_PACK + tid];
+#pragma unroll
+                for (int e = 0; e < TB_ELEMS; ++e) acc[e] += ws[e * Q + q] * sq;
+            }
+#pragma unroll
+            for (int e = 0; e < TB_ELEMS; ++e) {
+                const int64_t E = E0 + e;
+                if (E >= gc.nelem || fixed[e]) continue;
+                Ac[E * 576 + ti * 24 + tj] = acc[e];
+                if (ti != tj) Ac[E * 576 + tj * 24 + ti] = acc[e];
+            }
+        }
+    }
+}
+
+template <int N>
+static void launch_table(const double *w, const uint8_t *fm, const double *S, const FineGeom &fg, double *Ac,
+                         const Grid &gc, cudaStream_t st) {
+    int64_t grid = (gc.nelem + TB_ELEMS - 1) / TB_ELEMS;
+    const int64_t cap = (int64_t)4 * num_sms_c();
+    if (grid > cap) grid = cap;
+    if (grid < 1) grid = 1;
+    k_coarse_table<N><<<(unsigned)grid, TB_THREADS, 0, st>>>(w, fm, S, fg.g, fg.nelx_d, fg.nely_d, Ac, gc);
+    count_launch();
+}
+
+void launch_coarse_from_fine_table(const double *w, const uint8_t *freemask_f, const double *kepack, const double *S,
+                                   double *Ac, const FineGeom &fg, const Grid &gc, int n, cudaStream_t st) {
+    if (n == 1) {
+        launch_table<1>(w, freemask_f, S, fg, Ac, gc, st);
+        launch_cb<true, 1>(w, kepack, nullptr, freemask_f, fg.g, fg.nelx_d, fg.nely_d, Ac, gc, st, 1);
+    } else if (n == 2) {
+        launch_table<2>(w, freemask_f, S, fg, Ac, gc, st);
+        launch_cb<true, 2>(w, kepack, nullptr, freemask_f, fg.g, fg.nelx_d, fg.nely_d, Ac, gc, st, 1);
+    } else {
+        launch_table<3>(w, freemask_f, S, fg, Ac, gc, st);
+        launch_cb<true, 3>(w, kepack, nullptr, freemask_f, fg.g, fg.nelx_d, fg.nely_d, Ac, gc, st, 1);
+    }
 }
 
 void launch_coarse_from_coarse(const double *Af, const uint8_t *freemask_f, const Grid &gf, double *Ac,

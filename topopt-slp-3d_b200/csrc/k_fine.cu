@@ -16,6 +16,8 @@
 // on the brick faces.
 #include <cuda_bf16.h>
 
+#include <cstring>
+#include <type_traits>
 #include <utility>
 
 #include "brick.cuh"
@@ -135,6 +137,45 @@ template <typename T, int... Ts>
 __device__ __forceinline__ void all_pairs_mr2(const T *__restrict__ kt, const T (&wh)[8], const T (&u)[24],
                                               T (&acc)[24], std::integer_sequence<int, Ts...>) {
     (pair_step_mr2<T, Ts>(kt, wh, u, acc), ...);
+}
+
+// MR-2 Walsh-Hadamard coefficients as a kernel parameter (12 384 bytes, in
+// the constant bank): every coefficient index is a compile-time constant, so
+// the FMAs take them as constant-bank operands and no shared-memory load is
+// issued for them.  Entry t's non-zero modes start at mr2_off(t, 1).
+struct Mr2Table {
+    double v[kMr2Nonzeros];
+};
+
+template <int t>
+__device__ __forceinline__ void pair_step_mr2c(const Mr2Table &kt, const double (&wh)[8], const double (&u)[24],
+                                               double (&acc)[24]) {
+    constexpr int i = pair_i(t), j = pair_j(t);
+    constexpr unsigned MASK = mr2_mask(t);
+    constexpr int OFF = mr2_off(t, 1);
+    double k0 = 0.0, k1 = 0.0;
+    int idx = 0;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) {
+        if ((MASK >> m) & 1) {
+            if (idx & 1) k1 = fma(wh[m], kt.v[OFF + idx], k1);
+            else k0 = fma(wh[m], kt.v[OFF + idx], k0);
+            ++idx;
+        }
+    }
+    const double k = k0 + k1;
+    if constexpr (i == j) {
+        acc[i] = fma(k, u[i], acc[i]);
+    } else {
+        acc[i] = fma(k, u[j], acc[i]);
+        acc[j] = fma(k, u[i], acc[j]);
+    }
+}
+
+template <int... Ts>
+__device__ __forceinline__ void all_pairs_mr2c(const Mr2Table &kt, const double (&wh)[8], const double (&u)[24],
+                                               double (&acc)[24], std::integer_sequence<int, Ts...>) {
+    (pair_step_mr2c<Ts>(kt, wh, u, acc), ...);
 }
 
 template <typename T, int N> struct FineShape {
@@ -287,10 +328,14 @@ __device__ __forceinline__ void stage_brick64(int64_t brick, int buf, const doub
     }
 }
 
-template <int N>
+struct NoTable {};
+
+template <int N, typename KP>
 __global__ void __launch_bounds__(BRICK_ELEMS, N == 2 ? 3 : 1)
 k_fine_apply64(const double *__restrict__ x, double *__restrict__ y, const double *__restrict__ w,
-               const uint8_t *__restrict__ freemask, const double *__restrict__ ktg, FineGeom fg) {
+               const uint8_t *__restrict__ freemask, const double *__restrict__ ktg, FineGeom fg,
+               const __grid_constant__ KP ktc) {
+    constexpr bool CONST_KE = std::is_same<KP, Mr2Table>::value;
     using L = StagedLayout<N>;
     constexpr int NS = L::NS, NSP = FineShape<double, N>::NSP;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -300,7 +345,8 @@ k_fine_apply64(const double *__restrict__ x, double *__restrict__ y, const doubl
     uint16_t *pk = reinterpret_cast<uint16_t *>(smem_raw + L::OFF_PK);
     const int tid = threadIdx.x;
     const Grid &g = fg.g;
-    for (int i = tid; i < FineShape<double, N>::KT_LEN; i += BRICK_ELEMS) kt[i] = ktg[i];
+    if constexpr (!CONST_KE)
+        for (int i = tid; i < FineShape<double, N>::KT_LEN; i += BRICK_ELEMS) kt[i] = ktg[i];
     brick_slots_init(rel, pk, g, tid);
     __syncthreads();
 
@@ -351,7 +397,10 @@ k_fine_apply64(const double *__restrict__ x, double *__restrict__ y, const doubl
                         }
                     }
                 }
-                all_pairs_mr2<double>(kt, wh, u, acc, std::make_integer_sequence<int, KE_PACK>{});
+                if constexpr (CONST_KE)
+                    all_pairs_mr2c(ktc, wh, u, acc, std::make_integer_sequence<int, KE_PACK>{});
+                else
+                    all_pairs_mr2<double>(kt, wh, u, acc, std::make_integer_sequence<int, KE_PACK>{});
             } else {
                 double wv[NSP];
 #pragma unroll
@@ -459,11 +508,11 @@ static void launch_fine_t(const T *x, T *y, const TW *w, const uint8_t *fm, cons
     kern<<<(unsigned)grid, BRICK_ELEMS, smem, st>>>(x, y, w, fm, kt, fg); count_launch();
 }
 
-template <int N>
+template <int N, typename KP>
 static void launch_fine64_staged(const double *x, double *y, const double *w, const uint8_t *fm, const double *kt,
-                                 const FineGeom &fg, cudaStream_t st) {
+                                 const FineGeom &fg, cudaStream_t st, const KP &ktc) {
     const size_t smem = StagedLayout<N>::BYTES;
-    auto kern = k_fine_apply64<N>;
+    auto kern = k_fine_apply64<N, KP>;
     static int attr_dev = -1, per_sm = 0;
     int dev = 0;
     cudaGetDevice(&dev);
@@ -477,15 +526,33 @@ static void launch_fine64_staged(const double *x, double *y, const double *w, co
     int64_t grid = (int64_t)per_sm * num_sms();
     if (grid > fg.nbricks) grid = fg.nbricks;
     if (grid < 1) grid = 1;
-    kern<<<(unsigned)grid, BRICK_ELEMS, smem, st>>>(x, y, w, fm, kt, fg); count_launch();
+    kern<<<(unsigned)grid, BRICK_ELEMS, smem, st>>>(x, y, w, fm, kt, fg, ktc); count_launch();
+}
+
+// FP64 MR-2 operator with the coefficients passed in the launch (ktab: the
+// kMr2Nonzeros non-zero Walsh-Hadamard coefficients, host memory).
+void launch_fine_apply64_const(const double *x, double *y, const double *w, const uint8_t *freemask,
+                               const double *ktab, const FineGeom &fg, cudaStream_t st) {
+    Mr2Table t;
+    memcpy(t.v, ktab, sizeof(t.v));
+    launch_fine64_staged<2, Mr2Table>(x, y, w, freemask, nullptr, fg, st, t);
+}
+
+// The non-zero coefficients of the shared-memory table (padded to the vector
+// width `elem_bytes`) in the unpadded order of Mr2Table.
+void fine_mr2_const_table(const std::vector<double> &kt_padded, int elem_bytes, std::vector<double> &out) {
+    const int wv = elem_bytes == 8 ? 2 : 4;
+    out.clear();
+    for (int t = 0; t < KE_PACK; ++t)
+        for (int k = 0; k < mr2_nz(t); ++k) out.push_back(kt_padded[(size_t)mr2_off(t, wv) + k]);
 }
 
 template <typename T, typename TW>
 void launch_fine_apply(const T *x, T *y, const TW *w, const uint8_t *freemask, const T *kt, const FineGeom &fg, int n,
                        cudaStream_t st) {
     if constexpr (sizeof(T) == 8) {
-        if (n == 1) return launch_fine64_staged<1>(x, y, w, freemask, kt, fg, st);
-        if (n == 2) return launch_fine64_staged<2>(x, y, w, freemask, kt, fg, st);
+        if (n == 1) return launch_fine64_staged<1>(x, y, w, freemask, kt, fg, st, NoTable{});
+        if (n == 2) return launch_fine64_staged<2>(x, y, w, freemask, kt, fg, st, NoTable{});
     }
     if (n == 1) launch_fine_t<T, TW, 1>(x, y, w, freemask, kt, fg, st);
     else if (n == 2) launch_fine_t<T, TW, 2>(x, y, w, freemask, kt, fg, st);

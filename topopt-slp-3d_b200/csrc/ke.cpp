@@ -93,6 +93,48 @@ void pack_upper(const std::vector<double> &ks, int ns, std::vector<double> &pack
     }
 }
 
+// Galerkin sub-cell table for the finest coarsening: for child c of a coarse
+// element and sub-cube s of that child, S_(c,s) = Pi_c' KE_s Pi_c, where Pi_c
+// interpolates the coarse element's 8 nodes to the child's 8 nodes with the
+// trilinear weights of I/Prolongation.m:24-52.  Stored packed upper
+// (row-major, i <= j), q = c * n^3 + s.
+void coarse_fine_table(const std::vector<double> &ks, int n, std::vector<double> &S) {
+    const int ns = n * n * n;
+    auto phi1 = [](int f, int A) {
+        const int d = f - 2 * A;
+        return d == 0 ? 1.0 : ((d == 1 || d == -1) ? 0.5 : 0.0);
+    };
+    S.assign((size_t)8 * ns * KE_PACK, 0.0);
+    for (int c = 0; c < 8; ++c) {
+        double W[8][8];
+        const int cdx = (c >> 1) & 1, cdy = c & 1, cdz = (c >> 2) & 1;
+        for (int a = 0; a < 8; ++a)
+            for (int A = 0; A < 8; ++A)
+                W[a][A] = phi1(cdx + ((a >> 1) & 1), (A >> 1) & 1) * phi1(cdy + (a & 1), A & 1) *
+                          phi1(cdz + ((a >> 2) & 1), (A >> 2) & 1);
+        for (int s = 0; s < ns; ++s) {
+            const double *K = &ks[(size_t)s * 576];
+            double T[24][24];   // K Pi_c
+            for (int i = 0; i < 24; ++i)
+                for (int J = 0; J < 24; ++J) {
+                    const int B = J / 3, cb = J % 3;
+                    double v = 0.0;
+                    for (int b = 0; b < 8; ++b) v += K[i * 24 + b * 3 + cb] * W[b][B];
+                    T[i][J] = v;
+                }
+            double *out = &S[((size_t)c * ns + s) * KE_PACK];
+            int t = 0;
+            for (int I = 0; I < 24; ++I)
+                for (int J = I; J < 24; ++J) {
+                    const int A = I / 3, ca = I % 3;
+                    double v = 0.0;
+                    for (int a = 0; a < 8; ++a) v += W[a][A] * T[a * 3 + ca][J];
+                    out[t++] = v;
+                }
+        }
+    }
+}
+
 // Filter neighbourhood of I/ElemNeighborhood.m:93-122.  For each z-offset
 // kz <= floor(rmin/ew): x-reach floor(sqrt(rmin^2-dz^2)/el); for each x-offset:
 // y-reach floor(sqrt(rmin^2-dz^2-dx^2)/eh).  Gaussian (opfilter 1) or hat

@@ -51,8 +51,10 @@ struct tosp_handle {
     int64_t *d_freeidx = nullptr;
     // constants
     double *d_ke64 = nullptr;       // blocks packed per s (coarse build, Grad)
+    double *d_cbS = nullptr;        // sub-cell Galerkin table of the finest coarsening
     double *d_kt64 = nullptr;       // pair-major layout of the fine operator
     float *d_kt32 = nullptr;
+    std::vector<double> ktab_c;     // MR 2: FP64 Walsh-Hadamard coefficients passed with each launch
     uint16_t *d_tcimg = nullptr;    // mixed, MR 2: tensor-core B operand image of the blocks
     int *d_tcerr = nullptr;         // set by the tensor-core operator when an MMA wait times out
     // densities
@@ -184,12 +186,20 @@ int choose_levels(int nelx, int nely, int nelz, int ngrids, int nmaxchol, std::s
 }
 
 // ----- operators -------------------------------------------------------------
+// The FP64 finest-level kernel (coefficients as a launch parameter for MR 2).
+void launch_fine64(tosp_handle *h, const double *x, double *y) {
+    if (h->n == 2 && !h->ktab_c.empty())
+        launch_fine_apply64_const(x, y, h->d_w64, h->lev[0].fm, h->ktab_c.data(), h->fg, h->stream);
+    else
+        launch_fine_apply<double, double>(x, y, h->d_w64, h->lev[0].fm, h->d_kt64, h->fg, h->n, h->stream);
+}
+
 // y = K x at the finest level in the cycle precision (zeroes y first).
 template <typename T>
 int fine_apply(tosp_handle *h, const T *x, T *y) {
     CK(cudaMemsetAsync(y, 0, sizeof(T) * h->fg.g.ndof, h->stream));
     if constexpr (sizeof(T) == 8) {
-        launch_fine_apply<double, double>(x, y, h->d_w64, h->lev[0].fm, h->d_kt64, h->fg, h->n, h->stream);
+        launch_fine64(h, x, y);
     } else if (h->d_tcimg) {
         launch_fine_apply_tc(x, y, h->d_wbf, h->lev[0].fm, h->d_tcimg, h->fg, h->d_tcerr, h->stream);
     } else {
@@ -446,9 +456,16 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
     pack_upper(ks, h->ns, packed);
     TRY(dalloc(h, &h->d_ke64, (int64_t)packed.size()));
     CK(cudaMemcpy(h->d_ke64, packed.data(), sizeof(double) * packed.size(), cudaMemcpyHostToDevice));
+    if (h->mg_ok) {
+        std::vector<double> S;
+        coarse_fine_table(ks, h->n, S);
+        TRY(dalloc(h, &h->d_cbS, (int64_t)S.size()));
+        CK(cudaMemcpy(h->d_cbS, S.data(), sizeof(double) * S.size(), cudaMemcpyHostToDevice));
+    }
     {
         std::vector<double> kt64, kt32d;
         fine_block_table(packed, h->n, 8, kt64);
+        if (h->n == 2) fine_mr2_const_table(kt64, 8, h->ktab_c);
         fine_block_table(packed, h->n, 4, kt32d);
         std::vector<float> kt32(kt32d.begin(), kt32d.end());
         TRY(dalloc(h, &h->d_kt64, (int64_t)kt64.size()));
@@ -585,7 +602,8 @@ int setup_levels(tosp_handle *h) {
         launch_convert<double, float>(h->cs, (float *)h->lev[0].invd, nd0, h->stream);
     }
     CKL();
-    launch_coarse_from_fine(wh, h->lev[0].fm, h->d_ke64, h->lev[1].Ae, h->fg, h->lev[1].g, h->n, h->stream);
+    launch_coarse_from_fine_table(wh, h->lev[0].fm, h->d_ke64, h->d_cbS, h->lev[1].Ae, h->fg, h->lev[1].g, h->n,
+                                  h->stream);
     CKL();
     for (int l = 1; l < ng - 1; ++l) {
         Level &L = h->lev[l];
@@ -1040,8 +1058,7 @@ int tosp_time_operator(tosp_handle *h, int32_t precision, int32_t reps, double *
         if (precision == TOSP_PREC_FP64) {
             CK(cudaMemsetAsync(h->cq, 0, sizeof(double) * g0.ndof, h->stream));
             CK(cudaEventRecord(a, h->stream));
-            launch_fine_apply<double, double>(h->cd, h->cq, h->d_w64, h->lev[0].fm, h->d_kt64, h->fg, h->n,
-                                              h->stream);
+            launch_fine64(h, h->cd, h->cq);
         } else {
             Level &F = h->lev[0];
             CK(cudaMemsetAsync(F.t, 0, sizeof(float) * g0.ndof, h->stream));

@@ -87,6 +87,7 @@ constexpr int STENCIL_VALS = 27 * 9;
 void elem_stiff_mr(double el, double eh, double ew, double nu, int n, std::vector<double> &ks);
 // Pack the upper triangles (row-major i <= j) of ns 24x24 blocks.
 void pack_upper(const std::vector<double> &ks, int ns, std::vector<double> &packed);
+void coarse_fine_table(const std::vector<double> &ks, int n, std::vector<double> &S);
 
 struct FilterTap { int dx, dy, dz; double w; };
 // Neighbour offsets/weights of I/ElemNeighborhood.m:93-122 (all signs).
@@ -113,6 +114,9 @@ int fine_nsp(int n, int elem_bytes);
 // The operator's block table from the row-major packed blocks (n = 2: the
 // Walsh-Hadamard modes; otherwise pair-major with stride fine_nsp).
 void fine_block_table(const std::vector<double> &packed_rowmajor, int n, int elem_bytes, std::vector<double> &kt);
+void fine_mr2_const_table(const std::vector<double> &kt_padded, int elem_bytes, std::vector<double> &out);
+void launch_fine_apply64_const(const double *x, double *y, const double *w, const uint8_t *freemask,
+                               const double *ktab, const FineGeom &fg, cudaStream_t st);
 // Tensor-core finest operator of the mixed V-cycle (MR factor 2): B operand
 // image (BF16 pieces of the blocks, canonical shared-memory layout) and launch.
 void fine_tc_image(const std::vector<double> &packed_rowmajor, std::vector<uint16_t> &img);
@@ -125,8 +129,11 @@ void launch_grad(const double *u, const double *rho, const uint8_t *free_elem, c
                  double *g0, const FineGeom &fg, int n, double p, double emin, double E, cudaStream_t st);
 
 // Galerkin coarse element matrices (FP64, 576 per coarse element).
-void launch_coarse_from_fine(const double *w, const uint8_t *freemask_f, const double *kepack,
-                             double *Ac, const FineGeom &fg, const Grid &gc, int n, cudaStream_t st);
+// Finest coarsening by the sub-cell table (coarse elements whose fine nodes
+// are all free), then the masked triple products for the others.
+void launch_coarse_from_fine_table(const double *w, const uint8_t *freemask_f, const double *kepack,
+                                   const double *S, double *Ac, const FineGeom &fg, const Grid &gc, int n,
+                                   cudaStream_t st);
 void launch_coarse_from_coarse(const double *Af, const uint8_t *freemask_f, const Grid &gf,
                                double *Ac, const Grid &gc, cudaStream_t st);
 // Node stencil from element matrices (masked), plus omega/diag.
