@@ -305,7 +305,8 @@ __global__ void k_assemble_stencil(const double *__restrict__ Ae, const uint8_t 
                 for (int cj = 0; cj < 3; ++cj) {
                     const double v = (fi[ci] && fj[cj]) ? blk[ci * 3 + cj] : 0.0;
                     const int k = o * 9 + ci * 3 + cj;
-                    stv[node_major ? I * STENCIL_VALS + k : (int64_t)k * g.nnodes + I] = (T)v;
+                    if (node_major) stv[I * STENCIL_VALS + k] = (T)v;
+                    else if (o >= 13) stv[(int64_t)(k - 13 * 9) * g.nnodes + I] = (T)v;
                     if (o == 13 && ci == cj) invdiag[3 * I + ci] = (T)((fi[ci] && v != 0.0) ? omega / v : 0.0);
                 }
         }
@@ -325,7 +326,12 @@ template void launch_assemble_stencil<float>(const double *, const uint8_t *, co
                                              double, bool, cudaStream_t);
 
 // ---------------------------------------------------------------------------
-// Stencil products.  One thread per node, 3 dofs.
+// Stencil products.  One thread per node, 3 dofs.  The offset-major layout
+// keeps only the centre and the 13 "upper" offsets (o >= 13, 126 values per
+// node): the block of a lower offset o is the transpose of the block stored
+// at the neighbour J = I + off(o) for the opposite offset 26 - o, so the
+// stencil's bytes are halved and the transposed reads hit nearby z-planes,
+// which stay in L2.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(128)
@@ -342,10 +348,17 @@ k_stencil(const T *__restrict__ stv, const T *__restrict__ x, const T *__restric
             if (jx < 0 || jx >= g.nx || jy < 0 || jy >= g.ny || jz < 0 || jz >= g.nz) continue;
             const int64_t J = I + ((int64_t)oz * g.nx + ox) * g.ny + oy;
             const T x0 = x[3 * J], x1 = x[3 * J + 1], x2 = x[3 * J + 2];
-            const T *s = stv + (int64_t)(o * 9) * g.nnodes + I;
-            a0 += s[0] * x0 + s[g.nnodes] * x1 + s[2 * g.nnodes] * x2;
-            a1 += s[3 * g.nnodes] * x0 + s[4 * g.nnodes] * x1 + s[5 * g.nnodes] * x2;
-            a2 += s[6 * g.nnodes] * x0 + s[7 * g.nnodes] * x1 + s[8 * g.nnodes] * x2;
+            if (o >= 13) {
+                const T *s = stv + (int64_t)((o - 13) * 9) * g.nnodes + I;
+                a0 += s[0] * x0 + s[g.nnodes] * x1 + s[2 * g.nnodes] * x2;
+                a1 += s[3 * g.nnodes] * x0 + s[4 * g.nnodes] * x1 + s[5 * g.nnodes] * x2;
+                a2 += s[6 * g.nnodes] * x0 + s[7 * g.nnodes] * x1 + s[8 * g.nnodes] * x2;
+            } else {
+                const T *s = stv + (int64_t)((13 - o) * 9) * g.nnodes + J;   // block (J, 26 - o), transposed
+                a0 += s[0] * x0 + s[3 * g.nnodes] * x1 + s[6 * g.nnodes] * x2;
+                a1 += s[g.nnodes] * x0 + s[4 * g.nnodes] * x1 + s[7 * g.nnodes] * x2;
+                a2 += s[2 * g.nnodes] * x0 + s[5 * g.nnodes] * x1 + s[8 * g.nnodes] * x2;
+            }
         }
         if (mode == 0) {
             y[3 * I] = a0; y[3 * I + 1] = a1; y[3 * I + 2] = a2;
@@ -449,6 +462,20 @@ template void launch_jacobi_update<float>(float *, const float *, const float *,
                                           cudaStream_t);
 
 template <typename T>
+__global__ void k_jacobi_out(double *out, const T *x, const T *b, const T *t, const T *invd, int64_t n) {
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = (double)(x[i] + invd[i] * (b[i] - t[i]));
+}
+template <typename T>
+void launch_jacobi_out(double *out, const T *x, const T *b, const T *t, const T *invdiag, int64_t n, cudaStream_t st) {
+    k_jacobi_out<T><<<grid_for(n, 256), 256, 0, st>>>(out, x, b, t, invdiag, n); count_launch();
+}
+template void launch_jacobi_out<double>(double *, const double *, const double *, const double *, const double *,
+                                        int64_t, cudaStream_t);
+template void launch_jacobi_out<float>(double *, const float *, const float *, const float *, const float *, int64_t,
+                                       cudaStream_t);
+
+template <typename T>
 __global__ void k_invert_diag(const T *diag, const uint8_t *fm, T *invd, double omega, int64_t n) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const double d = (double)diag[i];
@@ -506,9 +533,10 @@ template void launch_prolong<double>(const double *, double *, const uint8_t *, 
 template void launch_prolong<float>(const float *, float *, const uint8_t *, const Grid &, const Grid &, bool,
                                     cudaStream_t);
 
+// tf (optional): restrict rf - tf, the residual b - A x of the finest level.
 template <typename T>
-__global__ void k_restrict(const T *__restrict__ rf, T *__restrict__ bc, const uint8_t *__restrict__ fmc, Grid gf,
-                           Grid gc) {
+__global__ void k_restrict(const T *__restrict__ rf, const T *__restrict__ tf, T *__restrict__ bc,
+                           const uint8_t *__restrict__ fmc, Grid gf, Grid gc) {
     for (int64_t J = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; J < gc.nnodes;
          J += (int64_t)gridDim.x * blockDim.x) {
         const int cy = (int)(J % gc.ny), cx = (int)((J / gc.ny) % gc.nx), cz = (int)(J / ((int64_t)gc.ny * gc.nx));
@@ -524,9 +552,15 @@ __global__ void k_restrict(const T *__restrict__ rf, T *__restrict__ bc, const u
                     if (fy < 0 || fy >= gf.ny) continue;
                     const T wt = (dx ? T(0.5) : T(1)) * (dy ? T(0.5) : T(1)) * (dz ? T(0.5) : T(1));
                     const int64_t I = ((int64_t)fz * gf.nx + fx) * gf.ny + fy;
-                    v0 += wt * rf[3 * I];
-                    v1 += wt * rf[3 * I + 1];
-                    v2 += wt * rf[3 * I + 2];
+                    if (tf) {
+                        v0 += wt * (rf[3 * I] - tf[3 * I]);
+                        v1 += wt * (rf[3 * I + 1] - tf[3 * I + 1]);
+                        v2 += wt * (rf[3 * I + 2] - tf[3 * I + 2]);
+                    } else {
+                        v0 += wt * rf[3 * I];
+                        v1 += wt * rf[3 * I + 1];
+                        v2 += wt * rf[3 * I + 2];
+                    }
                 }
             }
         }
@@ -538,8 +572,17 @@ __global__ void k_restrict(const T *__restrict__ rf, T *__restrict__ bc, const u
 
 template <typename T>
 void launch_restrict(const T *rf, T *bc, const uint8_t *freemask_c, const Grid &gf, const Grid &gc, cudaStream_t st) {
-    k_restrict<T><<<grid_for(gc.nnodes, 256), 256, 0, st>>>(rf, bc, freemask_c, gf, gc); count_launch();
+    k_restrict<T><<<grid_for(gc.nnodes, 256), 256, 0, st>>>(rf, nullptr, bc, freemask_c, gf, gc); count_launch();
 }
+template <typename T>
+void launch_restrict_res(const T *bf, const T *tf, T *bc, const uint8_t *freemask_c, const Grid &gf, const Grid &gc,
+                         cudaStream_t st) {
+    k_restrict<T><<<grid_for(gc.nnodes, 256), 256, 0, st>>>(bf, tf, bc, freemask_c, gf, gc); count_launch();
+}
+template void launch_restrict_res<double>(const double *, const double *, double *, const uint8_t *, const Grid &,
+                                          const Grid &, cudaStream_t);
+template void launch_restrict_res<float>(const float *, const float *, float *, const uint8_t *, const Grid &,
+                                         const Grid &, cudaStream_t);
 template void launch_restrict<double>(const double *, double *, const uint8_t *, const Grid &, const Grid &,
                                       cudaStream_t);
 template void launch_restrict<float>(const float *, float *, const uint8_t *, const Grid &, const Grid &,

@@ -76,6 +76,44 @@ void launch_dot(const double *a, const double *b, int64_t n, double *partials, d
     k_reduce_final<<<1, 256, 0, st>>>(partials, RED_BLOCKS, out); count_launch();
 }
 
+// a'b and a'c in one pass over a (partials: 2 * RED_BLOCKS).
+__global__ void k_dot2_partial(const double *a, const double *b, const double *c, int64_t n, double *partials) {
+    __shared__ double sh[32];
+    double s = 0.0, t = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double ai = a[i];
+        s += ai * b[i];
+        t += ai * c[i];
+    }
+    s = block_sum(s, sh);
+    t = block_sum(t, sh);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = s;
+        partials[RED_BLOCKS + blockIdx.x] = t;
+    }
+}
+
+__global__ void k_reduce2_final(const double *partials, int np, double *out0, double *out1) {
+    __shared__ double sh[32];
+    double s = 0.0, t = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) {
+        s += partials[i];
+        t += partials[np + i];
+    }
+    s = block_sum(s, sh);
+    t = block_sum(t, sh);
+    if (threadIdx.x == 0) {
+        out0[0] = s;
+        out1[0] = t;
+    }
+}
+
+void launch_dot2(const double *a, const double *b, const double *c, int64_t n, double *partials, double *out0,
+                 double *out1, cudaStream_t st) {
+    k_dot2_partial<<<RED_BLOCKS, 256, 0, st>>>(a, b, c, n, partials); count_launch();
+    k_reduce2_final<<<1, 256, 0, st>>>(partials, RED_BLOCKS, out0, out1); count_launch();
+}
+
 // Scalar slots (see solver.cpp): 0 rho, 1 gamma2 (previous rho), 2 d'q, 3 r'r,
 // 5 r's_old.  mode 1: first iteration (d = s); 0: beta = rho/gamma2
 // (I/SolveMG.m:43-46); 2: flexible beta = (rho - r's_old)/gamma2.  When sold
@@ -94,8 +132,11 @@ void launch_pcg_direction(double *d, const double *s, double *sold, const double
 }
 
 // x += alpha d ; r -= alpha q ; partial sums of r'r  (alpha = rho / d'q)
+// x += alpha d, r -= alpha q, partial r'r.  For the mixed V-cycle (b0 given)
+// it also writes the next cycle's FP32 right-hand side b0 = r and, when x0 is
+// given, its first Jacobi iterate x0 = invd0 b0 (the sweep from a zero guess).
 __global__ void k_pcg_update(double *x, double *r, const double *d, const double *q, const double *scal, int64_t n,
-                             double *partials) {
+                             double *partials, float *b0, const float *invd0, float *x0) {
     __shared__ double sh[32];
     const double alpha = scal[0] / scal[2];
     double s = 0.0;
@@ -104,6 +145,11 @@ __global__ void k_pcg_update(double *x, double *r, const double *d, const double
         const double ri = r[i] - alpha * q[i];
         r[i] = ri;
         s += ri * ri;
+        if (b0) {
+            const float bi = (float)ri;
+            b0[i] = bi;
+            if (x0) x0[i] = invd0[i] * bi;
+        }
     }
     s = block_sum(s, sh);
     if (threadIdx.x == 0) partials[blockIdx.x] = s;
@@ -122,8 +168,8 @@ __global__ void k_pcg_finalize(const double *partials, int np, double *scal) {
 }
 
 void launch_pcg_update(double *x, double *r, const double *d, const double *q, double *scal, double *partials,
-                       int64_t n, cudaStream_t st) {
-    k_pcg_update<<<RED_BLOCKS, 256, 0, st>>>(x, r, d, q, scal, n, partials); count_launch();
+                       int64_t n, cudaStream_t st, float *b0, const float *invd0, float *x0) {
+    k_pcg_update<<<RED_BLOCKS, 256, 0, st>>>(x, r, d, q, scal, n, partials, b0, invd0, x0); count_launch();
     k_pcg_finalize<<<1, 256, 0, st>>>(partials, RED_BLOCKS, scal); count_launch();
 }
 

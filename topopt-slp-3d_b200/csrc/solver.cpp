@@ -211,8 +211,12 @@ int fine_apply(tosp_handle *h, const T *x, T *y) {
 
 int fine_apply64(tosp_handle *h, const double *x, double *y) { return fine_apply<double>(h, x, y); }
 
+// Damped Jacobi sweeps (I/Smooth.m:14-23).  first_done: the first sweep from
+// a zero guess was already written into lev[l].x (fused into the CG update);
+// out (finest level only): the last sweep is written to out in FP64 instead of
+// lev[l].x (the preconditioned vector of the outer CG).
 template <typename T>
-int smooth(tosp_handle *h, int l, int niter, bool x_zero) {
+int smooth(tosp_handle *h, int l, int niter, bool x_zero, bool first_done = false, double *out = nullptr) {
     Level &L = h->lev[l];
     const int64_t nd = L.g.ndof;
     T *b = (T *)L.b;
@@ -220,10 +224,13 @@ int smooth(tosp_handle *h, int l, int niter, bool x_zero) {
     for (int it = 0; it < niter; ++it) {
         const bool first = x_zero && it == 0;
         if (first) {
-            launch_jacobi_update<T>((T *)L.x, b, nullptr, (const T *)L.invd, nd, 1, h->stream);
+            if (!first_done) launch_jacobi_update<T>((T *)L.x, b, nullptr, (const T *)L.invd, nd, 1, h->stream);
         } else if (l == 0) {
             TRY(fine_apply<T>(h, (const T *)L.x, (T *)L.t));
-            launch_jacobi_update<T>((T *)L.x, b, (const T *)L.t, (const T *)L.invd, nd, 0, h->stream);
+            if (out && it == niter - 1)
+                launch_jacobi_out<T>(out, (const T *)L.x, b, (const T *)L.t, (const T *)L.invd, nd, h->stream);
+            else
+                launch_jacobi_update<T>((T *)L.x, b, (const T *)L.t, (const T *)L.invd, nd, 0, h->stream);
         } else {
             launch_stencil<T>((const T *)L.st, (const T *)L.x, b, (const T *)L.invd, (T *)L.t, L.g, 2, L.nm,
                               h->stream);
@@ -258,14 +265,21 @@ int coarse_solve(tosp_handle *h) {
 
 // VCycle / WCycle (I/VCycle.m:23-43, I/WCycle.m:23-44) on level l, right-hand
 // side lev[l].b, iterate lev[l].x (zero when x_zero).
+// first_done / out: see smooth (finest level of the outermost cycle only).
 template <typename T>
-int cycle_vw(tosp_handle *h, int l, bool x_zero, bool wcycle) {
+int cycle_vw(tosp_handle *h, int l, bool x_zero, bool wcycle, bool first_done = false, double *out = nullptr) {
     const int Lc = h->ngrids - 1;
     Level &L = h->lev[l];
     Level &C = h->lev[l + 1];
-    TRY(smooth<T>(h, l, h->mg.smoothiter1, x_zero));
-    TRY(residual<T>(h, l));
-    launch_restrict<T>((const T *)L.r, (T *)C.b, C.fm, L.g, C.g, h->stream);
+    TRY(smooth<T>(h, l, h->mg.smoothiter1, x_zero, first_done));
+    if (l == 0) {
+        // finest residual b - A x restricted directly (no residual vector)
+        TRY(fine_apply<T>(h, (const T *)L.x, (T *)L.t));
+        launch_restrict_res<T>((const T *)L.b, (const T *)L.t, (T *)C.b, C.fm, L.g, C.g, h->stream);
+    } else {
+        TRY(residual<T>(h, l));
+        launch_restrict<T>((const T *)L.r, (T *)C.b, C.fm, L.g, C.g, h->stream);
+    }
     CKL();
     if (l + 1 == Lc) {
         TRY(coarse_solve<T>(h));
@@ -275,13 +289,13 @@ int cycle_vw(tosp_handle *h, int l, bool x_zero, bool wcycle) {
     }
     launch_prolong<T>((const T *)C.x, (T *)L.x, L.fm, L.g, C.g, true, h->stream);
     CKL();
-    TRY(smooth<T>(h, l, h->mg.smoothiter2, false));
+    TRY(smooth<T>(h, l, h->mg.smoothiter2, false, false, out));
     return TOSP_OK;
 }
 
 // FMVCycle (I/FMVCycle.m:22-39).
 template <typename T>
-int cycle_fmv(tosp_handle *h, int l) {
+int cycle_fmv(tosp_handle *h, int l, double *out = nullptr) {
     const int Lc = h->ngrids - 1;
     Level &L = h->lev[l];
     Level &C = h->lev[l + 1];
@@ -291,25 +305,41 @@ int cycle_fmv(tosp_handle *h, int l) {
     else TRY(cycle_fmv<T>(h, l + 1));
     launch_prolong<T>((const T *)C.x, (T *)L.x, L.fm, L.g, C.g, false, h->stream);
     CKL();
-    return cycle_vw<T>(h, l, false, false);
+    return cycle_vw<T>(h, l, false, false, false, out);
 }
 
+// The mixed CG update can prepare the next cycle's FP32 right-hand side and
+// first Jacobi iterate (V/W cycles with a pre-smoothing sweep).
+bool fused_first_sweep(const tosp_handle *h) { return h->mg.cycle != 2 && h->mg.smoothiter1 >= 1; }
+
 // s = M^{-1} r on full-length FP64 vectors (r, s distinct from the level buffers).
-int precondition(tosp_handle *h, const double *r, double *s) {
+// prepared (mixed only): lev[0].b = float(r) and, when fused_first_sweep,
+// lev[0].x = invD b were written by the CG update.
+int precondition(tosp_handle *h, const double *r, double *s, bool prepared = false) {
     Level &F = h->lev[0];
     const int64_t nd = F.g.ndof;
+    double *out = h->mg.smoothiter2 >= 1 ? s : nullptr;
     if (h->precision == TOSP_PREC_FP64) {
-        CK(cudaMemcpyAsync(F.b, r, sizeof(double) * nd, cudaMemcpyDeviceToDevice, h->stream));
-        if (h->mg.cycle == 2) TRY(cycle_fmv<double>(h, 0));
-        else TRY(cycle_vw<double>(h, 0, true, h->mg.cycle == 1));
-        CK(cudaMemcpyAsync(s, F.x, sizeof(double) * nd, cudaMemcpyDeviceToDevice, h->stream));
+        // the finest level reads r in place
+        void *own_b = F.b;
+        F.b = const_cast<double *>(r);
+        int rc = h->mg.cycle == 2 ? cycle_fmv<double>(h, 0, out) : cycle_vw<double>(h, 0, true, h->mg.cycle == 1,
+                                                                                     false, out);
+        F.b = own_b;
+        TRY(rc);
+        if (!out) CK(cudaMemcpyAsync(s, F.x, sizeof(double) * nd, cudaMemcpyDeviceToDevice, h->stream));
     } else {
-        launch_convert<double, float>(r, (float *)F.b, nd, h->stream);
-        CKL();
-        if (h->mg.cycle == 2) TRY(cycle_fmv<float>(h, 0));
-        else TRY(cycle_vw<float>(h, 0, true, h->mg.cycle == 1));
-        launch_convert<float, double>((const float *)F.x, s, nd, h->stream);
-        CKL();
+        if (!prepared) {
+            launch_convert<double, float>(r, (float *)F.b, nd, h->stream);
+            CKL();
+        }
+        const bool first_done = prepared && fused_first_sweep(h);
+        if (h->mg.cycle == 2) TRY(cycle_fmv<float>(h, 0, out));
+        else TRY(cycle_vw<float>(h, 0, true, h->mg.cycle == 1, first_done, out));
+        if (!out) {
+            launch_convert<float, double>((const float *)F.x, s, nd, h->stream);
+            CKL();
+        }
     }
     return TOSP_OK;
 }
@@ -543,7 +573,7 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
     TRY(dalloc(h, &h->cs, g0.ndof));
     TRY(dalloc(h, &h->cf, g0.ndof));
     if (mg->flexible) TRY(dalloc(h, &h->cso, g0.ndof));
-    TRY(dalloc(h, &h->d_partials, RED_BLOCKS));
+    TRY(dalloc(h, &h->d_partials, 2 * RED_BLOCKS));
     TRY(dalloc(h, &h->d_scal, 16));
     CK(cudaMallocHost(&h->h_scal, sizeof(double) * 16));
     TRY(dalloc(h, &h->d_ufull, g0.ndof));
@@ -676,15 +706,22 @@ int read_scalars(tosp_handle *h) {
 // asynchronous copy of the scalars to pinned host memory.  mode: 1 first
 // iteration, 0 reference beta, 2 flexible beta.
 int cg_iteration(tosp_handle *h, int mode) {
-    const int64_t nd = h->lev[0].g.ndof;
-    TRY(precondition(h, h->cr, h->cs));
-    launch_dot(h->cr, h->cs, nd, h->d_partials, h->d_scal + 0, h->stream);
-    if (mode == 2) launch_dot(h->cr, h->cso, nd, h->d_partials, h->d_scal + 5, h->stream);
+    Level &F = h->lev[0];
+    const int64_t nd = F.g.ndof;
+    const bool mixed = h->precision == TOSP_PREC_MIXED;
+    // iterations after the first find the V-cycle's input prepared by the
+    // previous update (mixed precision)
+    TRY(precondition(h, h->cr, h->cs, mixed && mode != 1));
+    if (mode == 2) launch_dot2(h->cr, h->cs, h->cso, nd, h->d_partials, h->d_scal + 0, h->d_scal + 5, h->stream);
+    else launch_dot(h->cr, h->cs, nd, h->d_partials, h->d_scal + 0, h->stream);
     launch_pcg_direction(h->cd, h->cs, h->mg.flexible ? h->cso : nullptr, h->d_scal, nd, mode, h->stream);
     CKL();
     TRY(fine_apply64(h, h->cd, h->cq));
     launch_dot(h->cd, h->cq, nd, h->d_partials, h->d_scal + 2, h->stream);
-    launch_pcg_update(h->cx, h->cr, h->cd, h->cq, h->d_scal, h->d_partials, nd, h->stream);
+    const bool first = mixed && fused_first_sweep(h);
+    launch_pcg_update(h->cx, h->cr, h->cd, h->cq, h->d_scal, h->d_partials, nd, h->stream,
+                      mixed ? (float *)F.b : nullptr, first ? (const float *)F.invd : nullptr,
+                      first ? (float *)F.x : nullptr);
     CKL();
     CK(cudaMemcpyAsync(h->h_scal, h->d_scal, sizeof(double) * 8, cudaMemcpyDeviceToHost, h->stream));
     return TOSP_OK;

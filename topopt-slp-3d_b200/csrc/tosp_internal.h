@@ -152,6 +152,10 @@ void launch_residual(const T *b, const T *t, T *r, int64_t n, cudaStream_t st);
 template <typename T>
 void launch_jacobi_update(T *x, const T *b, const T *t, const T *invdiag, int64_t n, int first,
                           cudaStream_t st);
+// Last sweep of a cycle written in FP64: out = x + invD (b - t) (computed in T).
+template <typename T>
+void launch_jacobi_out(double *out, const T *x, const T *b, const T *t, const T *invdiag, int64_t n,
+                       cudaStream_t st);
 template <typename T>
 void launch_invert_diag(const T *diag, const uint8_t *freemask, T *invdiag, double omega, int64_t n,
                         cudaStream_t st);
@@ -162,6 +166,10 @@ void launch_prolong(const T *xc, T *xf, const uint8_t *freemask_f, const Grid &g
 template <typename T>
 void launch_restrict(const T *rf, T *bc, const uint8_t *freemask_c, const Grid &gf, const Grid &gc,
                      cudaStream_t st);
+// Restriction of the residual bf - tf (the level-0 residual fused in).
+template <typename T>
+void launch_restrict_res(const T *bf, const T *tf, T *bc, const uint8_t *freemask_c, const Grid &gf,
+                         const Grid &gc, cudaStream_t st);
 void launch_coarse_freemask(const uint8_t *freemask_f, uint8_t *freemask_c, const Grid &gf,
                             const Grid &gc, cudaStream_t st);
 
@@ -187,11 +195,15 @@ void launch_convert(const TI *a, TO *b, int64_t n, cudaStream_t st);
 // Deterministic dot products: out[0] = sum a*b (fixed reduction tree).
 constexpr int RED_BLOCKS = 592;
 void launch_dot(const double *a, const double *b, int64_t n, double *partials, double *out, cudaStream_t st);
+// a'b -> out0 and a'c -> out1 in one pass (partials: 2 * RED_BLOCKS).
+void launch_dot2(const double *a, const double *b, const double *c, int64_t n, double *partials, double *out0,
+                 double *out1, cudaStream_t st);
 // PCG pieces (scalars in device memory, see solver.cpp for the slots).
 void launch_pcg_direction(double *d, const double *s, double *sold, const double *scal, int64_t n, int mode,
                           cudaStream_t st);
 void launch_pcg_update(double *x, double *r, const double *d, const double *q, double *scal, double *partials,
-                       int64_t n, cudaStream_t st);
+                       int64_t n, cudaStream_t st, float *b0 = nullptr, const float *invd0 = nullptr,
+                       float *x0 = nullptr);
 void launch_set_scalar(double *dst, const double *src, cudaStream_t st);
 
 // Handle internals used by entry points that live outside solver.cpp.
