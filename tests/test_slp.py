@@ -53,3 +53,50 @@ def test_slp_oracle_decreases_compliance():
     assert res.iters == 5
     assert res.F < res.history[0]["F"] + 1e-12 or res.F < Fs[0]
     assert abs(np.full(pb.nelem, 1.0) @ res.xstar / pb.nelem - 0.3) < 0.02
+
+
+def _knapsack_by_sort(g, a, c, lo, hi, rtol=1e-9):
+    """Sort-based statement of the same LP (all candidates sorted by cost per
+    unit of constraint), used to check the selection-based solver."""
+    s = np.where(g < 0, hi, lo).astype(np.float64)
+    excess = a @ s - c
+    if excess <= 0:
+        return s
+    cand = np.nonzero((g < 0) & (hi > lo))[0]
+    ratio = -g[cand] / a[cand]
+    srt = np.argsort(ratio, kind="stable")
+    order, ratio = cand[srt], ratio[srt]
+    red = a[order] * (hi[order] - lo[order])
+    newgrp = np.ones(order.size, dtype=bool)
+    newgrp[1:] = ratio[1:] - ratio[:-1] > rtol * np.abs(ratio[1:])
+    gid = np.cumsum(newgrp) - 1
+    gred = np.bincount(gid, weights=red)
+    gcum = np.cumsum(gred)
+    k = int(np.searchsorted(gcum, excess))
+    s[order[gid < k]] = lo[order[gid < k]]
+    frac = (excess - (gcum[k - 1] if k > 0 else 0.0)) / gred[k]
+    grp = order[gid == k]
+    s[grp] = hi[grp] - frac * (hi[grp] - lo[grp])
+    return s
+
+
+@pytest.mark.parametrize("seed", [0, 1, 2, 3])
+def test_knapsack_selection_matches_sort(seed):
+    """The selection-based knapsack equals the full-sort statement, with
+    exact ties (mirrored entries) and near ties inside the 1e-9 group rule."""
+    rng = np.random.default_rng(seed)
+    n = 20000
+    g = rng.standard_normal(n)
+    g[n // 2:] = g[:n // 2]                                  # exact ties
+    g[:50] = g[50:100] * (1 + 1e-12)                         # near ties
+    a = rng.uniform(0.5, 2.0, n)
+    a[n // 2:] = a[:n // 2]
+    lo = np.zeros(n)
+    hi = rng.uniform(0.2, 1.0, n)
+    hi[n // 2:] = hi[:n // 2]
+    for c in (0.05 * (a @ hi), 0.3 * (a @ hi), 0.9 * (a @ hi)):
+        s1, f1, lam, ok = slp.lp_knapsack(g, a, c, lo, hi)
+        s2 = _knapsack_by_sort(g, a, c, lo, hi)
+        assert ok
+        assert np.abs(s1 - s2).max() <= 1e-9
+        assert a @ s1 <= c * (1 + 1e-12)

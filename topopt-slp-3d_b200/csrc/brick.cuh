@@ -18,6 +18,14 @@ namespace tosp {
 __device__ __forceinline__ void brick_atomic_add(double *p, double v) { atomicAdd(p, v); }
 __device__ __forceinline__ void brick_atomic_add(float *p, float v) { atomicAdd(p, v); }
 
+// Brick coordinates of brick b (y fastest); bricks number far below 2^31.
+__device__ __forceinline__ void brick_xyz(int64_t b, const FineGeom &fg, int &bx, int &by, int &bz) {
+    const int i = (int)b, q = i / fg.nby;
+    by = i - q * fg.nby;
+    bz = q / fg.nbx;
+    bx = q - bz * fg.nbx;
+}
+
 // Base node of thread tid's element within the brick.
 __device__ __forceinline__ int brick_base_node(int tid) {
     const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);

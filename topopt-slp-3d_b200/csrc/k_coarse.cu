@@ -32,6 +32,21 @@ static unsigned grid_for(int64_t n, int threads, int max_per_sm = 16) {
     return (unsigned)b;
 }
 
+// (x, y, z) of node I (y fastest); 32-bit division whenever the index fits.
+__device__ __forceinline__ void node_xyz(int64_t I, int ny, int nx, int &x, int &y, int &z) {
+    if (I <= 0x7fffffff) {
+        const int i = (int)I, q = i / ny;
+        y = i - q * ny;
+        z = q / nx;
+        x = q - z * nx;
+    } else {
+        const int64_t q = I / ny;
+        y = (int)(I - q * ny);
+        z = (int)(q / nx);
+        x = (int)(q - (int64_t)z * nx);
+    }
+}
+
 __device__ __forceinline__ double phi1(int f, int A) {
     const int d = f - 2 * A;
     return d == 0 ? 1.0 : ((d == 1 || d == -1) ? 0.5 : 0.0);
@@ -276,7 +291,8 @@ __global__ void k_assemble_stencil(const double *__restrict__ Ae, const uint8_t 
                                    T *__restrict__ stv, T *__restrict__ invdiag, double omega, int node_major) {
     for (int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; I < g.nnodes;
          I += (int64_t)gridDim.x * blockDim.x) {
-        const int y = (int)(I % g.ny), x = (int)((I / g.ny) % g.nx), z = (int)(I / ((int64_t)g.ny * g.nx));
+        int x, y, z;
+        node_xyz(I, g.ny, g.nx, x, y, z);
         uint8_t fi[3];
         for (int c = 0; c < 3; ++c) fi[c] = fmask[3 * I + c];
         for (int o = 0; o < 27; ++o) {
@@ -339,7 +355,8 @@ k_stencil(const T *__restrict__ stv, const T *__restrict__ x, const T *__restric
           T *__restrict__ y, Grid g, int mode) {
     for (int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; I < g.nnodes;
          I += (int64_t)gridDim.x * blockDim.x) {
-        const int yy = (int)(I % g.ny), xx = (int)((I / g.ny) % g.nx), zz = (int)(I / ((int64_t)g.ny * g.nx));
+        int xx, yy, zz;
+        node_xyz(I, g.ny, g.nx, xx, yy, zz);
         T a0 = 0, a1 = 0, a2 = 0;
 #pragma unroll
         for (int o = 0; o < 27; ++o) {
@@ -385,7 +402,8 @@ k_stencil_warp(const T *__restrict__ stv, const T *__restrict__ x, const T *__re
     for (int64_t I = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5; I < g.nnodes; I += nw) {
         T a0 = 0, a1 = 0, a2 = 0;
         if (lane < 27) {
-            const int yy = (int)(I % g.ny), xx = (int)((I / g.ny) % g.nx), zz = (int)(I / ((int64_t)g.ny * g.nx));
+            int xx, yy, zz;
+            node_xyz(I, g.ny, g.nx, xx, yy, zz);
             const int oy = lane % 3 - 1, ox = (lane / 3) % 3 - 1, oz = lane / 9 - 1;
             const int jx = xx + ox, jy = yy + oy, jz = zz + oz;
             if (jx >= 0 && jx < g.nx && jy >= 0 && jy < g.ny && jz >= 0 && jz < g.nz) {
@@ -497,7 +515,8 @@ __global__ void k_prolong(const T *__restrict__ xc, T *__restrict__ xf, const ui
                           Grid gc, int accumulate) {
     for (int64_t I = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; I < gf.nnodes;
          I += (int64_t)gridDim.x * blockDim.x) {
-        const int fy = (int)(I % gf.ny), fx = (int)((I / gf.ny) % gf.nx), fz = (int)(I / ((int64_t)gf.ny * gf.nx));
+        int fx, fy, fz;
+        node_xyz(I, gf.ny, gf.nx, fx, fy, fz);
         const int x0 = fx >> 1, y0 = fy >> 1, z0 = fz >> 1;
         const int nxs = (fx & 1) ? 2 : 1, nys = (fy & 1) ? 2 : 1, nzs = (fz & 1) ? 2 : 1;
         const T wx = (fx & 1) ? T(0.5) : T(1), wy = (fy & 1) ? T(0.5) : T(1), wz = (fz & 1) ? T(0.5) : T(1);
@@ -539,7 +558,8 @@ __global__ void k_restrict(const T *__restrict__ rf, const T *__restrict__ tf, T
                            const uint8_t *__restrict__ fmc, Grid gf, Grid gc) {
     for (int64_t J = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; J < gc.nnodes;
          J += (int64_t)gridDim.x * blockDim.x) {
-        const int cy = (int)(J % gc.ny), cx = (int)((J / gc.ny) % gc.nx), cz = (int)(J / ((int64_t)gc.ny * gc.nx));
+        int cx, cy, cz;
+        node_xyz(J, gc.ny, gc.nx, cx, cy, cz);
         T v0 = 0, v1 = 0, v2 = 0;
         for (int dz = -1; dz <= 1; ++dz) {
             const int fz = 2 * cz + dz;
@@ -593,7 +613,8 @@ template void launch_restrict<float>(const float *, float *, const uint8_t *, co
 __global__ void k_coarse_mask(const uint8_t *fmf, uint8_t *fmc, Grid gf, Grid gc) {
     for (int64_t J = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; J < gc.nnodes;
          J += (int64_t)gridDim.x * blockDim.x) {
-        const int cy = (int)(J % gc.ny), cx = (int)((J / gc.ny) % gc.nx), cz = (int)(J / ((int64_t)gc.ny * gc.nx));
+        int cx, cy, cz;
+        node_xyz(J, gc.ny, gc.nx, cx, cy, cz);
         const int64_t I = ((int64_t)(2 * cz) * gf.nx + 2 * cx) * gf.ny + 2 * cy;
         for (int c = 0; c < 3; ++c) fmc[3 * J + c] = fmf[3 * I + c];
     }

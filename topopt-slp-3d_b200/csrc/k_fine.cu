@@ -203,9 +203,8 @@ k_fine_apply(const T *__restrict__ x, T *__restrict__ y, const TW *__restrict__ 
     const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
 
     for (int64_t brick = blockIdx.x; brick < fg.nbricks; brick += gridDim.x) {
-        const int bby = (int)(brick % fg.nby);
-        const int bbx = (int)((brick / fg.nby) % fg.nbx);
-        const int bbz = (int)(brick / ((int64_t)fg.nby * fg.nbx));
+        int bbx, bby, bbz;
+        brick_xyz(brick, fg, bbx, bby, bbz);
         const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
         __syncthreads();   // previous brick done with xs/ys (and kt loaded)
         for (int i = tid; i < BRICK_NODES * 3; i += BRICK_ELEMS) {
@@ -301,9 +300,8 @@ __device__ __forceinline__ void stage_brick64(int64_t brick, int buf, const doub
                                               const int32_t *rel, const uint16_t *pk, int tid) {
     using L = StagedLayout<N>;
     const Grid &g = fg.g;
-    const int bby = (int)(brick % fg.nby);
-    const int bbx = (int)((brick / fg.nby) % fg.nbx);
-    const int bbz = (int)(brick / ((int64_t)fg.nby * fg.nbx));
+    int bbx, bby, bbz;
+    brick_xyz(brick, fg, bbx, bby, bbz);
     const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
     double *xs = reinterpret_cast<double *>(smem + L::OFF_XS) + buf * L::XS;
     const double *xb = x + brick_base_dof(ex0, ey0, ez0, g);
@@ -363,9 +361,8 @@ k_fine_apply64(const double *__restrict__ x, double *__restrict__ y, const doubl
         __syncthreads();   // this brick's inputs landed; the previous write-out is done
         for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) ys[i] = 0.0;
 
-        const int bby = (int)(brick % fg.nby);
-        const int bbx = (int)((brick / fg.nby) % fg.nbx);
-        const int bbz = (int)(brick / ((int64_t)fg.nby * fg.nbx));
+        int bbx, bby, bbz;
+        brick_xyz(brick, fg, bbx, bby, bbz);
         const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
         const bool valid = ex0 + lx < g.nelx && ey0 + ly < g.nely && ez0 + lz < g.nelz;
         const double *xs = reinterpret_cast<const double *>(smem_raw + L::OFF_XS) + buf * L::XS;

@@ -221,9 +221,8 @@ __device__ __forceinline__ void stage_brick(int64_t brick, int buf, const float 
                                             unsigned char *smem, const int32_t *rel, const uint16_t *pk,
                                             int tid) {
     const Grid &g = fg.g;
-    const int bby = (int)(brick % fg.nby);
-    const int bbx = (int)((brick / fg.nby) % fg.nbx);
-    const int bbz = (int)(brick / ((int64_t)fg.nby * fg.nbx));
+    int bbx, bby, bbz;
+    brick_xyz(brick, fg, bbx, bby, bbz);
     const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
     float *xs = reinterpret_cast<float *>(smem + TC_OFF_XS) + buf * TC_XS_FLOATS;
     const float *xb = x + brick_base_dof(ex0, ey0, ez0, g);
@@ -319,9 +318,8 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
         if (next < fg.nbricks) stage_brick(next, buf ^ 1, x, w, fg, smem_raw, rel, pk, tid);
         cp_async_commit();
 
-        const int bby = (int)(brick % fg.nby);
-        const int bbx = (int)((brick / fg.nby) % fg.nbx);
-        const int bbz = (int)(brick / ((int64_t)fg.nby * fg.nbx));
+        int bbx, bby, bbz;
+        brick_xyz(brick, fg, bbx, bby, bbz);
         const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
         const bool valid = ex0 + lx < g.nelx && ey0 + ly < g.nely && ez0 + lz < g.nelz;
         const uint32_t a_addr = a_addr0 + (uint32_t)(buf * TC_A_BYTES);

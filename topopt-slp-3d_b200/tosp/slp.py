@@ -64,40 +64,101 @@ class SlpResult:
     history: list = field(default_factory=list)
 
 
-def lp_knapsack(g, a, c, lo, hi):
+def _threshold_ratio(ratio, red, excess):
+    """Smallest candidate ratio r with sum(red[ratio <= r]) >= excess, by a
+    weighted quickselect (linear time; no full sort).  A sample first brackets
+    the answer so that the selection runs on a small subset."""
+    r, w = ratio, red
+    offset = 0.0
+    if r.size > 200000:
+        rng = np.random.default_rng(12345)
+        smp = rng.choice(r.size, 20000, replace=False)
+        sr, sw = r[smp], w[smp]
+        o = np.argsort(sr)
+        cw = np.cumsum(sw[o]) * (float(w.sum()) / float(sw.sum()))
+        j = int(np.searchsorted(cw, excess))
+        lo_b = sr[o[max(j - 400, 0)]] if j - 400 >= 0 else -np.inf
+        hi_b = sr[o[min(j + 400, o.size - 1)]] if j + 400 < o.size else np.inf
+        s_below = float(np.sum(w, where=r < lo_b))
+        mid = (r >= lo_b) & (r <= hi_b)
+        s_mid = float(np.sum(w, where=mid))
+        if s_below < excess <= s_below + s_mid:
+            r, w, offset = r[mid], w[mid], s_below
+    while True:
+        if r.size == 0:                 # round-off in the running sums
+            return float(ratio.max())
+        pivot = np.partition(r, r.size // 2)[r.size // 2]
+        lt = r < pivot
+        s_lt = float(w[lt].sum())
+        if offset + s_lt >= excess and s_lt > 0.0:
+            r, w = r[lt], w[lt]
+            continue
+        eq = r == pivot
+        s_eq = float(w[eq].sum())
+        if offset + s_lt + s_eq >= excess:
+            return pivot
+        offset += s_lt + s_eq
+        gt = ~(lt | eq)
+        r, w = r[gt], w[gt]
+
+
+def lp_knapsack(g, a, c, lo, hi, rtol=1e-9):
     """min g's  s.t.  a's <= c, lo <= s <= hi  with a > 0.
 
     Returns (s, fval, lam, ok): start from the unconstrained minimiser
     (hi where g < 0, lo elsewhere); if a's > c, lower the variables that cost
     least per unit of constraint (smallest |g|/a among g < 0) until a's = c.
-    lam is the multiplier of the inequality (>= 0, MATLAB's lambda.ineqlin).
+    Candidates whose ratios differ by at most rtol (relative, chained) form one
+    group that moves by a common fraction, so the step does not depend on
+    round-off between mirror-symmetric elements.  lam is the multiplier of the
+    inequality (>= 0, MATLAB's lambda.ineqlin).
+
+    The threshold ratio is found by weighted selection; only the candidates in
+    a narrow window around it are sorted to form the groups.
     """
     s = np.where(g < 0, hi, lo).astype(np.float64)
     excess = a @ s - c
     if excess <= 0:
         return s, float(g @ s), 0.0, True
-    cand = np.nonzero((g < 0) & (hi > lo))[0]
-    ratio = -g[cand] / a[cand]
-    srt = np.argsort(ratio, kind="stable")
-    order, ratio = cand[srt], ratio[srt]
-    red = a[order] * (hi[order] - lo[order])        # constraint reduction if moved fully to lo
-    # equal ratios (mirror-symmetric elements) form one group that moves by a
-    # common fraction, so the step does not depend on round-off between them
-    newgrp = np.ones(order.size, dtype=bool)
-    newgrp[1:] = ratio[1:] - ratio[:-1] > 1e-9 * np.abs(ratio[1:])
-    gid = np.cumsum(newgrp) - 1
-    gred = np.bincount(gid, weights=red)
-    gcum = np.cumsum(gred)
-    k = int(np.searchsorted(gcum, excess))
-    if k >= gred.size:
+    candm = (g < 0) & (hi > lo)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ratio = np.where(candm, -g / a, np.inf)       # cost per unit of constraint
+    red = np.where(candm, a * (hi - lo), 0.0)          # reduction if moved fully to lo
+    if not candm.any() or float(red.sum()) < excess:
         return None, None, None, False                # infeasible within the box
-    done = gid < k
-    s[order[done]] = lo[order[done]]
-    prev = gcum[k - 1] if k > 0 else 0.0
+    cand = np.nonzero(candm)[0]
+    rstar = _threshold_ratio(ratio[cand], red[cand], excess)
+    width = 1e-3
+    while True:
+        lo_r, hi_r = rstar * (1 - width), rstar * (1 + width)
+        w_idx = np.nonzero((ratio >= lo_r) & (ratio <= hi_r))[0]
+        w_idx = w_idx[np.argsort(ratio[w_idx], kind="stable")]
+        wr = ratio[w_idx]
+        # groups chain by gaps <= rtol; a chain reaching the window edge could
+        # continue outside it, so widen the window then
+        gaps_ok = wr[1:] - wr[:-1] > rtol * np.abs(wr[1:])
+        edge_lo = wr[0] - lo_r <= rtol * abs(wr[0])
+        edge_hi = hi_r - wr[-1] <= rtol * abs(hi_r)
+        if not (edge_lo or edge_hi) or width >= 1.0:
+            break
+        width = min(1.0, width * 10)
+    below = ratio < lo_r
+    offset = float(np.sum(red, where=below))
+    newgrp = np.ones(wr.size, dtype=bool)
+    newgrp[1:] = gaps_ok
+    gid = np.cumsum(newgrp) - 1
+    gred = np.bincount(gid, weights=red[w_idx])
+    gcum = offset + np.cumsum(gred)
+    k = min(int(np.searchsorted(gcum, excess)), gred.size - 1)
+    grp_sel = gid == k
+    gmin = wr[grp_sel][0]
+    done = ratio < gmin                               # every earlier group moves fully to lo
+    s = np.where(done, lo, s)
+    prev = gcum[k - 1] if k > 0 else offset
     frac = (excess - prev) / gred[k]
-    grp = order[gid == k]
+    grp = w_idx[grp_sel]
     s[grp] = hi[grp] - frac * (hi[grp] - lo[grp])
-    lam = float(np.mean(ratio[gid == k]))
+    lam = float(np.mean(wr[grp_sel]))
     return s, float(g @ s), lam, True
 
 
