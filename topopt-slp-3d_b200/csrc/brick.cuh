@@ -50,6 +50,41 @@ __device__ __forceinline__ void brick_accumulate(T *ys, const T (&acc)[24], bool
     }
 }
 
+// Same with the brick's nodes padded to float4 (ys4[ln] = (x, y, z, -)): one
+// vector read-modify-write per corner.
+__device__ __forceinline__ void brick_accumulate4(float4 *ys4, const float (&acc)[24], bool valid, int ln0) {
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        const int dx = (a >> 1) & 1, dy = a & 1, dz = (a >> 2) & 1;
+        const int ln = ln0 + (dz * NBX + dx) * NBY + dy;
+        if (valid) {
+            float4 v = ys4[ln];
+            v.x += acc[3 * a];
+            v.y += acc[3 * a + 1];
+            v.z += acc[3 * a + 2];
+            ys4[ln] = v;
+        }
+        __syncthreads();
+    }
+}
+
+// FP64 nodes padded to 4 values: a 16-byte pair and a scalar per corner.
+__device__ __forceinline__ void brick_accumulate_pad(double *ys, const double (&acc)[24], bool valid, int ln0) {
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+        const int dx = (a >> 1) & 1, dy = a & 1, dz = (a >> 2) & 1;
+        const int ln = ln0 + (dz * NBX + dx) * NBY + dy;
+        if (valid) {
+            double2 v = reinterpret_cast<double2 *>(ys)[2 * ln];
+            v.x += acc[3 * a];
+            v.y += acc[3 * a + 1];
+            reinterpret_cast<double2 *>(ys)[2 * ln] = v;
+            ys[4 * ln + 2] += acc[3 * a + 2];
+        }
+        __syncthreads();
+    }
+}
+
 constexpr int BRICK_SLOTS = BRICK_NODES * 3;
 
 // Per-CTA table of the brick's node-value slots (i = 3 * local node + c):
@@ -79,8 +114,9 @@ __device__ __forceinline__ int64_t brick_base_dof(int ex0, int ey0, int ez0, con
     return 3 * (((int64_t)ez0 * g.nx + ex0) * g.ny + ey0);
 }
 
-// Write-out through the slot table.
-template <typename T>
+// Write-out through the slot table; NP values per node in ys (3, or 4 when
+// the nodes are padded).
+template <typename T, int NP = 3>
 __device__ __forceinline__ void brick_writeout_tab(const T *ys, T *__restrict__ y, const uint8_t *__restrict__ freemask,
                                                    const Grid &g, int ex0, int ey0, int ez0, const int32_t *rel,
                                                    const uint16_t *pk, int tid) {
@@ -91,8 +127,9 @@ __device__ __forceinline__ void brick_writeout_tab(const T *ys, T *__restrict__ 
         if (!interior && !brick_slot_in(p, ex0, ey0, ez0, g)) continue;
         const int64_t dof = base + rel[i];
         if (freemask[dof]) {
-            if (p >> 10) y[dof] = ys[i];
-            else brick_atomic_add(&y[dof], ys[i]);
+            const T v = ys[NP == 3 ? i : i + i / 3];
+            if (p >> 10) y[dof] = v;
+            else brick_atomic_add(&y[dof], v);
         }
     }
 }

@@ -285,13 +285,14 @@ template <int N>
 struct StagedLayout {
     static constexpr int NS = N * N * N;
     static constexpr int KT = (FineShape<double, N>::KT_LEN + 1) / 2 * 2;   // doubles, 16-byte multiple
-    static constexpr int XS = (BRICK_SLOTS + 1) / 2 * 2;                     // 676
+    static constexpr int XS = BRICK_NODES * 4;                               // nodes padded to 4 values
+    static constexpr int SLOTS = (BRICK_SLOTS + 1) / 2 * 2;                  // slot table length
     static constexpr size_t OFF_XS = sizeof(double) * KT;
     static constexpr size_t OFF_YS = OFF_XS + sizeof(double) * 2 * XS;
     static constexpr size_t OFF_WS = OFF_YS + sizeof(double) * XS;
     static constexpr size_t OFF_REL = OFF_WS + sizeof(double) * 2 * NS * BRICK_ELEMS;
-    static constexpr size_t OFF_PK = OFF_REL + sizeof(int32_t) * XS;
-    static constexpr size_t BYTES = OFF_PK + sizeof(uint16_t) * XS;
+    static constexpr size_t OFF_PK = OFF_REL + sizeof(int32_t) * SLOTS;
+    static constexpr size_t BYTES = OFF_PK + sizeof(uint16_t) * SLOTS;
 };
 
 template <int N>
@@ -306,11 +307,11 @@ __device__ __forceinline__ void stage_brick64(int64_t brick, int buf, const doub
     double *xs = reinterpret_cast<double *>(smem + L::OFF_XS) + buf * L::XS;
     const double *xb = x + brick_base_dof(ex0, ey0, ez0, g);
     if (brick_interior(ex0, ey0, ez0, g)) {
-        for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) cp_async8(xs + i, xb + rel[i], 8);
+        for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) cp_async8(xs + i + i / 3, xb + rel[i], 8);
     } else {
         for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) {
             const bool in = brick_slot_in(pk[i], ex0, ey0, ez0, g);
-            cp_async8(xs + i, in ? xb + rel[i] : x, in ? 8 : 0);
+            cp_async8(xs + i + i / 3, in ? xb + rel[i] : x, in ? 8 : 0);
         }
     }
     const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
@@ -359,7 +360,8 @@ k_fine_apply64(const double *__restrict__ x, double *__restrict__ y, const doubl
         asm volatile("cp.async.commit_group;" ::: "memory");
         asm volatile("cp.async.wait_group 1;" ::: "memory");
         __syncthreads();   // this brick's inputs landed; the previous write-out is done
-        for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) ys[i] = 0.0;
+        for (int i = tid; i < 2 * BRICK_NODES; i += BRICK_ELEMS)
+            reinterpret_cast<double2 *>(ys)[i] = make_double2(0.0, 0.0);
 
         int bbx, bby, bbz;
         brick_xyz(brick, fg, bbx, bby, bbz);
@@ -376,8 +378,10 @@ k_fine_apply64(const double *__restrict__ x, double *__restrict__ y, const doubl
             for (int a = 0; a < 8; ++a) {
                 const int dx = (a >> 1) & 1, dy = a & 1, dz = (a >> 2) & 1;
                 const int ln = ln0 + (dz * NBX + dx) * NBY + dy;
-#pragma unroll
-                for (int c = 0; c < 3; ++c) u[3 * a + c] = xs[3 * ln + c];
+                const double2 v01 = reinterpret_cast<const double2 *>(xs)[2 * ln];
+                u[3 * a] = v01.x;
+                u[3 * a + 1] = v01.y;
+                u[3 * a + 2] = xs[4 * ln + 2];
             }
             if constexpr (N == 2) {
                 double wh[8];
@@ -406,8 +410,8 @@ k_fine_apply64(const double *__restrict__ x, double *__restrict__ y, const doubl
             }
         }
         __syncthreads();   // ys cleared by every thread
-        brick_accumulate(ys, acc, valid, ln0);
-        brick_writeout_tab(ys, y, freemask, g, ex0, ey0, ez0, rel, pk, tid);
+        brick_accumulate_pad(ys, acc, valid, ln0);
+        brick_writeout_tab<double, 4>(ys, y, freemask, g, ex0, ey0, ez0, rel, pk, tid);
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
 }

@@ -47,7 +47,8 @@ constexpr int TC_GROUP = 8 * TC_K * 2;                // bytes of one 8-row grou
 constexpr int TC_B_TILE = TC_ROWS_B / 8 * TC_GROUP;   // 9728 per B tile
 constexpr int TC_B_BYTES = 2 * TC_B_TILE;             // B1 then B2
 constexpr int TC_A_BYTES = BRICK_ELEMS / 8 * TC_GROUP;        // 4096 per A buffer
-constexpr int TC_XS_FLOATS = (BRICK_NODES * 3 + 3) / 4 * 4;   // 676
+constexpr int TC_XS_FLOATS = BRICK_NODES * 4;                  // 900: nodes padded to float4
+constexpr int TC_SLOTS_PAD = (BRICK_SLOTS + 3) / 4 * 4;       // slot table length
 constexpr int TC_COLS = 128;                          // tensor-memory columns per CTA (2 x 64)
 constexpr int TC_CHUNK = 64;
 constexpr int TC_NCHUNK = 5;                          // 4 x 64 + 48 columns
@@ -207,8 +208,8 @@ constexpr size_t TC_OFF_A = TC_B_BYTES;
 constexpr size_t TC_OFF_XS = TC_OFF_A + 2 * TC_A_BYTES;
 constexpr size_t TC_OFF_YS = TC_OFF_XS + sizeof(float) * 2 * TC_XS_FLOATS;
 constexpr size_t TC_OFF_REL = TC_OFF_YS + sizeof(float) * TC_XS_FLOATS;
-constexpr size_t TC_OFF_PK = TC_OFF_REL + sizeof(int32_t) * TC_XS_FLOATS;
-constexpr size_t TC_SMEM_USED = TC_OFF_PK + sizeof(uint16_t) * TC_XS_FLOATS;
+constexpr size_t TC_OFF_PK = TC_OFF_REL + sizeof(int32_t) * TC_SLOTS_PAD;
+constexpr size_t TC_SMEM_USED = TC_OFF_PK + sizeof(uint16_t) * TC_SLOTS_PAD;
 constexpr size_t TC_SMEM = 52 * 1024;
 static_assert(TC_OFF_A % 16 == 0 && TC_OFF_XS % 16 == 0 && TC_OFF_YS % 16 == 0, "operand alignment");
 static_assert(TC_OFF_REL % 4 == 0 && TC_OFF_PK % 2 == 0, "slot table alignment");
@@ -227,11 +228,11 @@ __device__ __forceinline__ void stage_brick(int64_t brick, int buf, const float 
     float *xs = reinterpret_cast<float *>(smem + TC_OFF_XS) + buf * TC_XS_FLOATS;
     const float *xb = x + brick_base_dof(ex0, ey0, ez0, g);
     if (brick_interior(ex0, ey0, ez0, g)) {
-        for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) cp_async4(xs + i, xb + rel[i], 4);
+        for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) cp_async4(xs + i + i / 3, xb + rel[i], 4);
     } else {
         for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) {
             const bool in = brick_slot_in(pk[i], ex0, ey0, ez0, g);
-            cp_async4(xs + i, in ? xb + rel[i] : x, in ? 4 : 0);
+            cp_async4(xs + i + i / 3, in ? xb + rel[i] : x, in ? 4 : 0);
         }
     }
     const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
@@ -329,9 +330,10 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
 #pragma unroll
         for (int a = 0; a < 8; ++a) {
             const int dx = (a >> 1) & 1, dy = a & 1, dz = (a >> 2) & 1;
-            const int ln = ln0 + (dz * NBX + dx) * NBY + dy;
-#pragma unroll
-            for (int c = 0; c < 3; ++c) u[3 * a + c] = xs[3 * ln + c];
+            const float4 v = reinterpret_cast<const float4 *>(xs)[ln0 + (dz * NBX + dx) * NBY + dy];
+            u[3 * a] = v.x;
+            u[3 * a + 1] = v.y;
+            u[3 * a + 2] = v.z;
         }
 #pragma unroll
         for (int i = 0; i < 24; ++i) acc[i] = 0.f;
@@ -348,7 +350,8 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
             }
             if (c == 0) {
                 // every thread has finished the previous brick's write-out
-                for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) ys[i] = 0.f;
+                for (int i = tid; i < BRICK_NODES; i += BRICK_ELEMS)
+                    reinterpret_cast<float4 *>(ys)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
             }
             fence_after();
             const uint32_t taddr = tlane + (uint32_t)((c & 1) * TC_CHUNK);
@@ -381,8 +384,8 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
             issue_chunk(0, tmem, a_next, b_addr, mbar0);
             issue_chunk(1, tmem, a_next, b_addr, mbar1);
         }
-        brick_accumulate(ys, acc, valid, ln0);
-        brick_writeout_tab(ys, y, freemask, g, ex0, ey0, ez0, rel, pk, tid);
+        brick_accumulate4(reinterpret_cast<float4 *>(ys), acc, valid, ln0);
+        brick_writeout_tab<float, 4>(ys, y, freemask, g, ex0, ey0, ez0, rel, pk, tid);
     }
     cp_async_wait_0();
 
