@@ -100,3 +100,28 @@ def test_knapsack_selection_matches_sort(seed):
         assert ok
         assert np.abs(s1 - s2).max() <= 1e-9
         assert a @ s1 <= c * (1 + 1e-12)
+
+
+def test_heaviside_projection_keeps_volume():
+    """HeavisideProj (I/HeavisideProj.m): eta is chosen so that the projected
+    volume equals the requested one; the map is monotone, fixes 0 and 1 and
+    sharpens towards 0/1 as beta grows."""
+    rng = np.random.default_rng(5)
+    x = rng.uniform(0.0, 1.0, 5000)
+    velem = np.full(x.size, 1.0 / x.size)
+    prj = slp.PrjParams(op=True)
+    vol = float(velem @ x)
+    prev_gray = np.inf
+    for _ in range(6):
+        xs, prj = slp.heaviside_proj(x, prj, velem, vol, vol, True)
+        assert abs(velem @ xs - vol) <= 1e-10
+        o = np.argsort(x)
+        assert np.all(np.diff(xs[o]) >= -1e-15)
+        gray = float(np.mean((xs > 0.05) & (xs < 0.95)))
+        assert gray <= prev_gray + 1e-12
+        prev_gray = gray
+    c = np.tanh(prj.beta * prj.eta)
+    d = 1.0 / (c + np.tanh(prj.beta * (1.0 - prj.eta)))
+    assert abs((c + np.tanh(prj.beta * (0.0 - prj.eta))) * d) <= 1e-15
+    assert abs((c + np.tanh(prj.beta * (1.0 - prj.eta))) * d - 1.0) <= 1e-15
+    assert prj.beta == 64.0

@@ -49,6 +49,11 @@ class PrjParams:
     lt: float = 0.05
     vumin: float = 0.7
     vlmax: float = 0.3
+    heavi: bool = True
+    eta: float = 0.25
+    beta: float = 1.0
+    dbeta: float = 2.0
+    betamax: float = 1000.0
 
 
 @dataclass
@@ -169,6 +174,45 @@ def lp_highs(g, a, c, lo, hi):
         return None, None, None, False, 0
     lam = float(-res.ineqlin.marginals[0]) if res.ineqlin is not None else 0.0
     return res.x, float(res.fun), lam, True, int(res.nit)
+
+
+def _heav_root(eta, beta, x, velem, s):
+    """Volume of the projected densities minus s (I/HeavRoot.m)."""
+    c = np.tanh(beta * eta)
+    d = 1.0 / (c + np.tanh(beta * (1.0 - eta)))
+    return float(velem @ ((c + np.tanh(beta * (x - eta))) * d)) - s
+
+
+def heaviside_proj(x, prj, velem, scur, sdes, betaupd):
+    """Volume-preserving smooth Heaviside projection (I/HeavisideProj.m:1-40).
+
+    Optionally raises beta (times dbeta, capped at betamax); finds eta in
+    [0, 1] with the projected volume equal to sdes (moving the target towards
+    scur in 20 steps while f(0) f(1) > 0); returns (xstar, prj) with prj's eta
+    and beta updated.  MATLAB's fzero is replaced by Brent's method on [0, 1].
+    """
+    from scipy.optimize import brentq
+    x = np.asarray(x, dtype=np.float64)
+    if betaupd:
+        prj.beta = min(prj.beta * prj.dbeta, prj.betamax)
+    s = sdes
+    f0 = _heav_root(0.0, prj.beta, x, velem, s)
+    f1 = _heav_root(1.0, prj.beta, x, velem, s)
+    i = 0
+    while f0 * f1 > 0 and i < 20:
+        i += 1
+        s = scur * (i / 20.0) + sdes * (1 - i / 20.0)
+        f0 = _heav_root(0.0, prj.beta, x, velem, s)
+        f1 = _heav_root(1.0, prj.beta, x, velem, s)
+    if f0 == 0.0:
+        prj.eta = 0.0
+    elif f1 == 0.0:
+        prj.eta = 1.0
+    else:
+        prj.eta = brentq(lambda e: _heav_root(e, prj.beta, x, velem, s), 0.0, 1.0, xtol=1e-14, rtol=1e-15)
+    c = np.tanh(prj.beta * prj.eta)
+    cd = 1.0 / (c + np.tanh(prj.beta * (1.0 - prj.eta)))
+    return (c + np.tanh(prj.beta * (x - prj.eta))) * cd, prj
 
 
 def grad_proj(x, g, prj, Vmax, velem):
@@ -372,6 +416,16 @@ def str_slp(solver, pb, volfrac, x0, slp=None, prj=None, fixed=None, on_iter=Non
     else:
         res.opstop = 2
     if prj.op:
+        # rounding to 0/1 (I/StrSLP.m:566-592): optional volume-preserving
+        # Heaviside projection, sensitivities at the projected densities, GradProj
+        if prj.heavi:
+            vcur = float(velem @ xfil)
+            xfil, prj = heaviside_proj(xfil, prj, velem, vcur, vcur, False)
+            solver.SetupGMG(xfil)
+            ufull = np.zeros(3 * pb.nnodes)
+            ufull[pb.freedofs] = u
+            Fgrad = solver.Grad(ufull)
+            A = velem / Vmax
         res.xstar = grad_proj(xfil, Fgrad + lam * A, prj, Vmax, velem)
     else:
         res.xstar = xfil
