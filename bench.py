@@ -411,7 +411,7 @@ def main():
                     help="serving stream (seed 7): Poisson arrivals at --rates, p50/p99 latency and solves/s")
     ap.add_argument("--rates", default="10,20,50,100,200,500")
     ap.add_argument("--serving-count", type=int, default=512)
-    ap.add_argument("--slots", type=int, default=4)
+    ap.add_argument("--slots", type=int, default=8)
     ap.add_argument("--budget-gb", type=float, default=64.0)
     ap.add_argument("--profile-solve", action="store_true",
                     help="with --profile-kernels: also one full mixed-precision solve (launch lists)")
