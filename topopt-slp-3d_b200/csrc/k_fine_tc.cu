@@ -53,7 +53,8 @@ constexpr int TC_COLS = 128;                          // tensor-memory columns p
 constexpr int TC_CHUNK = 64;
 constexpr int TC_NCHUNK = 5;                          // 4 x 64 + 48 columns
 constexpr int TC_CTAS_PER_SM = 4;                     // 4 x 128 = 512 columns
-constexpr uint32_t TC_WAIT_LIMIT = 1u << 22;          // try_wait rounds before giving up
+constexpr uint32_t TC_WAIT_LIMIT = 1u << 16;          // try_wait rounds before giving up
+constexpr uint32_t TC_SUSPEND_NS = 20000;             // suspend-time hint of one try_wait round
 
 // Canonical no-swizzle K-major layout with K = 16: 8-row x 16-byte core
 // matrices, the two core matrices of a row group 128 B apart (leading byte
@@ -100,10 +101,10 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred P;\n\t"
-            "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2, %3;\n\t"
             "selp.u32 %0, 1, 0, P;\n\t}\n"
             : "=r"(done)
-            : "r"(mbar), "r"(phase)
+            : "r"(mbar), "r"(phase), "r"(TC_SUSPEND_NS)
             : "memory");
         if (done) return true;
     }
