@@ -56,17 +56,23 @@ void launch_dense_assemble(const double *Ae, const uint8_t *freemask, const Grid
 // P^{-1} of the 32x32 pivot block by a scalar sweep in shared memory.
 __global__ void k_sweep_pivot(const double *A, int64_t npad, int k, double *Pinv, int *info) {
     __shared__ double S[TS][TS + 1];
+    __shared__ double rd;
     const int r = threadIdx.y, c = threadIdx.x;   // 32 x 32
     S[r][c] = A[(int64_t)(k * TS + r) * npad + k * TS + c];
     for (int p = 0; p < TS; ++p) {
         __syncthreads();
-        const double d = S[p][p];
+        if (r == 0 && c == 0) {   // one division per step, shared by all threads
+            const double d = S[p][p];
+            if (!(d > 0.0)) atomicExch(info, 1 + k * TS + p);
+            rd = 1.0 / d;
+        }
+        __syncthreads();
+        const double q = rd;
         double v;
-        if (r == p && c == p) v = -1.0 / d;
-        else if (c == p) v = S[r][p] / d;
-        else if (r == p) v = S[p][c] / d;
-        else v = S[r][c] - S[r][p] * S[p][c] / d;
-        if (r == 0 && c == 0 && !(d > 0.0)) atomicExch(info, 1 + k * TS + p);
+        if (r == p && c == p) v = -q;
+        else if (c == p) v = S[r][p] * q;
+        else if (r == p) v = S[p][c] * q;
+        else v = S[r][c] - S[r][p] * (S[p][c] * q);
         __syncthreads();
         S[r][c] = v;
     }
@@ -90,21 +96,50 @@ __global__ void k_sweep_panel(const double *A, int64_t npad, int k, const double
     C[(int64_t)(i * TS + r) * TS + c] = v;
 }
 
-// A_ij -= C_i A_kj for all tiles with i != k and j != k.
-__global__ void k_sweep_update(double *A, int64_t npad, int k, const double *C, int nb) {
-    __shared__ double Ct[TS][TS + 1];
-    __shared__ double Rt[TS][TS + 1];
-    const int t = blockIdx.x;
-    const int i = t / nb, j = t % nb;
-    if (i == k || j == k) return;
-    const int r = threadIdx.y, c = threadIdx.x;
-    Ct[r][c] = C[(int64_t)(i * TS + r) * TS + c];
-    Rt[r][c] = A[(int64_t)(k * TS + r) * npad + j * TS + c];
+// A_ij -= C_i A_kj for all entries outside row and column block k: a
+// rank-32 update by 64 x 64 tiles, 256 threads, 4 x 4 outputs per thread
+// (rows ty + 16 a, columns tx + 16 b) from shared copies of the tile's C rows
+// and A_k columns.
+constexpr int UT = 64;
+__global__ void __launch_bounds__(256) k_sweep_update(double *A, int64_t npad, int k, const double *C, int ntile) {
+    __shared__ double Cs[UT][TS + 1];
+    __shared__ double Rs[TS][UT + 1];
+    const int ti = blockIdx.x / ntile, tj = blockIdx.x % ntile;
+    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+    const int row0 = ti * UT, col0 = tj * UT;
+    for (int e = threadIdx.x; e < UT * TS; e += 256) {
+        const int rr = e / TS, q = e % TS;
+        const int64_t gr = row0 + rr;
+        Cs[rr][q] = gr < npad ? C[gr * TS + q] : 0.0;
+        const int q2 = e / UT, cc = e % UT;
+        const int64_t gc = col0 + cc;
+        Rs[q2][cc] = gc < npad ? A[(int64_t)(k * TS + q2) * npad + gc] : 0.0;
+    }
     __syncthreads();
-    double v = 0.0;
+    double acc[4][4] = {};
 #pragma unroll 8
-    for (int q = 0; q < TS; ++q) v += Ct[r][q] * Rt[q][c];
-    A[(int64_t)(i * TS + r) * npad + j * TS + c] -= v;
+    for (int q = 0; q < TS; ++q) {
+        double cv[4], rv[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) cv[a] = Cs[ty + 16 * a][q];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) rv[b] = Rs[q][tx + 16 * b];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] = fma(cv[a], rv[b], acc[a][b]);
+    }
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int64_t gr = row0 + ty + 16 * a;
+        if (gr >= npad || gr / TS == k) continue;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int64_t gc = col0 + tx + 16 * b;
+            if (gc >= npad || gc / TS == k) continue;
+            A[gr * npad + gc] -= acc[a][b];
+        }
+    }
 }
 
 // Column and row blocks of k: A_ik = C_i, A_ki = C_i', A_kk = -P^{-1}.
@@ -127,12 +162,13 @@ __global__ void k_negate(double *A, int64_t nn) {
 
 int dense_sweep_inverse(double *A, double *C, double *Pinv, int64_t npad, int *d_info, cudaStream_t st) {
     const int nb = (int)(npad / TS);
+    const int ntile = (int)((npad + UT - 1) / UT);
     const dim3 blk(TS, TS);
     cudaMemsetAsync(d_info, 0, sizeof(int), st);
     for (int k = 0; k < nb; ++k) {
         k_sweep_pivot<<<1, blk, 0, st>>>(A, npad, k, Pinv, d_info); count_launch();
         k_sweep_panel<<<nb, blk, 0, st>>>(A, npad, k, Pinv, C); count_launch();
-        k_sweep_update<<<nb * nb, blk, 0, st>>>(A, npad, k, C, nb); count_launch();
+        k_sweep_update<<<ntile * ntile, 256, 0, st>>>(A, npad, k, C, ntile); count_launch();
         k_sweep_setrc<<<nb, blk, 0, st>>>(A, npad, k, C, Pinv); count_launch();
     }
     k_negate<<<1024, 256, 0, st>>>(A, npad * npad); count_launch();
