@@ -248,7 +248,8 @@ def run_slp(args):
                        "rmin": rmin, "lp": lp, "ngrids": ngr, "cycle": "VW"[cycle], "omega": omega},
             "slp": {"accepted": res.iters, "rejected": res.rejected, "opstop": res.opstop, "F_final": res.F,
                     "F_first": res.history[0]["F"] if res.history else None,
-                    "pcg_iterations_total": int(sum(res.pcgit)), "wall_s": round(wall, 3)},
+                    "pcg_iterations_total": int(sum(res.pcgit)), "pcg_iterations": [int(i) for i in res.pcgit],
+                    "unconverged_solves": int(sum(1 for st in res.pcgstatus if st != 0)), "wall_s": round(wall, 3)},
             "time_s": {k: round(v, 3) for k, v in timed.t.items()},
             "time_per_iteration_s": {k: round(v / max(steps, 1), 4) for k, v in timed.t.items()}}
     if prj.op:

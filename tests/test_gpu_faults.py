@@ -1,0 +1,70 @@
+"""Failure detection with faults injected on the host: bad densities, a zero
+load, a stalling mixed-precision solve that the serving loop re-runs in FP64,
+and requests that can never be admitted.  Nothing here faults, traps or hangs
+the GPU: every failure is a status code read back by the host."""
+import numpy as np
+import pytest
+
+from tosp import problems as P
+from tosp import workloads as W
+
+pytestmark = pytest.mark.gpu
+
+
+def _solver(tosp, pb, n=1, prec=0, **kw):
+    mg = dict(ngrids=3, cycle=0, omega=0.6, tolMG=1e-8, maxiterMG=500)
+    mg.update(kw)
+    return tosp.Solver(pb, tosp.default_mg(**mg), precision=prec, mr_n=n, p=3.0, emin=1e-9, opfilter=1,
+                       rmin=1.0 if n > 1 else 1.5)
+
+
+@pytest.mark.parametrize("bad", [np.nan, -0.5])
+def test_invalid_densities_stop_at_setup(tosp_mod, bad):
+    """A NaN or negative density gives a non-positive coarsest pivot: SetupGMG
+    reports TOSP_ERR_BREAKDOWN instead of producing a meaningless hierarchy."""
+    pb = P.cantilever(8, 4, 4)
+    x = np.full(pb.nelem, 0.5)
+    x[:] = bad
+    s = _solver(tosp_mod, pb)
+    with pytest.raises(tosp_mod.TospError) as e:
+        s.SetupGMG(x)
+    assert e.value.code == -4                       # TOSP_ERR_BREAKDOWN
+
+
+def test_zero_load_returns_the_start(tosp_mod):
+    """With f = 0 the reference's loop condition is false from the start
+    (I/SolveMG.m:30): the iterate is returned unchanged after no iteration."""
+    pb = P.cantilever(8, 4, 4)
+    s = _solver(tosp_mod, pb)
+    s.SetupGMG(np.full(pb.nelem, 0.5))
+    u, it, rr, rc = s.SolveMG(np.zeros(pb.f.size), np.zeros(pb.f.size))
+    assert rc == 0 and it == 1
+    assert not np.any(u)
+
+
+def test_stalled_mixed_request_falls_back_to_fp64(tosp_mod):
+    """A mixed-precision request whose residual does not halve within maxstall
+    iterations is re-run in FP64 by the serving loop and still converges."""
+    pb = W.serving_problem(16, "cantilever")
+    x = W.FieldPool(seed=3).field(16, 2, 0, 0.5)
+    srv = tosp_mod.Server(max_slots=1, hbm_budget_bytes=4 << 30)
+    mg = tosp_mod.default_mg(ngrids=3, cycle=0, omega=0.6, tolMG=1e-8, maxiterMG=1000, flexible=1, maxstall=1)
+    rid = srv.submit(pb, x, mg=mg, precision=1, mr_n=2, p=3.0, emin=1e-9, rmin=1.0)
+    srv.wait(rid)
+    u, g, st = srv.result(rid)
+    srv.close()
+    assert st["status"] == 0
+    assert st["precision"] == 0          # finished in FP64
+    assert st["relres"] <= 1e-8
+
+
+def test_unadmittable_request_is_rejected(tosp_mod):
+    """A request larger than the whole HBM budget is refused at submission."""
+    pb = W.serving_problem(32, "bridge")
+    x = W.FieldPool(seed=3).field(32, 2, 0, 0.5)
+    srv = tosp_mod.Server(max_slots=2, hbm_budget_bytes=1 << 20)
+    mg = tosp_mod.default_mg(ngrids=3, cycle=0, omega=0.6, tolMG=1e-8, maxiterMG=1000)
+    with pytest.raises(tosp_mod.TospError) as e:
+        srv.submit(pb, x, mg=mg, precision=1, mr_n=2, p=3.0, emin=1e-9, rmin=1.0)
+    assert e.value.code == -3
+    srv.close()

@@ -67,6 +67,7 @@ class SlpResult:
     opstop: int
     pcgit: list = field(default_factory=list)
     history: list = field(default_factory=list)
+    pcgstatus: list = field(default_factory=list)   # SolveMG status of every solve (0: converged)
 
 
 def _threshold_ratio(ratio, red, excess):
@@ -318,8 +319,9 @@ def str_slp(solver, pb, volfrac, x0, slp=None, prj=None, fixed=None, on_iter=Non
 
     xfil = solver.ApplyFilter(x)
     solver.SetupGMG(xfil)
-    u, pit, _, _ = solver.SolveMG(np.zeros(pb.f.size), pb.f)
+    u, pit, _, pst = solver.SolveMG(np.zeros(pb.f.size), pb.f)
     res.pcgit.append(pit)
+    res.pcgstatus.append(pst)
     Fold = float(pb.f @ u)
     F = Fold
     ufull = np.zeros(3 * pb.nnodes)
@@ -365,8 +367,9 @@ def str_slp(solver, pb, volfrac, x0, slp=None, prj=None, fixed=None, on_iter=Non
         xfil = solver.ApplyFilter(x)
         b = (velem @ xfil - Vmax) / Vmax
         solver.SetupGMG(xfil)
-        u, pit, _, _ = solver.SolveMG(u, pb.f)                # warm start, pcgp.opu0
+        u, pit, _, pst = solver.SolveMG(u, pb.f)              # warm start, pcgp.opu0
         res.pcgit.append(pit)
+        res.pcgstatus.append(pst)
         F = float(pb.f @ u)
         predopt = -fval
         predfsb = abs(bold) - abs(A @ s + bold)
