@@ -227,7 +227,12 @@ def run_slp(args):
     lp = args.lp or lp
     mg = tosp.default_mg(ngrids=ngr, cycle=cycle, omega=omega, smoothiter1=1, smoothiter2=1, tolMG=1e-8,
                          maxiterMG=2000, flexible=1 if prec == tosp.PREC_MIXED else 0)
-    solver = tosp.Solver(pb, mg, precision=prec, mr_n=n, p=3.0, emin=1e-9, opfilter=1, rmin=rmin)
+    if prec == tosp.PREC_MIXED:
+        # high-contrast designs defeat the FP32 V-cycle: stalled mixed solves
+        # are finished in FP64, which then serves the rest of the loop
+        solver = tosp.FallbackSolver(pb, mg, mr_n=n, p=3.0, emin=1e-9, opfilter=1, rmin=rmin, maxstall=100)
+    else:
+        solver = tosp.Solver(pb, mg, precision=prec, mr_n=n, p=3.0, emin=1e-9, opfilter=1, rmin=rmin)
     timed = _Timed(solver)
     x0 = np.full(pb.nelem * n ** 3, volfrac)
     per_it = []
@@ -252,6 +257,8 @@ def run_slp(args):
                     "unconverged_solves": int(sum(1 for st in res.pcgstatus if st != 0)), "wall_s": round(wall, 3)},
             "time_s": {k: round(v, 3) for k, v in timed.t.items()},
             "time_per_iteration_s": {k: round(v / max(steps, 1), 4) for k, v in timed.t.items()}}
+    if prec == tosp.PREC_MIXED:
+        line["slp"]["fp64_fallbacks"] = solver.fallbacks
     if prj.op:
         line["slp"]["volume_rounded"] = float(res.xstar.mean())
         line["slp"]["rounded_fraction_0_1"] = float(np.mean((res.xstar == 0) | (res.xstar == 1)))

@@ -68,3 +68,43 @@ def test_unadmittable_request_is_rejected(tosp_mod):
         srv.submit(pb, x, mg=mg, precision=1, mr_n=2, p=3.0, emin=1e-9, rmin=1.0)
     assert e.value.code == -3
     srv.close()
+
+
+def test_fallback_solver_finishes_stalled_solves_in_fp64(tosp_mod):
+    """FallbackSolver: a mixed solve that stalls (maxstall = 1 forces it) is
+    finished in FP64 from its iterate, and the FP64 path then serves the next
+    solve; the result matches a plain FP64 solve."""
+    pb = P.cantilever(16, 8, 8)
+    dens = np.random.default_rng(5).uniform(0.001, 1.0, pb.nelem * 8)
+    mg = tosp_mod.default_mg(ngrids=3, cycle=0, omega=0.6, tolMG=1e-8, maxiterMG=500)
+    fs = tosp_mod.FallbackSolver(pb, mg, mr_n=2, p=3.0, emin=1e-9, opfilter=1, rmin=1.0, maxstall=1)
+    fs.SetupGMG(dens)
+    u, it, rr, rc = fs.SolveMG(np.zeros(pb.f.size), pb.f)
+    assert rc == 0 and rr <= 1e-8
+    assert fs.fallbacks == 1 and fs.use_fp64
+    ref = _solver(tosp_mod, pb, n=2, ngrids=3)
+    ref.SetupGMG(dens)
+    u64, _, _, _ = ref.SolveMG(np.zeros(pb.f.size), pb.f)
+    assert abs(pb.f @ u - pb.f @ u64) <= 1e-6 * abs(pb.f @ u64)
+    fs.SetupGMG(dens * 0.9 + 0.05)          # the next design goes straight to FP64
+    u2, it2, rr2, rc2 = fs.SolveMG(u, pb.f)
+    assert rc2 == 0 and rr2 <= 1e-8 and fs.fallbacks == 1
+    uf = np.zeros(3 * pb.nnodes)
+    uf[pb.freedofs] = u2
+    ref.SetupGMG(dens * 0.9 + 0.05)
+    go = ref.Grad(uf)
+    assert np.abs(fs.Grad(uf) - go).max() <= 1e-12 * np.abs(go).max()
+    fs.close()
+
+
+def test_fallback_solver_keeps_converging_mixed_solves(tosp_mod):
+    """Without a stall the mixed path answers and no FP64 handle is made."""
+    pb = P.cantilever(16, 8, 8)
+    dens = np.random.default_rng(6).uniform(0.001, 1.0, pb.nelem * 8)
+    mg = tosp_mod.default_mg(ngrids=3, cycle=0, omega=0.6, tolMG=1e-8, maxiterMG=500)
+    fs = tosp_mod.FallbackSolver(pb, mg, mr_n=2, p=3.0, emin=1e-9, opfilter=1, rmin=1.0, maxstall=100)
+    fs.SetupGMG(dens)
+    u, it, rr, rc = fs.SolveMG(np.zeros(pb.f.size), pb.f)
+    assert rc == 0 and rr <= 1e-8
+    assert fs.fallbacks == 0 and fs.fp64 is None
+    fs.close()

@@ -26,6 +26,11 @@ __device__ __forceinline__ void brick_xyz(int64_t b, const FineGeom &fg, int &bx
     bx = q - bz * fg.nbx;
 }
 
+// Whether brick b's write-out must read the free-dof mask.
+__device__ __forceinline__ bool brick_check_fixed(int64_t b, const FineGeom &fg) {
+    return fg.bfix == nullptr || fg.bfix[b] != 0;
+}
+
 // Base node of thread tid's element within the brick.
 __device__ __forceinline__ int brick_base_node(int tid) {
     const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
@@ -115,18 +120,19 @@ __device__ __forceinline__ int64_t brick_base_dof(int ex0, int ey0, int ez0, con
 }
 
 // Write-out through the slot table; NP values per node in ys (3, or 4 when
-// the nodes are padded).
+// the nodes are padded).  check = false: no node of the brick has a fixed
+// dof, so the free-dof mask is not read.
 template <typename T, int NP = 3>
 __device__ __forceinline__ void brick_writeout_tab(const T *ys, T *__restrict__ y, const uint8_t *__restrict__ freemask,
                                                    const Grid &g, int ex0, int ey0, int ez0, const int32_t *rel,
-                                                   const uint16_t *pk, int tid) {
+                                                   const uint16_t *pk, int tid, bool check = true) {
     const int64_t base = brick_base_dof(ex0, ey0, ez0, g);
     const bool interior = brick_interior(ex0, ey0, ez0, g);
     for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) {
         const uint16_t p = pk[i];
         if (!interior && !brick_slot_in(p, ex0, ey0, ez0, g)) continue;
         const int64_t dof = base + rel[i];
-        if (freemask[dof]) {
+        if (!check || freemask[dof]) {
             const T v = ys[NP == 3 ? i : i + i / 3];
             if (p >> 10) y[dof] = v;
             else brick_atomic_add(&y[dof], v);

@@ -356,6 +356,7 @@ k_fine_apply64(const double *__restrict__ x, double *__restrict__ y, const doubl
     asm volatile("cp.async.commit_group;" ::: "memory");
     for (int64_t brick = blockIdx.x; brick < fg.nbricks; brick += gridDim.x, buf ^= 1) {
         const int64_t next = brick + gridDim.x;
+        const bool chk = brick_check_fixed(brick, fg);
         if (next < fg.nbricks) stage_brick64<N>(next, buf ^ 1, x, w, fg, smem_raw, rel, pk, tid);
         asm volatile("cp.async.commit_group;" ::: "memory");
         asm volatile("cp.async.wait_group 1;" ::: "memory");
@@ -411,7 +412,7 @@ k_fine_apply64(const double *__restrict__ x, double *__restrict__ y, const doubl
         }
         __syncthreads();   // ys cleared by every thread
         brick_accumulate_pad(ys, acc, valid, ln0);
-        brick_writeout_tab<double, 4>(ys, y, freemask, g, ex0, ey0, ez0, rel, pk, tid);
+        brick_writeout_tab<double, 4>(ys, y, freemask, g, ex0, ey0, ez0, rel, pk, tid, chk);
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
 }

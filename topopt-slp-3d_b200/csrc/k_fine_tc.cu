@@ -317,6 +317,7 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
         // the other buffers were last read by the previous brick, whose
         // threads have all passed its chunk barriers
         const int64_t next = brick + gridDim.x;
+        const bool chk = brick_check_fixed(brick, fg);
         if (next < fg.nbricks) stage_brick(next, buf ^ 1, x, w, fg, smem_raw, rel, pk, tid);
         cp_async_commit();
 
@@ -386,7 +387,7 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
             issue_chunk(1, tmem, a_next, b_addr, mbar1);
         }
         brick_accumulate4(reinterpret_cast<float4 *>(ys), acc, valid, ln0);
-        brick_writeout_tab<float, 4>(ys, y, freemask, g, ex0, ey0, ez0, rel, pk, tid);
+        brick_writeout_tab<float, 4>(ys, y, freemask, g, ex0, ey0, ez0, rel, pk, tid, chk);
     }
     cp_async_wait_0();
 

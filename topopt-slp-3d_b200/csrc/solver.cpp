@@ -49,6 +49,7 @@ struct tosp_handle {
     Grid dens{};               // density (= design) mesh as a grid of elements
     int64_t nfree = 0;
     int64_t *d_freeidx = nullptr;
+    uint8_t *d_bfix = nullptr;      // per finest brick: touches a fixed dof
     // constants
     double *d_ke64 = nullptr;       // blocks packed per s (coarse build, Grad)
     double *d_cbS = nullptr;        // sub-cell Galerkin table of the finest coarsening
@@ -402,6 +403,25 @@ int build_masks(tosp_handle *h, const int64_t *freedofs, int64_t nfree) {
     h->nfree = nfree;
     CK(cudaMemcpy(h->d_freeidx, idx.data(), sizeof(int64_t) * nfree, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(h->lev[0].fm, fm.data(), g0.ndof, cudaMemcpyHostToDevice));
+    // bricks whose nodes carry a fixed dof: a node at x lies in brick x / BX
+    // and, on a brick boundary, in brick x / BX - 1 (same in y and z)
+    {
+        const FineGeom &fg = h->fg;
+        std::vector<uint8_t> bf((size_t)fg.nbricks, 0);
+        for (int64_t d = 0; d < g0.ndof; ++d) {
+            if (fm[d]) continue;
+            const int64_t node = d / 3;
+            const int ny = (int)(node % g0.ny), nx = (int)((node / g0.ny) % g0.nx), nz = (int)(node / ((int64_t)g0.ny * g0.nx));
+            for (int bz = (nz - 1) / BZ; bz <= nz / BZ; ++bz)
+                for (int bx = (nx - 1) / BX; bx <= nx / BX; ++bx)
+                    for (int by = (ny - 1) / BY; by <= ny / BY; ++by)
+                        if (bx >= 0 && by >= 0 && bz >= 0 && bx < fg.nbx && by < fg.nby && bz < fg.nbz)
+                            bf[((size_t)bz * fg.nbx + bx) * fg.nby + by] = 1;
+        }
+        if (h->d_bfix == nullptr) TRY(dalloc(h, &h->d_bfix, fg.nbricks));
+        CK(cudaMemcpy(h->d_bfix, bf.data(), bf.size(), cudaMemcpyHostToDevice));
+        h->fg.bfix = h->d_bfix;
+    }
     for (int l = 0; l + 1 < h->ngrids; ++l)
         launch_coarse_freemask(h->lev[l].fm, h->lev[l + 1].fm, h->lev[l].g, h->lev[l + 1].g, h->stream);
     CKL();

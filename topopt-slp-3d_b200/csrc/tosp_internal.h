@@ -74,6 +74,9 @@ struct FineGeom {
     int nelx_d, nely_d;        // density mesh (n x finer)
     int nbx, nby, nbz;         // bricks per direction
     int64_t nbricks;
+    // per brick: 1 when one of its nodes has a fixed dof (the write-out then
+    // reads the free-dof mask); null: every brick reads it
+    const uint8_t *bfix;
 };
 
 // Coarse-level stencil: 27 neighbour blocks of 3x3 per node, stored

@@ -23,6 +23,7 @@ LIB_PATH = os.path.join(_HERE, "libtosp.so")
 
 TOSP_OK = 0
 TOSP_NOT_CONVERGED = 1
+TOSP_ERR_BREAKDOWN = -4
 PREC_FP64 = 0
 PREC_MIXED = 1
 STATUS = {0: "OK", 1: "NOT_CONVERGED", -1: "BAD_ARG", -2: "CUDA_ERROR", -3: "OOM", -4: "BREAKDOWN",
@@ -297,6 +298,88 @@ class Solver:
         fd1, fdp = _i64(np.asarray(freedofs) + 1)
         self._check(_lib.tosp_set_freedofs(self.h, fdp, fd1.size))
         self.nfree = fd1.size
+
+
+class FallbackSolver:
+    """The mixed-precision solve path with an FP64 fallback, for designs whose
+    contrast the FP32 V-cycle cannot resolve.
+
+    Same entry points as :class:`Solver`.  A mixed ``SolveMG`` that stalls
+    (relative residual not halved in ``maxstall`` iterations), runs out of
+    iterations or breaks down is finished by an FP64 solve (second handle, same
+    problem and multigrid parameters) started from the mixed iterate; the
+    returned iteration count is the sum of both.  After ``sticky`` fallbacks
+    the FP64 path serves every later solve (an SLP design only gets crisper),
+    so ``SetupGMG`` then builds only the FP64 hierarchy.  ``Grad``,
+    ``ApplyFilter`` and ``Compliance`` are FP64 in both handles and run on the
+    one holding the current densities.
+    """
+
+    def __init__(self, pb, mg=None, mr_n=1, p=3.0, emin=1e-9, opfilter=1, rmin=1.5, maxstall=100, sticky=1,
+                 **kw):
+        mg = mg if mg is not None else default_mg()
+        mgm = MgParams.from_buffer_copy(mg)
+        mgm.maxstall = maxstall
+        mgm.flexible = 1
+        mg64 = MgParams.from_buffer_copy(mg)
+        mg64.maxstall = 0
+        mg64.flexible = 0
+        self._args = dict(mr_n=mr_n, p=p, emin=emin, opfilter=opfilter, rmin=rmin, **kw)
+        self.pb, self._mg64, self.sticky = pb, mg64, sticky
+        self.mixed = Solver(pb, mgm, precision=PREC_MIXED, **self._args)
+        self.fp64 = None
+        self.fallbacks = 0
+        self.use_fp64 = False
+        self._x = None           # densities of the last SetupGMG
+        self._fp64_ready = False
+
+    def _fp64(self):
+        if self.fp64 is None:
+            self.fp64 = Solver(self.pb, self._mg64, precision=PREC_FP64, **self._args)
+        if not self._fp64_ready:
+            self.fp64.SetupGMG(self._x)
+            self._fp64_ready = True
+        return self.fp64
+
+    def _active(self):
+        return self._fp64() if self.use_fp64 else self.mixed
+
+    def close(self):
+        self.mixed.close()
+        if self.fp64 is not None:
+            self.fp64.close()
+
+    def SetupGMG(self, xfil):
+        self._x = np.array(xfil, dtype=np.float64, copy=True)
+        self._fp64_ready = False
+        self._active().SetupGMG(self._x)
+
+    def SolveMG(self, x, f):
+        it0 = 0
+        if not self.use_fp64:
+            try:
+                u, it, rr, rc = self.mixed.SolveMG(x, f)
+            except TospError as e:
+                if e.code != TOSP_ERR_BREAKDOWN:
+                    raise
+                u, it, rc = np.array(x, dtype=np.float64, copy=True), 0, e.code
+            if rc == TOSP_OK:
+                return u, it, rr, rc
+            self.fallbacks += 1
+            x, it0 = u, it
+            if self.fallbacks >= self.sticky:
+                self.use_fp64 = True
+        u, it, rr, rc = self._fp64().SolveMG(x, f)
+        return u, it0 + it, rr, rc
+
+    def Grad(self, u_full, return_unfiltered=False):
+        return self._active().Grad(u_full, return_unfiltered=return_unfiltered)
+
+    def ApplyFilter(self, x, trans=False):
+        return self.mixed.ApplyFilter(x, trans=trans)
+
+    def Compliance(self, f, u):
+        return self.mixed.Compliance(f, u)
 
 
 def _problem_struct(pb, mr_n, p, emin, opfilter, rmin, fixed_dens=None, free_dens_g=None):
