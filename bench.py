@@ -215,7 +215,7 @@ def run_slp(args):
     torch.cuda.set_device(0)
     if args.slp == "config0":
         pb = P.cantilever(48, 24, 24)
-        n, prec, ngr, rmin, volfrac, iters, lp, omega, cycle = 1, tosp.PREC_FP64, 3, 1.5, 0.3, 20, "highs", 0.6, 0
+        n, prec, ngr, rmin, volfrac, iters, lp, omega, cycle = 1, tosp.PREC_FP64, 3, 1.5, 0.3, 20, "knapsack", 0.6, 0
         prj = slp.PrjParams(op=False)
     else:
         pb = P.bridge(160, 80, 40)
@@ -407,6 +407,7 @@ def main():
     ap.add_argument("--fp64-steps", type=int, default=2)
     ap.add_argument("--cpu-iters", type=int, default=2)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-w-cycle", action="store_true", help="skip the secondary W-cycle measurement")
     ap.add_argument("--ngrids", type=int, default=0, help="override the workload's grid count")
     ap.add_argument("--flexible", type=int, default=1, help="flexible (Polak-Ribiere) CG beta in both arms")
     ap.add_argument("--slp", default="", choices=["", "config0", "config3"],
@@ -586,7 +587,7 @@ def main():
                           "nominal_peak_tflops": 37.0}}
     rf32 = {"bound": "hbm", "achieved": round(ach32, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": round(ach32 / peaks["hbm_gbs"], 4), "traffic": traffic.get("fp32_operator_bytes_per_launch"),
-            "kernel": "k_fine_apply_tc2 (V-cycle operator, tcgen05 element matrices)" if n == 2 else
+            "kernel": "k_fine_apply_tc2 (V-cycle operator, tcgen05 sub-cell block products)" if n == 2 else
                       "k_fine_apply<float,bf16> (V-cycle operator)",
             "algorithmic_bytes_per_launch": bytes32, "ms_per_launch": round(ms_op32, 4), "peak_source": peak_kind}
     # the dominant kernel of the timed step carries the contract's roofline
@@ -625,6 +626,24 @@ def main():
         "kernels": kernels,
         "clocks": clk,
     }
+    if not args.no_w_cycle:
+        # the reference's default cycle (W, I/TopOpt3D.m:172-174) on the same
+        # workload, both arms, as a secondary figure
+        mgw = tosp.MgParams.from_buffer_copy(mg)
+        mgw.cycle = 1
+        smw = tosp.Solver(pb, mgw, precision=tosp.PREC_MIXED, **kw)
+        s6w = tosp.Solver(pb, mgw, precision=tosp.PREC_FP64, **kw)
+        per_w, its_w, _ = timed(smw, 2, 1)
+        per_w64, its_w64, _ = timed(s6w, 2, 1)
+        tw, tw64 = max_over_ranks(sum(per_w)), max_over_ranks(sum(per_w64))
+        line["w_cycle"] = {
+            "mixed": {"value": round(world * 2 / (tw * 1e-3), 4), "ms_per_step": round(tw / 2, 3),
+                      "pcg_iterations": its_w[-1][0], "relres": its_w[-1][1]},
+            "fp64": {"value": round(world * 2 / (tw64 * 1e-3), 4), "ms_per_step": round(tw64 / 2, 3),
+                     "pcg_iterations": its_w64[-1][0], "relres": its_w64[-1][1]},
+            "mixed_over_fp64": round(tw64 / tw, 3), "unit": "solves/s"}
+        smw.close()
+        s6w.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args, pb, n, xfil, spec, its_64[-1][0])
     if rank == 0:

@@ -92,6 +92,11 @@ typedef struct tosp_mg_params {
                               stencil node-major and apply it with one warp per node (small
                               levels are latency-bound with one thread per node); 0: 65536,
                               -1: never.  A tuning knob with no reference counterpart.       */
+    int32_t small_cycle_max; /* 0: off (default); k > 0: V/W cycles below the first coarse level
+                              with at most k nodes run as one persistent cooperative kernel
+                              (one launch per visit instead of one per sweep and transfer).
+                              Measured slower than the graph-replayed launches on a B200, so
+                              off by default.  A tuning knob with no reference counterpart.   */
 } tosp_mg_params;
 
 /* Statistics of the last tosp_solve_mg call. */

@@ -97,6 +97,36 @@ def s_fp64_product(tosp_mod, pb, n, dens, x):
     return s.KelemProd(x)
 
 
+@pytest.mark.parametrize("prec,tol", [(0, 1e-13), (1, 1e-6)])
+@pytest.mark.parametrize("cycle", [0, 1])
+@pytest.mark.parametrize("dims,n,ngrids", [((16, 8, 8), 1, 3), ((16, 8, 8), 1, 4), ((16, 8, 8), 2, 4),
+                                           ((32, 16, 16), 1, 5)])
+def test_small_cycle_matches_launch_per_step(tosp_mod, prec, tol, cycle, dims, n, ngrids):
+    """The persistent small-level cycle (one cooperative kernel for the levels
+    below the first small one) gives the cycle of one launch per step: same
+    arithmetic, so equal to rounding; and a solve (CUDA-graph iterations)
+    reaches the same compliance.  (On these small meshes the CG is erratic
+    enough that rounding-level differences move the iteration count by a few
+    per cent, so it is not compared.)"""
+    pb = P.cantilever(*dims)
+    kw = dict(ngrids=ngrids, cycle=cycle, flexible=1 if prec else 0, omega=0.5, maxiterMG=2000)
+    on = solver(tosp_mod, pb, n, prec=prec, small_cycle_max=16384, **kw)
+    off = solver(tosp_mod, pb, n, prec=prec, small_cycle_max=0, **kw)
+    dens = make(pb, n, seed=11)
+    on.SetupGMG(dens)
+    off.SetupGMG(dens)
+    r = np.random.default_rng(4).standard_normal(pb.freedofs.size)
+    for _ in range(2):   # the second application starts from the first one's buffers
+        assert rel(on.MGCycle(r), off.MGCycle(r)) <= tol
+    dens = make(pb, n, seed=12, lo=0.2)
+    on.SetupGMG(dens)
+    off.SetupGMG(dens)
+    u1, it1, rr1, rc1 = on.SolveMG(np.zeros(pb.f.size), pb.f)
+    u0, it0, rr0, rc0 = off.SolveMG(np.zeros(pb.f.size), pb.f)
+    assert rc1 == rc0 == 0
+    assert rr1 <= 1e-8 and abs(pb.f @ u1 - pb.f @ u0) <= 1e-9 * abs(pb.f @ u0)
+
+
 @pytest.mark.parametrize("wsm", [0, -1])
 @pytest.mark.parametrize("cycle", [0, 1, 2])
 @pytest.mark.parametrize("dims,n,ngrids", [((8, 4, 4), 2, 3), ((16, 8, 8), 1, 3), ((16, 8, 8), 1, 4),

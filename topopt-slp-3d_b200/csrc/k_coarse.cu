@@ -510,6 +510,10 @@ template void launch_invert_diag<double>(const double *, const uint8_t *, double
 // ---------------------------------------------------------------------------
 // Trilinear transfers (I/Prolongation.m:24-52 weights 1, 1/2, 1/4, 1/8).
 // ---------------------------------------------------------------------------
+// All 8 candidate parents are read with clamped indices and the absent ones
+// weighted by zero, so the loads issue together (a data-dependent trip count
+// serialises them); the sum keeps the order of the parents, so the result is
+// the same bit for bit.
 template <typename T>
 __global__ void k_prolong(const T *__restrict__ xc, T *__restrict__ xf, const uint8_t *__restrict__ fmf, Grid gf,
                           Grid gc, int accumulate) {
@@ -518,18 +522,28 @@ __global__ void k_prolong(const T *__restrict__ xc, T *__restrict__ xf, const ui
         int fx, fy, fz;
         node_xyz(I, gf.ny, gf.nx, fx, fy, fz);
         const int x0 = fx >> 1, y0 = fy >> 1, z0 = fz >> 1;
-        const int nxs = (fx & 1) ? 2 : 1, nys = (fy & 1) ? 2 : 1, nzs = (fz & 1) ? 2 : 1;
-        const T wx = (fx & 1) ? T(0.5) : T(1), wy = (fy & 1) ? T(0.5) : T(1), wz = (fz & 1) ? T(0.5) : T(1);
+        const T wt = ((fx & 1) ? T(0.5) : T(1)) * ((fy & 1) ? T(0.5) : T(1)) * ((fz & 1) ? T(0.5) : T(1));
         T v0 = 0, v1 = 0, v2 = 0;
-        for (int kz = 0; kz < nzs; ++kz)
-            for (int kx = 0; kx < nxs; ++kx)
-                for (int ky = 0; ky < nys; ++ky) {
-                    const int64_t J = ((int64_t)(z0 + kz) * gc.nx + (x0 + kx)) * gc.ny + (y0 + ky);
-                    const T wt = wx * wy * wz;
-                    v0 += wt * xc[3 * J];
-                    v1 += wt * xc[3 * J + 1];
-                    v2 += wt * xc[3 * J + 2];
+#pragma unroll
+        for (int kz = 0; kz < 2; ++kz) {
+            const bool okz = kz == 0 || (fz & 1);
+            const int cz = min(z0 + kz, gc.nz - 1);
+#pragma unroll
+            for (int kx = 0; kx < 2; ++kx) {
+                const bool okx = kx == 0 || (fx & 1);
+                const int cx = min(x0 + kx, gc.nx - 1);
+#pragma unroll
+                for (int ky = 0; ky < 2; ++ky) {
+                    const bool oky = ky == 0 || (fy & 1);
+                    const int cy = min(y0 + ky, gc.ny - 1);
+                    const T w = (okz && okx && oky) ? wt : T(0);
+                    const int64_t J = ((int64_t)cz * gc.nx + cx) * gc.ny + cy;
+                    v0 += w * xc[3 * J];
+                    v1 += w * xc[3 * J + 1];
+                    v2 += w * xc[3 * J + 2];
                 }
+            }
+        }
         const T v[3] = {v0, v1, v2};
         for (int c = 0; c < 3; ++c) {
             const int64_t d = 3 * I + c;
@@ -552,27 +566,38 @@ template void launch_prolong<double>(const double *, double *, const uint8_t *, 
 template void launch_prolong<float>(const float *, float *, const uint8_t *, const Grid &, const Grid &, bool,
                                     cudaStream_t);
 
-// tf (optional): restrict rf - tf, the residual b - A x of the finest level.
-template <typename T>
+// RES: restrict rf - tf, the residual b - A x of the finest level.  The 27
+// fine neighbours are read with clamped indices, those outside the mesh
+// weighted by zero (loads issue together; same sum, same order).
+template <typename T, bool RES>
 __global__ void k_restrict(const T *__restrict__ rf, const T *__restrict__ tf, T *__restrict__ bc,
-                           const uint8_t *__restrict__ fmc, Grid gf, Grid gc) {
+                           const uint8_t *__restrict__ fmc, Grid gf, Grid gc, const T *__restrict__ invdc,
+                           T *__restrict__ xc) {
     for (int64_t J = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; J < gc.nnodes;
          J += (int64_t)gridDim.x * blockDim.x) {
         int cx, cy, cz;
         node_xyz(J, gc.ny, gc.nx, cx, cy, cz);
         T v0 = 0, v1 = 0, v2 = 0;
+#pragma unroll
         for (int dz = -1; dz <= 1; ++dz) {
             const int fz = 2 * cz + dz;
-            if (fz < 0 || fz >= gf.nz) continue;
+            const bool oz = fz >= 0 && fz < gf.nz;
+            const int fzc = min(max(fz, 0), gf.nz - 1);
+#pragma unroll
             for (int dx = -1; dx <= 1; ++dx) {
                 const int fx = 2 * cx + dx;
-                if (fx < 0 || fx >= gf.nx) continue;
+                const bool ox = fx >= 0 && fx < gf.nx;
+                const int fxc = min(max(fx, 0), gf.nx - 1);
+#pragma unroll
                 for (int dy = -1; dy <= 1; ++dy) {
                     const int fy = 2 * cy + dy;
-                    if (fy < 0 || fy >= gf.ny) continue;
-                    const T wt = (dx ? T(0.5) : T(1)) * (dy ? T(0.5) : T(1)) * (dz ? T(0.5) : T(1));
-                    const int64_t I = ((int64_t)fz * gf.nx + fx) * gf.ny + fy;
-                    if (tf) {
+                    const bool oy = fy >= 0 && fy < gf.ny;
+                    const int fyc = min(max(fy, 0), gf.ny - 1);
+                    const T wt = (oz && ox && oy)
+                                     ? (dx ? T(0.5) : T(1)) * (dy ? T(0.5) : T(1)) * (dz ? T(0.5) : T(1))
+                                     : T(0);
+                    const int64_t I = ((int64_t)fzc * gf.nx + fxc) * gf.ny + fyc;
+                    if constexpr (RES) {
                         v0 += wt * (rf[3 * I] - tf[3 * I]);
                         v1 += wt * (rf[3 * I + 1] - tf[3 * I + 1]);
                         v2 += wt * (rf[3 * I + 2] - tf[3 * I + 2]);
@@ -584,29 +609,34 @@ __global__ void k_restrict(const T *__restrict__ rf, const T *__restrict__ tf, T
                 }
             }
         }
-        bc[3 * J] = fmc[3 * J] ? v0 : T(0);
-        bc[3 * J + 1] = fmc[3 * J + 1] ? v1 : T(0);
-        bc[3 * J + 2] = fmc[3 * J + 2] ? v2 : T(0);
+        const T b[3] = {fmc[3 * J] ? v0 : T(0), fmc[3 * J + 1] ? v1 : T(0), fmc[3 * J + 2] ? v2 : T(0)};
+        for (int c = 0; c < 3; ++c) {
+            bc[3 * J + c] = b[c];
+            if (xc) xc[3 * J + c] = invdc[3 * J + c] * b[c];
+        }
     }
 }
 
 template <typename T>
-void launch_restrict(const T *rf, T *bc, const uint8_t *freemask_c, const Grid &gf, const Grid &gc, cudaStream_t st) {
-    k_restrict<T><<<grid_for(gc.nnodes, 256), 256, 0, st>>>(rf, nullptr, bc, freemask_c, gf, gc); count_launch();
+void launch_restrict(const T *rf, T *bc, const uint8_t *freemask_c, const Grid &gf, const Grid &gc, cudaStream_t st,
+                     const T *invd_c, T *xc) {
+    k_restrict<T, false><<<grid_for(gc.nnodes, 256), 256, 0, st>>>(rf, nullptr, bc, freemask_c, gf, gc, invd_c, xc);
+    count_launch();
 }
 template <typename T>
 void launch_restrict_res(const T *bf, const T *tf, T *bc, const uint8_t *freemask_c, const Grid &gf, const Grid &gc,
-                         cudaStream_t st) {
-    k_restrict<T><<<grid_for(gc.nnodes, 256), 256, 0, st>>>(bf, tf, bc, freemask_c, gf, gc); count_launch();
+                         cudaStream_t st, const T *invd_c, T *xc) {
+    k_restrict<T, true><<<grid_for(gc.nnodes, 256), 256, 0, st>>>(bf, tf, bc, freemask_c, gf, gc, invd_c, xc);
+    count_launch();
 }
 template void launch_restrict_res<double>(const double *, const double *, double *, const uint8_t *, const Grid &,
-                                          const Grid &, cudaStream_t);
+                                          const Grid &, cudaStream_t, const double *, double *);
 template void launch_restrict_res<float>(const float *, const float *, float *, const uint8_t *, const Grid &,
-                                         const Grid &, cudaStream_t);
+                                         const Grid &, cudaStream_t, const float *, float *);
 template void launch_restrict<double>(const double *, double *, const uint8_t *, const Grid &, const Grid &,
-                                      cudaStream_t);
+                                      cudaStream_t, const double *, double *);
 template void launch_restrict<float>(const float *, float *, const uint8_t *, const Grid &, const Grid &,
-                                     cudaStream_t);
+                                     cudaStream_t, const float *, float *);
 
 // Coarse dof is free when the fine dof at the same position is free
 // (I/Prolongation.m:38-46,54).

@@ -54,30 +54,52 @@ __device__ __forceinline__ double block_sum(double v, double *sh) {
     return s;   // valid in thread 0
 }
 
-__global__ void k_dot_partial(const double *a, const double *b, int64_t n, double *partials) {
+// Reductions finish in the last block to arrive (a self-resetting counter
+// after the 2 * RED_BLOCKS partials), which sums the partials in the fixed
+// order of a single-block reduction: one launch per dot, deterministic.
+__device__ __forceinline__ unsigned *red_counter(double *partials) {
+    return reinterpret_cast<unsigned *>(partials + 2 * RED_BLOCKS);
+}
+
+// Call after thread 0 wrote this block's partial(s); true in every thread of
+// the last block, which then sees all partials.
+__device__ __forceinline__ bool last_block(unsigned *counter) {
+    __shared__ bool s_last;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        s_last = atomicInc(counter, gridDim.x - 1) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (s_last) __threadfence();
+    return s_last;
+}
+
+__device__ __forceinline__ double sum_partials(const double *partials, int np, double *sh) {
+    double s = 0.0;
+    for (int i = threadIdx.x; i < np; i += blockDim.x) s += __ldcg(partials + i);
+    return block_sum(s, sh);
+}
+
+__global__ void k_dot_partial(const double *a, const double *b, int64_t n, double *partials, double *out) {
     __shared__ double sh[32];
     double s = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         s += a[i] * b[i];
     s = block_sum(s, sh);
     if (threadIdx.x == 0) partials[blockIdx.x] = s;
-}
-
-__global__ void k_reduce_final(const double *partials, int np, double *out) {
-    __shared__ double sh[32];
-    double s = 0.0;
-    for (int i = threadIdx.x; i < np; i += blockDim.x) s += partials[i];
-    s = block_sum(s, sh);
-    if (threadIdx.x == 0) out[0] = s;
+    if (last_block(red_counter(partials))) {
+        const double t = sum_partials(partials, gridDim.x, sh);
+        if (threadIdx.x == 0) out[0] = t;
+    }
 }
 
 void launch_dot(const double *a, const double *b, int64_t n, double *partials, double *out, cudaStream_t st) {
-    k_dot_partial<<<RED_BLOCKS, 256, 0, st>>>(a, b, n, partials); count_launch();
-    k_reduce_final<<<1, 256, 0, st>>>(partials, RED_BLOCKS, out); count_launch();
+    k_dot_partial<<<RED_BLOCKS, 256, 0, st>>>(a, b, n, partials, out); count_launch();
 }
 
 // a'b and a'c in one pass over a (partials: 2 * RED_BLOCKS).
-__global__ void k_dot2_partial(const double *a, const double *b, const double *c, int64_t n, double *partials) {
+__global__ void k_dot2_partial(const double *a, const double *b, const double *c, int64_t n, double *partials,
+                               double *out0, double *out1) {
     __shared__ double sh[32];
     double s = 0.0, t = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -91,27 +113,19 @@ __global__ void k_dot2_partial(const double *a, const double *b, const double *c
         partials[blockIdx.x] = s;
         partials[RED_BLOCKS + blockIdx.x] = t;
     }
-}
-
-__global__ void k_reduce2_final(const double *partials, int np, double *out0, double *out1) {
-    __shared__ double sh[32];
-    double s = 0.0, t = 0.0;
-    for (int i = threadIdx.x; i < np; i += blockDim.x) {
-        s += partials[i];
-        t += partials[np + i];
-    }
-    s = block_sum(s, sh);
-    t = block_sum(t, sh);
-    if (threadIdx.x == 0) {
-        out0[0] = s;
-        out1[0] = t;
+    if (last_block(red_counter(partials))) {
+        const double s0 = sum_partials(partials, gridDim.x, sh);
+        const double s1 = sum_partials(partials + RED_BLOCKS, gridDim.x, sh);
+        if (threadIdx.x == 0) {
+            out0[0] = s0;
+            out1[0] = s1;
+        }
     }
 }
 
 void launch_dot2(const double *a, const double *b, const double *c, int64_t n, double *partials, double *out0,
                  double *out1, cudaStream_t st) {
-    k_dot2_partial<<<RED_BLOCKS, 256, 0, st>>>(a, b, c, n, partials); count_launch();
-    k_reduce2_final<<<1, 256, 0, st>>>(partials, RED_BLOCKS, out0, out1); count_launch();
+    k_dot2_partial<<<RED_BLOCKS, 256, 0, st>>>(a, b, c, n, partials, out0, out1); count_launch();
 }
 
 // Scalar slots (see solver.cpp): 0 rho, 1 gamma2 (previous rho), 2 d'q, 3 r'r,
@@ -131,11 +145,11 @@ void launch_pcg_direction(double *d, const double *s, double *sold, const double
     k_pcg_direction<<<gridv(n), 256, 0, st>>>(d, s, sold, scal, n, mode); count_launch();
 }
 
-// x += alpha d ; r -= alpha q ; partial sums of r'r  (alpha = rho / d'q)
-// x += alpha d, r -= alpha q, partial r'r.  For the mixed V-cycle (b0 given)
-// it also writes the next cycle's FP32 right-hand side b0 = r and, when x0 is
-// given, its first Jacobi iterate x0 = invd0 b0 (the sweep from a zero guess).
-__global__ void k_pcg_update(double *x, double *r, const double *d, const double *q, const double *scal, int64_t n,
+// x += alpha d, r -= alpha q (alpha = rho / d'q), r'r into slot 3 and
+// gamma2 = rho (last block).  For the mixed V-cycle (b0 given) it also writes
+// the next cycle's FP32 right-hand side b0 = r and, when x0 is given, its
+// first Jacobi iterate x0 = invd0 b0 (the sweep from a zero guess).
+__global__ void k_pcg_update(double *x, double *r, const double *d, const double *q, double *scal, int64_t n,
                              double *partials, float *b0, const float *invd0, float *x0) {
     __shared__ double sh[32];
     const double alpha = scal[0] / scal[2];
@@ -153,24 +167,18 @@ __global__ void k_pcg_update(double *x, double *r, const double *d, const double
     }
     s = block_sum(s, sh);
     if (threadIdx.x == 0) partials[blockIdx.x] = s;
-}
-
-// finalize r'r into slot 3 and roll gamma2 = rho
-__global__ void k_pcg_finalize(const double *partials, int np, double *scal) {
-    __shared__ double sh[32];
-    double s = 0.0;
-    for (int i = threadIdx.x; i < np; i += blockDim.x) s += partials[i];
-    s = block_sum(s, sh);
-    if (threadIdx.x == 0) {
-        scal[3] = s;
-        scal[1] = scal[0];
+    if (last_block(red_counter(partials))) {
+        const double t = sum_partials(partials, gridDim.x, sh);
+        if (threadIdx.x == 0) {
+            scal[3] = t;
+            scal[1] = scal[0];
+        }
     }
 }
 
 void launch_pcg_update(double *x, double *r, const double *d, const double *q, double *scal, double *partials,
                        int64_t n, cudaStream_t st, float *b0, const float *invd0, float *x0) {
     k_pcg_update<<<RED_BLOCKS, 256, 0, st>>>(x, r, d, q, scal, n, partials, b0, invd0, x0); count_launch();
-    k_pcg_finalize<<<1, 256, 0, st>>>(partials, RED_BLOCKS, scal); count_launch();
 }
 
 __global__ void k_set_scalar(double *dst, const double *src) { *dst = *src; }

@@ -1,5 +1,6 @@
 // Handle, multigrid hierarchy, cycles and the MG-preconditioned CG, plus the
 // extern "C" entry points of tosp.h.
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -75,6 +76,14 @@ struct tosp_handle {
     int64_t ncoarse = 0, npad = 0;
     int *d_info = nullptr;
     bool setup_done = false;
+    // persistent small-level cycle: first level it covers (-1: off), its grid
+    // and three step lists (entered with the first sweep done, from zero, warm)
+    int small_l = -1;
+    bool small_built = false;
+    int small_blocks = 0;
+    GridBarrier *d_bar = nullptr;
+    unsigned char *d_steps = nullptr;
+    int small_n[3] = {0, 0, 0};
     cudaGraphExec_t iter_graph = nullptr;   // one CG iteration (it >= 2), captured once per handle
     bool graph_failed = false;
     // CG (FP64, full-length vectors with zeros on fixed dofs)
@@ -264,6 +273,168 @@ int coarse_solve(tosp_handle *h) {
     return TOSP_OK;
 }
 
+// Persistent small-level cycle: step lists that replay cycle_vw / smooth from
+// level small_l down with every buffer resolved (the x / t ping-pong of the
+// stencil sweeps is followed on copies of the level pointers; a final copy
+// returns level small_l's iterate to lev[small_l].x).
+constexpr int SMALL_MAX_STEPS = 2048;
+
+template <typename T>
+struct SmallBuilder {
+    tosp_handle *h;
+    std::vector<SmallStep<T>> out;
+    std::vector<T *> X, Tt;
+
+    SmallStep<T> blank(int kind, const Grid &g) {
+        SmallStep<T> s;
+        memset(&s, 0, sizeof s);
+        s.kind = kind;
+        s.g = g;
+        return s;
+    }
+    void smooth(int l, int niter, bool x_zero, bool first_done) {
+        Level &L = h->lev[l];
+        if (niter == 0 && x_zero) {
+            SmallStep<T> s = blank(SS_COPY, L.g);
+            s.y = X[l];
+            out.push_back(s);
+        }
+        for (int it = 0; it < niter; ++it) {
+            if (x_zero && it == 0) {
+                if (!first_done) {
+                    SmallStep<T> s = blank(SS_JACOBI0, L.g);
+                    s.b = (const T *)L.b;
+                    s.invd = (const T *)L.invd;
+                    s.y = X[l];
+                    out.push_back(s);
+                }
+            } else {
+                SmallStep<T> s = blank(SS_STENCIL, L.g);
+                s.mode = 2;
+                s.st = (const T *)L.st;
+                s.x = X[l];
+                s.b = (const T *)L.b;
+                s.invd = (const T *)L.invd;
+                s.y = Tt[l];
+                out.push_back(s);
+                std::swap(X[l], Tt[l]);
+            }
+        }
+    }
+    void cycle(int l, bool x_zero, bool wcycle, bool first_done) {
+        const int Lc = h->ngrids - 1;
+        Level &L = h->lev[l];
+        Level &C = h->lev[l + 1];
+        smooth(l, h->mg.smoothiter1, x_zero, first_done);
+        const bool fuse = l + 1 < Lc && h->mg.smoothiter1 >= 1;
+        SmallStep<T> r = blank(SS_STENCIL, L.g);
+        r.mode = 1;
+        r.st = (const T *)L.st;
+        r.x = X[l];
+        r.b = (const T *)L.b;
+        r.y = (T *)L.r;
+        out.push_back(r);
+        SmallStep<T> rs = blank(SS_RESTRICT, L.g);
+        rs.gc = C.g;
+        rs.x = (const T *)L.r;
+        rs.y = (T *)C.b;
+        rs.fm = C.fm;
+        if (fuse) {
+            rs.invdc = (const T *)C.invd;
+            rs.xc = X[l + 1];
+        }
+        out.push_back(rs);
+        if (l + 1 == Lc) {
+            SmallStep<T> d = blank(SS_DENSE, C.g);
+            d.b = (const T *)C.b;
+            d.y = X[l + 1];
+            d.X = h->d_Adense;
+            d.n = C.g.ndof;
+            d.npad = h->npad;
+            out.push_back(d);
+        } else {
+            cycle(l + 1, true, wcycle, fuse);
+            if (wcycle) cycle(l + 1, false, wcycle, false);
+        }
+        SmallStep<T> p = blank(SS_PROLONG, L.g);
+        p.gc = C.g;
+        p.x = X[l + 1];
+        p.y = X[l];
+        p.fm = L.fm;
+        out.push_back(p);
+        smooth(l, h->mg.smoothiter2, false, false);
+    }
+    void build(int ls, bool x_zero, bool first_done) {
+        out.clear();
+        X.assign(h->ngrids, nullptr);
+        Tt.assign(h->ngrids, nullptr);
+        for (int l = 0; l < h->ngrids; ++l) {
+            X[l] = (T *)h->lev[l].x;
+            Tt[l] = (T *)h->lev[l].t;
+        }
+        cycle(ls, x_zero, h->mg.cycle == 1, first_done);
+        if (X[ls] != (T *)h->lev[ls].x) {
+            SmallStep<T> c = blank(SS_COPY, h->lev[ls].g);
+            c.x = X[ls];
+            c.y = (T *)h->lev[ls].x;
+            out.push_back(c);
+        }
+    }
+};
+
+// Chooses the first level of the persistent cycle and uploads its step lists
+// (once per handle: the buffers never move).  Off unless small_cycle_max > 0,
+// for FMV cycles, for hierarchies with thread-per-node stencils and when no
+// stencil level is small.
+template <typename T>
+int build_small(tosp_handle *h) {
+    h->small_built = true;
+    h->small_l = -1;
+    const int Lc = h->ngrids - 1;
+    if (!h->mg_ok || h->mg.cycle == 2 || h->mg.small_cycle_max <= 0 || Lc < 2) return TOSP_OK;
+    const int64_t smax = h->mg.small_cycle_max;
+    int ls = -1;
+    for (int l = 1; l < Lc; ++l)
+        if (h->lev[l].g.nnodes <= smax) {
+            ls = l;
+            break;
+        }
+    if (ls < 0) return TOSP_OK;
+    for (int l = ls; l < Lc; ++l)
+        if (!h->lev[l].nm) return TOSP_OK;
+    const int maxb = small_cycle_max_blocks(sizeof(T) == 8);
+    if (maxb < 1) return TOSP_OK;
+    SmallBuilder<T> b{h, {}, {}, {}};
+    std::vector<SmallStep<T>> all;
+    int n[3];
+    const bool variant[3][2] = {{true, true}, {true, false}, {false, false}};
+    for (int v = 0; v < 3; ++v) {
+        b.build(ls, variant[v][0], variant[v][1]);
+        if ((int)b.out.size() > SMALL_MAX_STEPS) return TOSP_OK;
+        n[v] = (int)b.out.size();
+        b.out.resize(SMALL_MAX_STEPS);
+        all.insert(all.end(), b.out.begin(), b.out.end());
+    }
+    TRY(dalloc(h, &h->d_steps, (int64_t)(sizeof(SmallStep<T>) * all.size())));
+    CK(cudaMemcpy(h->d_steps, all.data(), sizeof(SmallStep<T>) * all.size(), cudaMemcpyHostToDevice));
+    TRY(dalloc(h, &h->d_bar, 1));
+    CK(cudaMemset(h->d_bar, 0, sizeof(GridBarrier)));
+    // about two nodes per warp on the largest level, at most what is co-resident
+    const int64_t want = (h->lev[ls].g.nnodes + 15) / 16;
+    h->small_blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, maxb));
+    for (int v = 0; v < 3; ++v) h->small_n[v] = n[v];
+    h->small_l = ls;
+    return TOSP_OK;
+}
+
+template <typename T>
+int small_cycle(tosp_handle *h, int variant) {
+    const SmallStep<T> *steps = reinterpret_cast<const SmallStep<T> *>(h->d_steps) + (size_t)variant * SMALL_MAX_STEPS;
+    launch_small_cycle<T>(steps, h->small_n[variant], h->d_bar, h->small_blocks, h->stream);
+    CKL();
+    return TOSP_OK;
+}
+
 // VCycle / WCycle (I/VCycle.m:23-43, I/WCycle.m:23-44) on level l, right-hand
 // side lev[l].b, iterate lev[l].x (zero when x_zero).
 // first_done / out: see smooth (finest level of the outermost cycle only).
@@ -273,19 +444,26 @@ int cycle_vw(tosp_handle *h, int l, bool x_zero, bool wcycle, bool first_done = 
     Level &L = h->lev[l];
     Level &C = h->lev[l + 1];
     TRY(smooth<T>(h, l, h->mg.smoothiter1, x_zero, first_done));
+    // the restriction also writes the coarse level's first sweep from zero
+    const bool fuse = l + 1 < Lc && h->mg.smoothiter1 >= 1;
+    const T *cinvd = fuse ? (const T *)C.invd : nullptr;
+    T *cx = fuse ? (T *)C.x : nullptr;
     if (l == 0) {
         // finest residual b - A x restricted directly (no residual vector)
         TRY(fine_apply<T>(h, (const T *)L.x, (T *)L.t));
-        launch_restrict_res<T>((const T *)L.b, (const T *)L.t, (T *)C.b, C.fm, L.g, C.g, h->stream);
+        launch_restrict_res<T>((const T *)L.b, (const T *)L.t, (T *)C.b, C.fm, L.g, C.g, h->stream, cinvd, cx);
     } else {
         TRY(residual<T>(h, l));
-        launch_restrict<T>((const T *)L.r, (T *)C.b, C.fm, L.g, C.g, h->stream);
+        launch_restrict<T>((const T *)L.r, (T *)C.b, C.fm, L.g, C.g, h->stream, cinvd, cx);
     }
     CKL();
     if (l + 1 == Lc) {
         TRY(coarse_solve<T>(h));
+    } else if (l + 1 == h->small_l) {
+        TRY(small_cycle<T>(h, fuse ? 0 : 1));
+        if (wcycle) TRY(small_cycle<T>(h, 2));
     } else {
-        TRY(cycle_vw<T>(h, l + 1, true, wcycle));
+        TRY(cycle_vw<T>(h, l + 1, true, wcycle, fuse));
         if (wcycle) TRY(cycle_vw<T>(h, l + 1, false, wcycle));
     }
     launch_prolong<T>((const T *)C.x, (T *)L.x, L.fm, L.g, C.g, true, h->stream);
@@ -593,7 +771,8 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
     TRY(dalloc(h, &h->cs, g0.ndof));
     TRY(dalloc(h, &h->cf, g0.ndof));
     if (mg->flexible) TRY(dalloc(h, &h->cso, g0.ndof));
-    TRY(dalloc(h, &h->d_partials, 2 * RED_BLOCKS));
+    TRY(dalloc(h, &h->d_partials, 2 * RED_BLOCKS + 1));   // + the reductions' arrival counter
+    CK(cudaMemset(h->d_partials, 0, sizeof(double) * (2 * RED_BLOCKS + 1)));
     TRY(dalloc(h, &h->d_scal, 16));
     CK(cudaMallocHost(&h->h_scal, sizeof(double) * 16));
     TRY(dalloc(h, &h->d_ufull, g0.ndof));
@@ -675,6 +854,7 @@ int setup_levels(tosp_handle *h) {
         h->err = "coarsest-grid inversion failed: non-positive pivot at dof " + std::to_string(info - 1);
         return TOSP_ERR_BREAKDOWN;
     }
+    if (!h->small_built) TRY(build_small<T>(h));
     return TOSP_OK;
 }
 
@@ -697,6 +877,15 @@ int need_mg(tosp_handle *h) {
 // Reads (and clears) the tensor-core operator's timeout flag; call after a
 // stream synchronisation.
 int check_tc(tosp_handle *h) {
+    if (h->d_bar) {
+        GridBarrier b{};
+        CK(cudaMemcpy(&b, h->d_bar, sizeof b, cudaMemcpyDeviceToHost));
+        if (b.err) {
+            CK(cudaMemset(h->d_bar, 0, sizeof b));
+            h->err = "persistent coarse cycle: grid barrier wait timed out";
+            return TOSP_ERR_TIMEOUT;
+        }
+    }
     if (!h->d_tcerr) return TOSP_OK;
     int e = 0;
     CK(cudaMemcpy(&e, h->d_tcerr, sizeof(int), cudaMemcpyDeviceToHost));
@@ -874,6 +1063,7 @@ void tosp_default_mg_params(tosp_mg_params *mg) {
     mg->flexible = 0;
     mg->maxstall = 0;
     mg->warp_stencil_max = 0;
+    mg->small_cycle_max = 0;
 }
 
 int tosp_create(const tosp_problem *prob, const tosp_mg_params *mg, int32_t precision, tosp_handle **out) {

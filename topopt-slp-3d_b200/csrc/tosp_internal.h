@@ -163,16 +163,18 @@ template <typename T>
 void launch_invert_diag(const T *diag, const uint8_t *freemask, T *invdiag, double omega, int64_t n,
                         cudaStream_t st);
 // Transfers (masked).  prolong: xf (+)= P xc ; restrict: bc = P^T rf.
+// invd_c / xc (optional): also write the coarse level's first Jacobi sweep
+// from zero, xc = invd_c bc.
 template <typename T>
 void launch_prolong(const T *xc, T *xf, const uint8_t *freemask_f, const Grid &gf, const Grid &gc,
                     bool accumulate, cudaStream_t st);
 template <typename T>
 void launch_restrict(const T *rf, T *bc, const uint8_t *freemask_c, const Grid &gf, const Grid &gc,
-                     cudaStream_t st);
+                     cudaStream_t st, const T *invd_c = nullptr, T *xc = nullptr);
 // Restriction of the residual bf - tf (the level-0 residual fused in).
 template <typename T>
 void launch_restrict_res(const T *bf, const T *tf, T *bc, const uint8_t *freemask_c, const Grid &gf,
-                         const Grid &gc, cudaStream_t st);
+                         const Grid &gc, cudaStream_t st, const T *invd_c = nullptr, T *xc = nullptr);
 void launch_coarse_freemask(const uint8_t *freemask_f, uint8_t *freemask_c, const Grid &gf,
                             const Grid &gc, cudaStream_t st);
 
@@ -184,6 +186,38 @@ void launch_dense_assemble(const double *Ae, const uint8_t *freemask, const Grid
 int dense_sweep_inverse(double *A, double *C, double *Pinv, int64_t npad, int *d_info, cudaStream_t st);
 template <typename T>
 void launch_dense_solve(const double *X, const T *b, T *x, int64_t n, int64_t npad, cudaStream_t st);
+
+// Persistent small-level cycle (k_small.cu): the steps of a V/W cycle below a
+// level, resolved to buffers on the host, run by one cooperative kernel with a
+// grid barrier between steps.
+enum SmallStepKind : int32_t {
+    SS_STENCIL = 0,    // y = b - A x (mode 1) or x + invd (b - A x) (mode 2), warp per node
+    SS_RESTRICT = 1,   // y = P^T x on the coarse grid gc (masked), optional xc = invdc y
+    SS_PROLONG = 2,    // y += P x from the coarse grid gc (masked)
+    SS_JACOBI0 = 3,    // y = invd b (first sweep from zero)
+    SS_DENSE = 4,      // y = X b (coarsest direct solve)
+    SS_COPY = 5,       // y = x (x null: y = 0)
+};
+template <typename T>
+struct SmallStep {
+    int32_t kind, mode;
+    Grid g, gc;                  // the level's grid; a transfer's coarse grid
+    const T *st, *x, *b, *invd;
+    T *y;
+    const uint8_t *fm;           // mask of the written level
+    const T *invdc;              // restriction: the coarse level's first sweep
+    T *xc;
+    const double *X;             // dense solve: inverse, n x n used of npad x npad
+    int64_t n, npad;
+};
+struct GridBarrier {
+    unsigned count, gen;
+    int err, pad;
+};
+// Largest grid of 256-thread blocks that can be co-resident (cooperative launch).
+int small_cycle_max_blocks(bool fp64);
+template <typename T>
+void launch_small_cycle(const SmallStep<T> *steps_dev, int nsteps, GridBarrier *bar, int blocks, cudaStream_t st);
 
 // Filter (I/ApplyFilter.m): trans 0: (W x)./w, 1: W (x./w); weights: w = W 1.
 void launch_filter(const double *x, double *y, const double *wsum, const uint8_t *fixed,

@@ -51,7 +51,7 @@ class MgParams(C.Structure):
     _fields_ = [("ngrids", C.c_int32), ("cycle", C.c_int32), ("smoother", C.c_int32), ("omega", C.c_double),
                 ("smoothiter1", C.c_int32), ("smoothiter2", C.c_int32), ("tolMG", C.c_double),
                 ("maxiterMG", C.c_int32), ("nmaxchol", C.c_int32), ("flexible", C.c_int32),
-                ("maxstall", C.c_int32), ("warp_stencil_max", C.c_int32)]
+                ("maxstall", C.c_int32), ("warp_stencil_max", C.c_int32), ("small_cycle_max", C.c_int32)]
 
 
 class RequestStats(C.Structure):
