@@ -140,6 +140,30 @@ __device__ __forceinline__ void brick_writeout_tab(const T *ys, T *__restrict__ 
     }
 }
 
+// The same write-out node by node, for nodes padded to four values in ys:
+// one slot-table lookup, one range test and one address per node instead of
+// per value (BRICK_NODES / BRICK_ELEMS = 1.8 trips per thread instead of 5.3).
+template <typename T>
+__device__ __forceinline__ void brick_writeout_nodes(const T *ys, T *__restrict__ y,
+                                                     const uint8_t *__restrict__ freemask, const Grid &g, int ex0,
+                                                     int ey0, int ez0, const int32_t *rel, const uint16_t *pk, int tid,
+                                                     bool check) {
+    const int64_t base = brick_base_dof(ex0, ey0, ez0, g);
+    const bool interior = brick_interior(ex0, ey0, ez0, g);
+    for (int ln = tid; ln < BRICK_NODES; ln += BRICK_ELEMS) {
+        const uint16_t p = pk[3 * ln];
+        if (!interior && !brick_slot_in(p, ex0, ey0, ez0, g)) continue;
+        const int64_t dof = base + rel[3 * ln];
+        const T v[3] = {ys[4 * ln], ys[4 * ln + 1], ys[4 * ln + 2]};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (check && !freemask[dof + c]) continue;
+            if (p >> 10) y[dof + c] = v[c];
+            else brick_atomic_add(&y[dof + c], v[c]);
+        }
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void brick_writeout(const T *ys, T *__restrict__ y, const uint8_t *__restrict__ freemask,
                                                const Grid &g, int ex0, int ey0, int ez0, int tid) {

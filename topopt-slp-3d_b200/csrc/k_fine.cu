@@ -306,12 +306,23 @@ __device__ __forceinline__ void stage_brick64(int64_t brick, int buf, const doub
     const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
     double *xs = reinterpret_cast<double *>(smem + L::OFF_XS) + buf * L::XS;
     const double *xb = x + brick_base_dof(ex0, ey0, ez0, g);
+    // node by node: three values into a node's 4-value slot
     if (brick_interior(ex0, ey0, ez0, g)) {
-        for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) cp_async8(xs + i + i / 3, xb + rel[i], 8);
+        for (int ln = tid; ln < BRICK_NODES; ln += BRICK_ELEMS) {
+            const double *src = xb + rel[3 * ln];
+            double *dst = xs + 4 * ln;
+            cp_async8(dst, src, 8);
+            cp_async8(dst + 1, src + 1, 8);
+            cp_async8(dst + 2, src + 2, 8);
+        }
     } else {
-        for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) {
-            const bool in = brick_slot_in(pk[i], ex0, ey0, ez0, g);
-            cp_async8(xs + i + i / 3, in ? xb + rel[i] : x, in ? 8 : 0);
+        for (int ln = tid; ln < BRICK_NODES; ln += BRICK_ELEMS) {
+            const bool in = brick_slot_in(pk[3 * ln], ex0, ey0, ez0, g);
+            const double *src = in ? xb + rel[3 * ln] : x;
+            double *dst = xs + 4 * ln;
+            cp_async8(dst, src, in ? 8 : 0);
+            cp_async8(dst + 1, in ? src + 1 : x, in ? 8 : 0);
+            cp_async8(dst + 2, in ? src + 2 : x, in ? 8 : 0);
         }
     }
     const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
@@ -412,7 +423,7 @@ k_fine_apply64(const double *__restrict__ x, double *__restrict__ y, const doubl
         }
         __syncthreads();   // ys cleared by every thread
         brick_accumulate_pad(ys, acc, valid, ln0);
-        brick_writeout_tab<double, 4>(ys, y, freemask, g, ex0, ey0, ez0, rel, pk, tid, chk);
+        brick_writeout_nodes<double>(ys, y, freemask, g, ex0, ey0, ez0, rel, pk, tid, chk);
     }
     asm volatile("cp.async.wait_group 0;" ::: "memory");
 }

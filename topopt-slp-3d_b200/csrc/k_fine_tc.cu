@@ -223,12 +223,23 @@ __device__ __forceinline__ void stage_brick(int64_t brick, float *xs, unsigned c
     brick_xyz(brick, fg, bbx, bby, bbz);
     const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
     const float *xb = x + brick_base_dof(ex0, ey0, ez0, g);
+    // node by node: three values into a node's float4 slot
     if (brick_interior(ex0, ey0, ez0, g)) {
-        for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) cp_async4(xs + i + i / 3, xb + rel[i], 4);
+        for (int ln = tid; ln < BRICK_NODES; ln += BRICK_ELEMS) {
+            const float *src = xb + rel[3 * ln];
+            float *dst = xs + 4 * ln;
+            cp_async4(dst, src, 4);
+            cp_async4(dst + 1, src + 1, 4);
+            cp_async4(dst + 2, src + 2, 4);
+        }
     } else {
-        for (int i = tid; i < BRICK_SLOTS; i += BRICK_ELEMS) {
-            const bool in = brick_slot_in(pk[i], ex0, ey0, ez0, g);
-            cp_async4(xs + i + i / 3, in ? xb + rel[i] : x, in ? 4 : 0);
+        for (int ln = tid; ln < BRICK_NODES; ln += BRICK_ELEMS) {
+            const bool in = brick_slot_in(pk[3 * ln], ex0, ey0, ez0, g);
+            const float *src = in ? xb + rel[3 * ln] : x;
+            float *dst = xs + 4 * ln;
+            cp_async4(dst, src, in ? 4 : 0);
+            cp_async4(dst + 1, in ? src + 1 : x, in ? 4 : 0);
+            cp_async4(dst + 2, in ? src + 2 : x, in ? 4 : 0);
         }
     }
     const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
@@ -428,7 +439,7 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
             issue_chunk(1, tmem, a_addr, b_addr, mbar1);
         }
         brick_accumulate4(reinterpret_cast<float4 *>(ys), acc, valid, ln0);
-        brick_writeout_tab<float, 4>(ys, y, freemask, g, ex0, ey0, ez0, rel, pk, tid, chk);
+        brick_writeout_nodes<float>(ys, y, freemask, g, ex0, ey0, ez0, rel, pk, tid, chk);
     }
     cp_async_wait_0();
 
