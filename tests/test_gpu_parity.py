@@ -97,7 +97,7 @@ def s_fp64_product(tosp_mod, pb, n, dens, x):
     return s.KelemProd(x)
 
 
-@pytest.mark.parametrize("prec,tol", [(0, 1e-13), (1, 1e-6)])
+@pytest.mark.parametrize("prec,tol", [(0, 1e-13), (1, 5e-5)])
 @pytest.mark.parametrize("cycle", [0, 1])
 @pytest.mark.parametrize("dims,n,ngrids", [((16, 8, 8), 1, 3), ((16, 8, 8), 1, 4), ((16, 8, 8), 2, 4),
                                            ((32, 16, 16), 1, 5)])
@@ -105,7 +105,10 @@ def test_small_cycle_matches_launch_per_step(tosp_mod, prec, tol, cycle, dims, n
     """The persistent small-level cycle (one cooperative kernel for the levels
     below the first small one) gives the cycle of one launch per step: same
     arithmetic, so equal to rounding; and a solve (CUDA-graph iterations)
-    reaches the same compliance.  (On these small meshes the CG is erratic
+    reaches the same compliance.  In mixed precision the finest FP32 product
+    adds brick-face nodes with atomics, so two runs differ at rounding level,
+    which the cycle amplifies to a few 1e-6: hence 5e-5 there.  (On these
+    small meshes the CG is erratic
     enough that rounding-level differences move the iteration count by a few
     per cent, so it is not compared.)"""
     pb = P.cantilever(*dims)

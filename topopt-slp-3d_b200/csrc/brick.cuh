@@ -155,6 +155,26 @@ __device__ __forceinline__ void brick_writeout_nodes(const T *ys, T *__restrict_
         if (!interior && !brick_slot_in(p, ex0, ey0, ez0, g)) continue;
         const int64_t dof = base + rel[3 * ln];
         const T v[3] = {ys[4 * ln], ys[4 * ln + 1], ys[4 * ln + 2]};
+        if constexpr (sizeof(T) == 4) {
+            if (!check) {
+                // FP32: one 8-byte access for the two of the node's three values
+                // that share an 8-byte-aligned pair (decided from the address)
+                // and one 4-byte access for the third
+                float *a = reinterpret_cast<float *>(y + dof);
+                const bool lo = (reinterpret_cast<uintptr_t>(a) & 7u) == 0;
+                float *pair = lo ? a : a + 1;
+                float *one = lo ? a + 2 : a;
+                const float p0 = lo ? v[0] : v[1], p1 = lo ? v[1] : v[2], s1 = lo ? v[2] : v[0];
+                if (p >> 10) {
+                    asm volatile("st.global.v2.f32 [%0], {%1, %2};" ::"l"(pair), "f"(p0), "f"(p1) : "memory");
+                    *one = s1;
+                } else {
+                    asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(pair), "f"(p0), "f"(p1) : "memory");
+                    atomicAdd(one, s1);
+                }
+                continue;
+            }
+        }
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             if (check && !freemask[dof + c]) continue;
