@@ -66,6 +66,7 @@ struct tosp_handle {
     uint8_t *d_free_elem = nullptr;
     // filter
     FilterTap *d_taps = nullptr;
+    int filt_r = 0;                 // largest |offset| of the taps
     int ntaps = 0;
     uint8_t *d_fixed = nullptr;
     double *d_fw = nullptr;
@@ -786,6 +787,9 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
             filter_taps(pb->rmin, eld, ehd, ewd, pb->opfilter, taps);
         }
         h->ntaps = (int)taps.size();
+        h->filt_r = 0;
+        for (const FilterTap &t : taps)
+            h->filt_r = std::max(h->filt_r, std::max(std::abs(t.dx), std::max(std::abs(t.dy), std::abs(t.dz))));
         if (h->ntaps) {
             TRY(dalloc(h, &h->d_taps, h->ntaps));
             CK(cudaMemcpy(h->d_taps, taps.data(), sizeof(FilterTap) * taps.size(), cudaMemcpyHostToDevice));
@@ -806,7 +810,7 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
         TRY(dalloc(h, &h->d_fw, nd));
         if (h->ntaps) {
             launch_filter(nullptr, h->d_fw, nullptr, h->d_fixed, h->d_taps, h->ntaps, h->dens.nelx, h->dens.nely,
-                          h->dens.nelz, 0, 1, h->stream);
+                          h->dens.nelz, 0, 1, h->filt_r, h->stream);
             CKL();
         }
     }
@@ -1219,7 +1223,7 @@ int tosp_apply_filter(tosp_handle *h, const double *x, double *y, int64_t ndens,
         CK(cudaMemcpyAsync(dst, src, sizeof(double) * ndens, cudaMemcpyDefault, h->stream));
     } else {
         launch_filter(src, dst, h->d_fw, h->d_fixed, h->d_taps, h->ntaps, h->dens.nelx, h->dens.nely, h->dens.nelz,
-                      trans ? 1 : 0, 0, h->stream);
+                      trans ? 1 : 0, 0, h->filt_r, h->stream);
         CKL();
     }
     if (!dout) TRY(store_vec(h, y, dst, ndens));
@@ -1257,7 +1261,7 @@ int tosp_grad(tosp_handle *h, const double *u, int64_t nfull, double *fgrad, dou
         CK(cudaMemcpyAsync(dst, h->d_g0, sizeof(double) * ndens, cudaMemcpyDeviceToDevice, h->stream));
     } else {
         launch_filter(h->d_g0, dst, h->d_fw, h->d_fixed, h->d_taps, h->ntaps, h->dens.nelx, h->dens.nely,
-                      h->dens.nelz, 1, 0, h->stream);
+                      h->dens.nelz, 1, 0, h->filt_r, h->stream);
         CKL();
     }
     if (!dout) TRY(store_vec(h, fgrad, dst, ndens));

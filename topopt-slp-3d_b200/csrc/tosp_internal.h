@@ -220,9 +220,11 @@ template <typename T>
 void launch_small_cycle(const SmallStep<T> *steps_dev, int nsteps, GridBarrier *bar, int blocks, cudaStream_t st);
 
 // Filter (I/ApplyFilter.m): trans 0: (W x)./w, 1: W (x./w); weights: w = W 1.
+// radius: largest |offset| of the taps (the shared-memory tile's halo); -1
+// selects the per-element kernel.
 void launch_filter(const double *x, double *y, const double *wsum, const uint8_t *fixed,
                    const FilterTap *taps_dev, int ntaps, int nelx, int nely, int nelz, int trans,
-                   int weights_only, cudaStream_t st);
+                   int weights_only, int radius, cudaStream_t st);
 
 // Vector kernels.
 void launch_scatter_free(const double *v, const int64_t *idx, int64_t nfree, double *full, cudaStream_t st);
