@@ -375,6 +375,28 @@ def run_serving(args):
     return 0
 
 
+def profile_filter(args):
+    import torch
+    import tosp
+    from tosp.workloads import WORKLOADS
+    spec = WORKLOADS[args.workload]
+    pb = tosp.problems.cantilever(*spec["dims"])
+    n = spec["n"]
+    s = tosp.Solver(pb, tosp.default_mg(ngrids=args.ngrids or spec["ngrids"]), precision=tosp.PREC_MIXED, mr_n=n,
+                    p=3.0, emin=1e-9, opfilter=1, rmin=spec["rmin"])   # launches the weights pass
+    nd = pb.nelem * n ** 3
+    x = torch.rand(nd, dtype=torch.float64, device="cuda", generator=torch.Generator("cuda").manual_seed(0))
+    y = torch.empty_like(x)
+    for trans in (0, 1):
+        rc = tosp._lib.tosp_apply_filter(s.h, x.data_ptr(), y.data_ptr(), nd, trans)
+        if rc != 0:
+            raise tosp.TospError(rc, tosp._lib.tosp_last_error(s.h).decode())
+    torch.cuda.synchronize()
+    s.close()
+    print("profile-filter done")
+    return 0
+
+
 def profile_kernels(args):
     import torch
     import tosp
@@ -424,6 +446,9 @@ def main():
     ap.add_argument("--budget-gb", type=float, default=64.0)
     ap.add_argument("--profile-solve", action="store_true",
                     help="with --profile-kernels: also one full mixed-precision solve (launch lists)")
+    ap.add_argument("--profile-filter", action="store_true",
+                    help="one handle on the workload's density mesh: the filter weights, then one forward and one "
+                         "transposed ApplyFilter on device vectors (a short run for ncu captures of the filter)")
     ap.add_argument("--profile-kernels", action="store_true",
                     help="one mixed-precision handle: setup, one FP64 product and one V-cycle, then exit "
                          "(a short run for ncu captures of the operator kernels)")
@@ -433,6 +458,8 @@ def main():
         return run_reference(args, world, rank)
     if args.profile_kernels:
         return profile_kernels(args)
+    if args.profile_filter:
+        return profile_filter(args)
     if args.serving:
         return run_serving(args)
     if args.slp:
