@@ -963,10 +963,17 @@ void capture_iteration(tosp_handle *h) {
 
 int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
     const int64_t nd = h->lev[0].g.ndof;
-    // r = f - K x
-    TRY(fine_apply64(h, h->cx, h->cq));
-    launch_residual<double>(h->cf, h->cq, h->cr, nd, h->stream);
+    // r = f - K x; from a zero start (K 0 = 0 exactly) r = f without the product
+    launch_dot(h->cx, h->cx, nd, h->d_partials, h->d_scal + 3, h->stream);
     CKL();
+    TRY(read_scalars(h));
+    if (h->h_scal[3] == 0.0) {
+        CK(cudaMemcpyAsync(h->cr, h->cf, sizeof(double) * nd, cudaMemcpyDeviceToDevice, h->stream));
+    } else {
+        TRY(fine_apply64(h, h->cx, h->cq));
+        launch_residual<double>(h->cf, h->cq, h->cr, nd, h->stream);
+        CKL();
+    }
     launch_dot(h->cf, h->cf, nd, h->d_partials, h->d_scal + 4, h->stream);
     launch_dot(h->cr, h->cr, nd, h->d_partials, h->d_scal + 3, h->stream);
     CKL();
