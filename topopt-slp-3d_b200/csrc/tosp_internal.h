@@ -121,7 +121,8 @@ void fine_mr2_const_table(const std::vector<double> &kt_padded, int elem_bytes, 
 void launch_fine_apply64_const(const double *x, double *y, const double *w, const uint8_t *freemask,
                                const double *ktab, const FineGeom &fg, cudaStream_t st);
 // Tensor-core finest operator of the mixed V-cycle (MR factor 2): B operand
-// image (BF16 pieces of the blocks, canonical shared-memory layout) and launch.
+// image (FP16 pieces of the scaled blocks, canonical shared-memory layout,
+// then the block scale) and launch.
 void fine_tc_image(const std::vector<double> &packed_rowmajor, std::vector<uint16_t> &img);
 size_t fine_tc_image_bytes();
 void launch_fine_apply_tc(const float *x, float *y, const __nv_bfloat16 *w, const uint8_t *fm, const void *bimg,
