@@ -129,33 +129,54 @@ void launch_dot2(const double *a, const double *b, const double *c, int64_t n, d
 }
 
 // Scalar slots (see solver.cpp): 0 rho, 1 gamma2 (previous rho), 2 d'q, 3 r'r,
-// 5 r's_old.  mode 1: first iteration (d = s); 0: beta = rho/gamma2
-// (I/SolveMG.m:43-46); 2: flexible beta = (rho - r's_old)/gamma2.  When sold
-// is given it receives s (the next iteration's s_old).
-__global__ void k_pcg_direction(double *d, const double *s, double *sold, const double *scal, int64_t n, int mode) {
+// 5 r's_old, 6 the previous iteration's alpha.  mode 1: first iteration
+// (d = s); 0: beta = rho/gamma2 (I/SolveMG.m:43-46); 2: flexible beta =
+// (rho - r's_old)/gamma2.  When sold is given it receives s (the next
+// iteration's s_old).  The iterate update of the previous iteration,
+// x += alpha d (I/SolveMG.m:40), is done here, while d is read anyway, before
+// d is replaced (modes 0 and 2); launch_pcg_finish applies the last one.
+__global__ void k_pcg_direction(double *d, const double *s, double *sold, const double *scal, int64_t n, int mode,
+                                double *x) {
     const double beta = mode == 1 ? 0.0 : (mode == 2 ? (scal[0] - scal[5]) / scal[1] : scal[0] / scal[1]);
+    const double alpha = scal[6];
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const double si = s[i];
-        d[i] = mode == 1 ? si : beta * d[i] + si;
+        if (mode == 1) {
+            d[i] = si;
+        } else {
+            const double di = d[i];
+            x[i] += alpha * di;
+            d[i] = beta * di + si;
+        }
         if (sold) sold[i] = si;
     }
 }
 void launch_pcg_direction(double *d, const double *s, double *sold, const double *scal, int64_t n, int mode,
-                          cudaStream_t st) {
-    k_pcg_direction<<<gridv(n), 256, 0, st>>>(d, s, sold, scal, n, mode); count_launch();
+                          double *x, cudaStream_t st) {
+    k_pcg_direction<<<gridv(n), 256, 0, st>>>(d, s, sold, scal, n, mode, x); count_launch();
 }
 
-// x += alpha d, r -= alpha q (alpha = rho / d'q), r'r into slot 3 and
-// gamma2 = rho (last block).  For the mixed V-cycle (b0 given) it also writes
-// the next cycle's FP32 right-hand side b0 = r and, when x0 is given, its
-// first Jacobi iterate x0 = invd0 b0 (the sweep from a zero guess).
-__global__ void k_pcg_update(double *x, double *r, const double *d, const double *q, double *scal, int64_t n,
-                             double *partials, float *b0, const float *invd0, float *x0) {
+// x += alpha d with the last iteration's alpha (slot 6).
+__global__ void k_pcg_finish(double *x, const double *d, const double *scal, int64_t n) {
+    const double alpha = scal[6];
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        x[i] += alpha * d[i];
+}
+void launch_pcg_finish(double *x, const double *d, const double *scal, int64_t n, cudaStream_t st) {
+    k_pcg_finish<<<gridv(n), 256, 0, st>>>(x, d, scal, n); count_launch();
+}
+
+// r -= alpha q (alpha = rho / d'q, kept in slot 6 for the iterate update),
+// r'r into slot 3 and gamma2 = rho (last block).  For the mixed V-cycle (b0
+// given) it also writes the next cycle's FP32 right-hand side b0 = r and, when
+// x0 is given, its first Jacobi iterate x0 = invd0 b0 (the sweep from a zero
+// guess).
+__global__ void k_pcg_update(double *r, const double *q, double *scal, int64_t n, double *partials, float *b0,
+                             const float *invd0, float *x0) {
     __shared__ double sh[32];
     const double alpha = scal[0] / scal[2];
     double s = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        x[i] += alpha * d[i];
         const double ri = r[i] - alpha * q[i];
         r[i] = ri;
         s += ri * ri;
@@ -172,13 +193,14 @@ __global__ void k_pcg_update(double *x, double *r, const double *d, const double
         if (threadIdx.x == 0) {
             scal[3] = t;
             scal[1] = scal[0];
+            scal[6] = alpha;
         }
     }
 }
 
-void launch_pcg_update(double *x, double *r, const double *d, const double *q, double *scal, double *partials,
-                       int64_t n, cudaStream_t st, float *b0, const float *invd0, float *x0) {
-    k_pcg_update<<<RED_BLOCKS, 256, 0, st>>>(x, r, d, q, scal, n, partials, b0, invd0, x0); count_launch();
+void launch_pcg_update(double *r, const double *q, double *scal, double *partials, int64_t n, cudaStream_t st,
+                       float *b0, const float *invd0, float *x0) {
+    k_pcg_update<<<RED_BLOCKS, 256, 0, st>>>(r, q, scal, n, partials, b0, invd0, x0); count_launch();
 }
 
 __global__ void k_set_scalar(double *dst, const double *src) { *dst = *src; }

@@ -927,14 +927,13 @@ int cg_iteration(tosp_handle *h, int mode) {
     TRY(precondition(h, h->cr, h->cs, mixed && mode != 1));
     if (mode == 2) launch_dot2(h->cr, h->cs, h->cso, nd, h->d_partials, h->d_scal + 0, h->d_scal + 5, h->stream);
     else launch_dot(h->cr, h->cs, nd, h->d_partials, h->d_scal + 0, h->stream);
-    launch_pcg_direction(h->cd, h->cs, h->mg.flexible ? h->cso : nullptr, h->d_scal, nd, mode, h->stream);
+    launch_pcg_direction(h->cd, h->cs, h->mg.flexible ? h->cso : nullptr, h->d_scal, nd, mode, h->cx, h->stream);
     CKL();
     TRY(fine_apply64(h, h->cd, h->cq));
     launch_dot(h->cd, h->cq, nd, h->d_partials, h->d_scal + 2, h->stream);
     const bool first = mixed && fused_first_sweep(h);
-    launch_pcg_update(h->cx, h->cr, h->cd, h->cq, h->d_scal, h->d_partials, nd, h->stream,
-                      mixed ? (float *)F.b : nullptr, first ? (const float *)F.invd : nullptr,
-                      first ? (float *)F.x : nullptr);
+    launch_pcg_update(h->cr, h->cq, h->d_scal, h->d_partials, nd, h->stream, mixed ? (float *)F.b : nullptr,
+                      first ? (const float *)F.invd : nullptr, first ? (float *)F.x : nullptr);
     CKL();
     CK(cudaMemcpyAsync(h->h_scal, h->d_scal, sizeof(double) * 8, cudaMemcpyDeviceToHost, h->stream));
     return TOSP_OK;
@@ -1018,6 +1017,11 @@ int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
             rc = TOSP_NOT_CONVERGED;
             break;
         }
+    }
+    // the last iteration's x += alpha d (the others ride on the direction update)
+    if (it > 1) {
+        launch_pcg_finish(h->cx, h->cd, h->d_scal, nd, h->stream);
+        CKL();
     }
     if (rc == TOSP_OK && nr > h->mg.tolMG && it > h->mg.maxiterMG) rc = TOSP_NOT_CONVERGED;
     if (it_out) *it_out = it;

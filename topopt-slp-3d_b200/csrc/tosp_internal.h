@@ -240,10 +240,10 @@ void launch_dot2(const double *a, const double *b, const double *c, int64_t n, d
                  double *out1, cudaStream_t st);
 // PCG pieces (scalars in device memory, see solver.cpp for the slots).
 void launch_pcg_direction(double *d, const double *s, double *sold, const double *scal, int64_t n, int mode,
-                          cudaStream_t st);
-void launch_pcg_update(double *x, double *r, const double *d, const double *q, double *scal, double *partials,
-                       int64_t n, cudaStream_t st, float *b0 = nullptr, const float *invd0 = nullptr,
-                       float *x0 = nullptr);
+                          double *x, cudaStream_t st);
+void launch_pcg_finish(double *x, const double *d, const double *scal, int64_t n, cudaStream_t st);
+void launch_pcg_update(double *r, const double *q, double *scal, double *partials, int64_t n, cudaStream_t st,
+                       float *b0 = nullptr, const float *invd0 = nullptr, float *x0 = nullptr);
 void launch_set_scalar(double *dst, const double *src, cudaStream_t st);
 
 // Handle internals used by entry points that live outside solver.cpp.
