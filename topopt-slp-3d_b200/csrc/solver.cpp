@@ -85,7 +85,9 @@ struct tosp_handle {
     GridBarrier *d_bar = nullptr;
     unsigned char *d_steps = nullptr;
     int small_n[3] = {0, 0, 0};
-    cudaGraphExec_t iter_graph = nullptr;   // one CG iteration (it >= 2), captured once per handle
+    // one CG iteration (it >= 2) per parity of the iteration number (the
+    // preconditioned residual alternates between cs and cso), captured once
+    cudaGraphExec_t iter_graph[2] = {nullptr, nullptr};
     bool graph_failed = false;
     // CG (FP64, full-length vectors with zeros on fixed dofs)
     double *cx = nullptr, *cr = nullptr, *cd = nullptr, *cq = nullptr, *cs = nullptr, *cf = nullptr, *cso = nullptr;
@@ -918,16 +920,21 @@ int read_scalars(tosp_handle *h) {
 // One iteration of I/SolveMG.m:31-52 from the current r, ending with an
 // asynchronous copy of the scalars to pinned host memory.  mode: 1 first
 // iteration, 0 reference beta, 2 flexible beta.
-int cg_iteration(tosp_handle *h, int mode) {
+int cg_iteration(tosp_handle *h, int mode, int k) {
     Level &F = h->lev[0];
     const int64_t nd = F.g.ndof;
     const bool mixed = h->precision == TOSP_PREC_MIXED;
+    // flexible beta: s of iteration k alternates between cso (k odd) and cs
+    // (k even), so the previous s is in the other buffer without a copy
+    const bool alt = h->mg.flexible && (k & 1);
+    double *s = alt ? h->cso : h->cs;
+    double *s_old = alt ? h->cs : h->cso;
     // iterations after the first find the V-cycle's input prepared by the
     // previous update (mixed precision)
-    TRY(precondition(h, h->cr, h->cs, mixed && mode != 1));
-    if (mode == 2) launch_dot2(h->cr, h->cs, h->cso, nd, h->d_partials, h->d_scal + 0, h->d_scal + 5, h->stream);
-    else launch_dot(h->cr, h->cs, nd, h->d_partials, h->d_scal + 0, h->stream);
-    launch_pcg_direction(h->cd, h->cs, h->mg.flexible ? h->cso : nullptr, h->d_scal, nd, mode, h->cx, h->stream);
+    TRY(precondition(h, h->cr, s, mixed && mode != 1));
+    if (mode == 2) launch_dot2(h->cr, s, s_old, nd, h->d_partials, h->d_scal + 0, h->d_scal + 5, h->stream);
+    else launch_dot(h->cr, s, nd, h->d_partials, h->d_scal + 0, h->stream);
+    launch_pcg_direction(h->cd, s, nullptr, h->d_scal, nd, mode, h->cx, h->stream);
     CKL();
     TRY(fine_apply64(h, h->cd, h->cq));
     launch_dot(h->cd, h->cq, nd, h->d_partials, h->d_scal + 2, h->stream);
@@ -939,22 +946,22 @@ int cg_iteration(tosp_handle *h, int mode) {
     return TOSP_OK;
 }
 
-// Capture the generic iteration (it >= 2) into a CUDA graph: all buffers
-// are fixed per handle, so the graph is reused by every later solve.  On any
-// capture failure the solver keeps launching the same kernels one by one.
-void capture_iteration(tosp_handle *h) {
+// Capture the generic iteration (it >= 2) of one parity into a CUDA graph: all
+// buffers are fixed per handle, so the graph is reused by every later solve.
+// On any capture failure the solver keeps launching the same kernels one by one.
+void capture_iteration(tosp_handle *h, int parity) {
     cudaGraph_t g = nullptr;
     if (cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         cudaGetLastError();
         h->graph_failed = true;
         return;
     }
-    const int rc = cg_iteration(h, h->mg.flexible ? 2 : 0);
+    const int rc = cg_iteration(h, h->mg.flexible ? 2 : 0, parity);
     const cudaError_t e = cudaStreamEndCapture(h->stream, &g);
     if (rc != TOSP_OK || e != cudaSuccess || !g ||
-        cudaGraphInstantiate(&h->iter_graph, g, 0) != cudaSuccess) {
+        cudaGraphInstantiate(&h->iter_graph[parity], g, 0) != cudaSuccess) {
         cudaGetLastError();
-        h->iter_graph = nullptr;
+        h->iter_graph[parity] = nullptr;
         h->graph_failed = true;
     }
     if (g) cudaGraphDestroy(g);
@@ -985,13 +992,14 @@ int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
     int best_it = 1;
     while (nr > h->mg.tolMG && it <= h->mg.maxiterMG) {
         if (it == 1) {
-            TRY(cg_iteration(h, 1));
+            TRY(cg_iteration(h, 1, it));
         } else {
-            if (!h->iter_graph && !h->graph_failed) capture_iteration(h);
-            if (h->iter_graph) {
-                CK(cudaGraphLaunch(h->iter_graph, h->stream));
+            const int par = it & 1;
+            if (!h->iter_graph[par] && !h->graph_failed) capture_iteration(h, par);
+            if (h->iter_graph[par]) {
+                CK(cudaGraphLaunch(h->iter_graph[par], h->stream));
             } else {
-                TRY(cg_iteration(h, h->mg.flexible ? 2 : 0));
+                TRY(cg_iteration(h, h->mg.flexible ? 2 : 0, it));
             }
         }
         TRY(sync(h));
@@ -1105,7 +1113,8 @@ int tosp_create(const tosp_problem *prob, const tosp_mg_params *mg, int32_t prec
 int tosp_destroy(tosp_handle *h) {
     if (!h) return TOSP_OK;
     if (h->stream) cudaStreamSynchronize(h->stream);
-    if (h->iter_graph) cudaGraphExecDestroy(h->iter_graph);
+    for (cudaGraphExec_t gx : h->iter_graph)
+        if (gx) cudaGraphExecDestroy(gx);
     for (void *p : h->allocs) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
     if (h->ev0) cudaEventDestroy(h->ev0);
