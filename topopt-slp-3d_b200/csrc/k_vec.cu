@@ -128,6 +128,52 @@ void launch_dot2(const double *a, const double *b, const double *c, int64_t n, d
     k_dot2_partial<<<RED_BLOCKS, 256, 0, st>>>(a, b, c, n, partials, out0, out1); count_launch();
 }
 
+// The finest post-sweep of the preconditioner written as the FP64 CG vector,
+// s = x + invd (b - t) (k_jacobi_out), with the CG's dots of the new s in the
+// same pass: r's -> out0 and, when so is given, r's_old -> out1.  Same grid,
+// loop order and reduction tree as k_dot2_partial / k_dot_partial, so the
+// dots are bitwise those of the separate kernels.
+template <typename T>
+__global__ void k_jacobi_out_dot(double *out, const T *x, const T *b, const T *t, const T *invd, int64_t n,
+                                 const double *r, const double *so, double *partials, double *out0, double *out1) {
+    __shared__ double sh[32];
+    double s0 = 0.0, s1 = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double si = (double)(x[i] + invd[i] * (b[i] - t[i]));
+        out[i] = si;
+        const double ri = r[i];
+        s0 += ri * si;
+        if (so) s1 += ri * so[i];
+    }
+    s0 = block_sum(s0, sh);
+    if (so) s1 = block_sum(s1, sh);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = s0;
+        partials[RED_BLOCKS + blockIdx.x] = s1;
+    }
+    if (last_block(red_counter(partials))) {
+        const double t0 = sum_partials(partials, gridDim.x, sh);
+        const double t1 = so ? sum_partials(partials + RED_BLOCKS, gridDim.x, sh) : 0.0;
+        if (threadIdx.x == 0) {
+            out0[0] = t0;
+            if (so) out1[0] = t1;
+        }
+    }
+}
+
+template <typename T>
+void launch_jacobi_out_dot(double *out, const T *x, const T *b, const T *t, const T *invd, int64_t n, const double *r,
+                           const double *so, double *partials, double *out0, double *out1, cudaStream_t st) {
+    k_jacobi_out_dot<T><<<RED_BLOCKS, 256, 0, st>>>(out, x, b, t, invd, n, r, so, partials, out0, out1);
+    count_launch();
+}
+template void launch_jacobi_out_dot<float>(double *, const float *, const float *, const float *, const float *,
+                                           int64_t, const double *, const double *, double *, double *, double *,
+                                           cudaStream_t);
+template void launch_jacobi_out_dot<double>(double *, const double *, const double *, const double *, const double *,
+                                            int64_t, const double *, const double *, double *, double *, double *,
+                                            cudaStream_t);
+
 // Scalar slots (see solver.cpp): 0 rho, 1 gamma2 (previous rho), 2 d'q, 3 r'r,
 // 5 r's_old, 6 the previous iteration's alpha.  mode 1: first iteration
 // (d = s); 0: beta = rho/gamma2 (I/SolveMG.m:43-46); 2: flexible beta =

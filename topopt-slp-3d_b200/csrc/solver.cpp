@@ -79,6 +79,12 @@ struct tosp_handle {
     bool setup_done = false;
     // persistent small-level cycle: first level it covers (-1: off), its grid
     // and three step lists (entered with the first sweep done, from zero, warm)
+    // dots the CG wants from the preconditioner's last sweep (cg_iteration)
+    struct {
+        const double *r = nullptr, *so = nullptr;
+        double *o0 = nullptr, *o1 = nullptr;
+        bool want = false, done = false;
+    } fdot;
     int small_l = -1;
     bool small_built = false;
     int small_blocks = 0;
@@ -240,7 +246,11 @@ int smooth(tosp_handle *h, int l, int niter, bool x_zero, bool first_done = fals
             if (!first_done) launch_jacobi_update<T>((T *)L.x, b, nullptr, (const T *)L.invd, nd, 1, h->stream);
         } else if (l == 0) {
             TRY(fine_apply<T>(h, (const T *)L.x, (T *)L.t));
-            if (out && it == niter - 1)
+            if (out && it == niter - 1 && h->fdot.want) {
+                launch_jacobi_out_dot<T>(out, (const T *)L.x, b, (const T *)L.t, (const T *)L.invd, nd, h->fdot.r,
+                                         h->fdot.so, h->d_partials, h->fdot.o0, h->fdot.o1, h->stream);
+                h->fdot.done = true;
+            } else if (out && it == niter - 1)
                 launch_jacobi_out<T>(out, (const T *)L.x, b, (const T *)L.t, (const T *)L.invd, nd, h->stream);
             else
                 launch_jacobi_update<T>((T *)L.x, b, (const T *)L.t, (const T *)L.invd, nd, 0, h->stream);
@@ -931,9 +941,21 @@ int cg_iteration(tosp_handle *h, int mode, int k) {
     double *s_old = alt ? h->cs : h->cso;
     // iterations after the first find the V-cycle's input prepared by the
     // previous update (mixed precision)
-    TRY(precondition(h, h->cr, s, mixed && mode != 1));
-    if (mode == 2) launch_dot2(h->cr, s, s_old, nd, h->d_partials, h->d_scal + 0, h->d_scal + 5, h->stream);
-    else launch_dot(h->cr, s, nd, h->d_partials, h->d_scal + 0, h->stream);
+    // the dots of the new s ride on the preconditioner's last sweep when it
+    // writes s (post-smoothing), else they take their own pass
+    h->fdot.r = h->cr;
+    h->fdot.so = mode == 2 ? s_old : nullptr;
+    h->fdot.o0 = h->d_scal + 0;
+    h->fdot.o1 = h->d_scal + 5;
+    h->fdot.want = true;
+    h->fdot.done = false;
+    const int prc = precondition(h, h->cr, s, mixed && mode != 1);
+    h->fdot.want = false;
+    TRY(prc);
+    if (!h->fdot.done) {
+        if (mode == 2) launch_dot2(h->cr, s, s_old, nd, h->d_partials, h->d_scal + 0, h->d_scal + 5, h->stream);
+        else launch_dot(h->cr, s, nd, h->d_partials, h->d_scal + 0, h->stream);
+    }
     launch_pcg_direction(h->cd, s, nullptr, h->d_scal, nd, mode, h->cx, h->stream);
     CKL();
     TRY(fine_apply64(h, h->cd, h->cq));

@@ -242,6 +242,11 @@ void launch_dot2(const double *a, const double *b, const double *c, int64_t n, d
 void launch_pcg_direction(double *d, const double *s, double *sold, const double *scal, int64_t n, int mode,
                           double *x, cudaStream_t st);
 void launch_pcg_finish(double *x, const double *d, const double *scal, int64_t n, cudaStream_t st);
+// launch_jacobi_out with the CG's dots r's (-> out0) and r's_old (-> out1,
+// when so is given) of the new s in the same pass.
+template <typename T>
+void launch_jacobi_out_dot(double *out, const T *x, const T *b, const T *t, const T *invd, int64_t n, const double *r,
+                           const double *so, double *partials, double *out0, double *out1, cudaStream_t st);
 void launch_pcg_update(double *r, const double *q, double *scal, double *partials, int64_t n, cudaStream_t st,
                        float *b0 = nullptr, const float *invd0 = nullptr, float *x0 = nullptr);
 void launch_set_scalar(double *dst, const double *src, cudaStream_t st);
