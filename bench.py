@@ -97,85 +97,114 @@ def dist_setup():
     return world, rank, local
 
 
+def host_cores():
+    """Host threads this process may use (the CPU arms use all of them)."""
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def bench_config(args, spec, pb, n, ngrids, world):
+    """The workload keys shared by the GPU line and the reference line."""
+    return {"workload": args.workload, "mesh": list(spec["dims"]), "mr_n": n, "ndof": 3 * pb.nnodes,
+            "nfree": int(pb.freedofs.size), "density_elements": int(pb.nelem * n ** 3), "ngrids": ngrids,
+            "cycle": "V", "omega": spec["omega"], "smooth": "1+1 Jacobi", "tol": 1e-8,
+            "l2": "inputs larger than L2 (densities 113 MB, vectors 44 MB each)" if n == 2 and pb.nelem > 10 ** 6
+                  else "inputs of this size (between steps the setup rewrites every level)",
+            "parallelism": f"replicas x{world}"}
+
+
+def cpu_solver(args, spec):
+    """The assembled-path oracle port for the workload, and the workload built
+    with its host filter (no GPU involved)."""
+    from oracle.cpu_assembled import CpuAssembled
+    from tosp import problems
+    from tosp.workloads import build_workload
+    n = spec["n"]
+    ngrids = args.ngrids or spec["ngrids"]
+    pb0 = problems.cantilever(*spec["dims"])
+    ca = CpuAssembled(pb0, n, ngrids, spec["omega"], rmin=spec["rmin"], nthreads=host_cores())
+    pb, n, xfil, spec = build_workload(args.workload, filter_fn=ca.filter)
+    return ca, pb, n, xfil, spec, ngrids
+
+
+def _full(pb, u_free):
+    out = np.zeros(3 * pb.nnodes)
+    out[pb.freedofs] = u_free
+    return out
+
+
+def cpu_whole_solve(ca, pb, xfil):
+    """One complete solve on the host: SetupGMG + SolveMG from zero to 1e-8 +
+    Grad.  Returns the seconds of each part and the results."""
+    f = pb.f_full()
+    t0 = time.perf_counter()
+    ca.setup(xfil)
+    t1 = time.perf_counter()
+    u, it, nr = ca.solve(np.zeros(f.size), f, 1e-8, 1000)
+    t2 = time.perf_counter()
+    g, _ = ca.grad(u)
+    t3 = time.perf_counter()
+    return {"setup_s": t1 - t0, "solve_s": t2 - t1, "grad_s": t3 - t2, "total_s": t3 - t0, "it": it, "relres": nr,
+            "u": u, "g": g}
+
+
 def run_reference(args, world, rank):
-    """Reference algorithm on the host cores (oracle C/OpenMP port)."""
+    """The reference's default assembled path (genK = true: GlobalStiffMatrix,
+    SetupGMG, SolveMG, Grad) restated in C/OpenMP under oracle/, on all host
+    threads.  The K timed steps together run ONE complete solve (setup, PCG
+    to 1e-8, Grad), split by PCG iteration, so the value is a measured
+    whole-solve rate; the W warm-up steps run a setup and W iterations."""
     if rank != 0:
         return 0
-    from oracle.cpu_wok import CpuWok
-    from tosp.workloads import WORKLOADS, build_workload
+    from tosp.workloads import WORKLOADS
     spec = WORKLOADS[args.workload]
-    pb, n, xfil, spec = build_workload(args.workload, filter_fn=_cpu_filter(args.workload))
-    cores = os.cpu_count()
-    cw = CpuWok(pb, n, spec["ngrids"], spec["omega"], nthreads=cores)
+    ca, pb, n, xfil, spec, ngrids = cpu_solver(args, spec)
+    cores = host_cores()
     f = pb.f_full()
-    its = spec.get("pcg_iterations_fp64")
-    samples = []
-
-    def one_step():
-        t0 = time.perf_counter()
-        cw.setup(xfil)
-        t1 = time.perf_counter()
-        u, it, per_it = cw.solve(np.zeros(f.size), f, 1e-8, 1000, max_iterations=1)
-        t2 = time.perf_counter()
-        cw.grad0(u)
-        t3 = time.perf_counter()
-        return (t1 - t0) + (its or 1) * float(np.mean(per_it)) + (t3 - t2), per_it
-
+    # warm-up (untimed): a setup, then one PCG iteration per warm-up step
+    ca.setup(xfil)
+    gen = ca.solve_iter(np.zeros(f.size), f, 1e-8, 1000)
     for _ in range(args.warmup):
-        one_step()
-    for _ in range(args.steps):
-        t, _ = one_step()
-        samples.append(t)
-    t_mean = float(np.mean(samples))
-    value = 1.0 / t_mean
-    sample = (f"per step: SetupGMG (Galerkin hierarchy + coarsest Cholesky) + 1 of {its} PCG iterations "
-              f"of the full {args.workload} solve + Grad, timed; solve time projected as setup + {its} x "
-              f"iteration + Grad")
+        next(gen, None)
+    its_planned = spec.get("pcg_iterations_fp64") or 100
+    per, parts = [], {"setup_s": 0.0, "solve_s": 0.0, "grad_s": 0.0}
+    gen, done = None, False
+    for k in range(args.steps):
+        t0 = time.perf_counter()
+        if k == 0:
+            ca.setup(xfil)
+            gen = ca.solve_iter(np.zeros(f.size), f, 1e-8, 1000)
+            parts["setup_s"] = time.perf_counter() - t0
+        ts = time.perf_counter()
+        last = k == args.steps - 1
+        target = its_planned * (k + 1) / args.steps
+        while not done and (last or ca.it - 1 < target):
+            done = next(gen, None) is None
+        parts["solve_s"] += time.perf_counter() - ts
+        if last:
+            tg = time.perf_counter()
+            ca.grad(ca.x)
+            parts["grad_s"] = time.perf_counter() - tg
+        per.append(time.perf_counter() - t0)
+    total = float(sum(per))
+    value = 1.0 / total
+    sample = (f"one complete {args.workload} solve (SetupGMG + SolveMG from zero to 1e-8 in {ca.it - 1} PCG "
+              f"iterations + Grad with the transposed filter) of the assembled path restated in C/OpenMP, "
+              f"{total:.1f} s on {cores} host threads, split over the {args.steps} timed steps by PCG iteration")
     line = {"impl": "reference", "metric": METRIC, "value": round(value, 6), "unit": "solves/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * t_mean, 3),
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1000 * total / args.steps, 3),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": args.workload},
+            "data": "synthetic", "config": bench_config(args, spec, pb, n, ngrids, world),
+            "cg": "reference beta (I/SolveMG.m:43-46)",
+            "solve": {"pcg_iterations": int(ca.it), "relres": float(ca.nr),
+                      **{k: round(v, 3) for k, v in parts.items()}},
             "cpu_baseline": {"value": round(value, 6), "unit": "solves/s", "cores": cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": round(value, 6), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
-
-
-def _cpu_filter(workload):
-    """Host filter for building the uniform-filtered workload without a GPU."""
-    from oracle import filt
-    from tosp.workloads import WORKLOADS
-    spec = WORKLOADS[workload]
-    if spec["density"] != "uniform_filtered":
-        return None
-    nelx, nely, nelz = spec["dims"]
-    n = spec["n"]
-
-    def f(x):
-        W, w = filt.elem_neighborhood(nelx * n, nely * n, nelz * n, 1.0 / n, 1.0 / n, 1.0 / n, spec["rmin"], 1)
-        return filt.apply_filter(x, W, w, 1, False)
-    return f
-
-
-def cpu_baseline(args, pb, n, xfil, spec, it_fp64):
-    """Bounded CPU sample of the same workload (oracle port, all host cores)."""
-    from oracle.cpu_wok import CpuWok
-    cores = os.cpu_count()
-    cw = CpuWok(pb, n, spec["ngrids"], spec["omega"], nthreads=cores)
-    f = pb.f_full()
-    t0 = time.perf_counter()
-    cw.setup(xfil)
-    t1 = time.perf_counter()
-    u, it, per_it = cw.solve(np.zeros(f.size), f, 1e-8, 1000, max_iterations=args.cpu_iters)
-    t2 = time.perf_counter()
-    cw.grad0(u)
-    t3 = time.perf_counter()
-    t_solve = (t1 - t0) + it_fp64 * float(np.mean(per_it)) + (t3 - t2)
-    return {"value": round(1.0 / t_solve, 6), "unit": "solves/s", "cores": cores, "kind": "port",
-            "sample": (f"SetupGMG + {len(per_it)} of {it_fp64} PCG iterations (reference WOK algorithm: "
-                       f"AciProd coarse products) + Grad on the full workload, "
-                       f"{t3 - t0:.1f} s timed; full solve projected as setup + {it_fp64} x iteration + Grad")}
 
 
 class _Timed:
@@ -426,8 +455,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="tosp", choices=["tosp", "reference"])
     ap.add_argument("--workload", default="cantilever192x96x96_mr2")
-    ap.add_argument("--fp64-steps", type=int, default=2)
-    ap.add_argument("--cpu-iters", type=int, default=2)
+    ap.add_argument("--fp64-steps", type=int, default=0, help="timed steps of the FP64 arm (0: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-w-cycle", action="store_true", help="skip the secondary W-cycle measurement")
     ap.add_argument("--ngrids", type=int, default=0, help="override the workload's grid count")
@@ -548,8 +576,16 @@ def main():
     per_mx, its_mx, launches = timed(smx, args.steps, args.warmup)
     clk = clocks.stop()
     total_ms = max_over_ranks(sum(per_mx))
-    per_64, its_64, _ = timed(s64, args.fp64_steps, 1)
+    fp64_steps = args.fp64_steps or args.steps
+    per_64, its_64, _ = timed(s64, fp64_steps, args.warmup)
     total64 = max_over_ranks(sum(per_64))
+    # solutions of both arms (outside the timed regions) for the true residuals
+    # and the mixed-vs-FP64 errors
+    sol = {}
+    for key, s in (("mixed", smx), ("fp64", s64)):
+        step_dev(s)
+        g_full = g_d.cpu().numpy().copy()
+        sol[key] = (u_d.cpu().numpy().copy(), g_full)
     stats_mx = smx.stats()
 
     # ---- end to end through the C ABI with pinned host buffers ------------------
@@ -570,7 +606,7 @@ def main():
         lib.tosp_grad(s.h, uf_h.data_ptr(), uf_h.numel(), g_h.data_ptr(), None, g_h.numel())
         return it.value
 
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = max(3, args.steps)
     step_host(smx)
     torch.cuda.synchronize()
     barrier()
@@ -583,6 +619,13 @@ def main():
     d2h = 8 * (pb.freedofs.size + xfil.size)
     # parity guard: the host path gives the same gradient as the device path
     assert torch.allclose(g_h, g_d.cpu(), rtol=1e-6, atol=1e-12 * float(g_h.abs().max()))
+
+    # true relative residuals ||f - K u|| / ||f|| of both arms' solutions, with
+    # one FP64 product each (not the CG's recurrence residual)
+    relres_true = {}
+    nf = float(np.linalg.norm(pb.f))
+    for key, (u_sol, _) in sol.items():
+        relres_true[key] = float(np.linalg.norm(pb.f - s64.KelemProd(u_sol)) / nf)
 
     # ---- kernel roofline (finest-level operators) ---------------------------------
     peaks, peak_kind = load_peaks()
@@ -633,17 +676,15 @@ def main():
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 3), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64 outer CG / f32+bf16 V-cycle",
         "data": "synthetic",
-        "config": {"workload": args.workload, "mesh": list(spec["dims"]), "mr_n": n, "ndof": ndof,
-                   "nfree": int(pb.freedofs.size), "density_elements": int(nsub), "ngrids": ngrids, "cg_beta": "flexible" if args.flexible else "reference",
-                   "cycle": "V", "omega": spec0["omega"], "smooth": "1+1 Jacobi", "tol": 1e-8,
-                   "l2": "inputs larger than L2 (densities 113 MB, vectors 44 MB each)",
-                   "parallelism": f"replicas x{world}"},
+        "config": bench_config(args, spec0, pb, n, ngrids, world),
         "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3), "p99": round(float(np.percentile(lat, 99)), 3)},
         "pcg_iterations": {"mixed": it_mx, "fp64": its_64[-1][0]},
         "relres": {"mixed": its_mx[-1][1], "fp64": its_64[-1][1]},
-        "fp64": {"value": round(world * args.fp64_steps / (total64 * 1e-3), 4), "unit": "solves/s",
-                 "ms_per_step": round(total64 / args.fp64_steps, 3)},
-        "mixed_over_fp64": round((args.steps / total_ms) / (args.fp64_steps / total64), 3),
+        "relres_true": relres_true,
+        "cg": "flexible beta r'(s - s_old)/rho_old in both arms" if args.flexible else "reference beta",
+        "fp64": {"value": round(world * fp64_steps / (total64 * 1e-3), 4), "unit": "solves/s",
+                 "ms_per_step": round(total64 / fp64_steps, 3), "steps": fp64_steps},
+        "mixed_over_fp64": round((args.steps / total_ms) / (fp64_steps / total64), 3),
         "setup_ms": round(stats_mx["ms_setup"], 3),
         "e2e": {"value": round(world * e2e_steps / e2e_s, 4), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                 "d2h_bytes_per_step": int(d2h)},
@@ -660,19 +701,41 @@ def main():
         mgw.cycle = 1
         smw = tosp.Solver(pb, mgw, precision=tosp.PREC_MIXED, **kw)
         s6w = tosp.Solver(pb, mgw, precision=tosp.PREC_FP64, **kw)
-        per_w, its_w, _ = timed(smw, 2, 1)
-        per_w64, its_w64, _ = timed(s6w, 2, 1)
+        per_w, its_w, _ = timed(smw, 3, 3)
+        per_w64, its_w64, _ = timed(s6w, 3, 3)
         tw, tw64 = max_over_ranks(sum(per_w)), max_over_ranks(sum(per_w64))
         line["w_cycle"] = {
-            "mixed": {"value": round(world * 2 / (tw * 1e-3), 4), "ms_per_step": round(tw / 2, 3),
+            "mixed": {"value": round(world * 3 / (tw * 1e-3), 4), "ms_per_step": round(tw / 3, 3),
                       "pcg_iterations": its_w[-1][0], "relres": its_w[-1][1]},
-            "fp64": {"value": round(world * 2 / (tw64 * 1e-3), 4), "ms_per_step": round(tw64 / 2, 3),
+            "fp64": {"value": round(world * 3 / (tw64 * 1e-3), 4), "ms_per_step": round(tw64 / 3, 3),
                      "pcg_iterations": its_w64[-1][0], "relres": its_w64[-1][1]},
             "mixed_over_fp64": round(tw64 / tw, 3), "unit": "solves/s"}
         smw.close()
         s6w.close()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(args, pb, n, xfil, spec, its_64[-1][0])
+        # one complete solve of the same workload on the host cores (the
+        # reference's assembled path restated in C/OpenMP), which is also the
+        # FP64 oracle the GPU arms' errors are stated against
+        ca, _, _, _, _, _ = cpu_solver(args, spec0)
+        cs = cpu_whole_solve(ca, pb, xfil)
+        cores = host_cores()
+        line["cpu_baseline"] = {
+            "value": round(1.0 / cs["total_s"], 6), "unit": "solves/s", "cores": cores, "kind": "port",
+            "sample": (f"one complete solve of the same workload, measured: SetupGMG {cs['setup_s']:.1f} s + "
+                       f"SolveMG {cs['solve_s']:.1f} s ({cs['it'] - 1} PCG iterations to {cs['relres']:.2e}) + Grad "
+                       f"{cs['grad_s']:.1f} s, the reference's assembled path restated in C/OpenMP on {cores} "
+                       f"host threads")}
+        uo, go = cs["u"][pb.freedofs], cs["g"]
+        Fo = float(pb.f @ uo)
+        line["error_vs_fp64_oracle"] = {
+            key: {"u_rel_max": float(np.abs(u_sol - uo).max() / np.abs(uo).max()),
+                  "F_rel": float(abs(pb.f @ u_sol - Fo) / abs(Fo)),
+                  "dFdrho_rel_max": float(np.abs(g_sol - go).max() / np.abs(go).max())}
+            for key, (u_sol, g_sol) in sol.items()}
+        line["error_vs_fp64_oracle"]["oracle"] = "the CPU solve above (assembled K, FP64, reference beta)"
+        line["relres_true_cpu_operator"] = {
+            key: float(np.linalg.norm((pb.f_full() - ca.apply(0, _full(pb, u_sol)))[pb.freedofs]) / nf)
+            for key, (u_sol, _) in sol.items()}
     if rank == 0:
         print(json.dumps(line))
     smx.close()

@@ -14,7 +14,8 @@
  *   - Index arrays crossing the ABI are 1-based int64 (MATLAB convention).
  *   - Vectors are float64.  Every pointer argument may be host memory or CUDA
  *     device memory of the handle's device (detected per call); device
- *     pointers avoid host<->device copies.
+ *     pointers avoid host<->device copies.  Device memory of another GPU is
+ *     refused with TOSP_ERR_BAD_ARG.
  *   - Every call returns a status code (TOSP_OK = 0); tosp_last_error() gives
  *     the message of the last failing call on a handle.
  *   - Calls on one handle are serialised on that handle's CUDA stream and
@@ -198,16 +199,20 @@ int64_t tosp_kernel_launches(void);
  * handles only).  Writes the mean device time per launch in ms. */
 int tosp_time_operator(tosp_handle *h, int32_t precision, int32_t reps, double *ms_per_launch);
 
-/* KelemProd for callers that cannot allocate device memory at call time
- * (stream capture in progress, a host-managed GPU memory pool such as a
- * MATLAB gpuArray session, or multi-stream pipelines where cudaMalloc would
- * synchronise the device).  No counterpart in the reference: it is
- * tosp_kelem_prod restricted to device pointers, with its scratch (two
- * full-length vectors) taken from a fixed 16 MiB array built into the
- * library instead of the handle.  Problems above 1,048,576 dofs (3*nnodes) are
- * rejected with TOSP_ERR_BAD_ARG.  The first call on a device resolves the
- * array's address and should come before any stream capture.  All calls share
- * the array: calls whose GPU work overlaps race. */
+/* KelemProd for callers that cannot allocate device memory at call time: a
+ * host whose GPU memory belongs to its own pooling allocator (a MATLAB
+ * gpuArray session), pipelines with work in flight on several streams, which
+ * a cudaMalloc/cudaFree may synchronise, and services that fix their device
+ * footprint at start-up.  No counterpart in the reference: it is
+ * tosp_kelem_prod restricted to device pointers of the handle's GPU, with its
+ * scratch (two full-length vectors) taken from a fixed 16 MiB array built
+ * into the library instead of the handle.  The call runs at once on the
+ * handle's stream and returns after y is written, so x must be complete
+ * before the call.  Problems above 1,048,576 dofs (3*nnodes) are rejected
+ * with TOSP_ERR_BAD_ARG; device ordinals from 64 up with
+ * TOSP_ERR_UNSUPPORTED.  The first call on a device resolves the array's
+ * address and should come before any stream capture.  All calls share the
+ * array: calls whose GPU work overlaps race. */
 int tosp_kelem_prod_noalloc(tosp_handle *h, const double *x, double *y, int64_t nfree);
 
 /* ---- serving loop ------------------------------------------------------

@@ -55,3 +55,33 @@ def test_python_binding_names_mirror_reference():
     for name in ("SetupGMG", "SolveMG", "KelemProd", "Grad", "ApplyFilter", "MGCycle"):
         assert hasattr(tosp.Solver, name)
     assert callable(tosp.ElemStiffMatrixGQMR)
+
+
+def test_pointer_rule_refuses_other_gpus_memory(tmp_path):
+    """Where a pointer argument lives, from faked cudaPointerGetAttributes
+    results (csrc/ptr_kind.h compiled with g++; no GPU needed): device memory
+    of the handle's GPU is used in place, another GPU's device memory is
+    refused (the kernels would fault on it), host and managed memory work."""
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    src = tmp_path / "ptr_rule.cpp"
+    src.write_text(
+        '#include <cstdio>\n#include "ptr_kind.h"\n'
+        "using namespace tosp;\n"
+        "int main() {\n"
+        "  int bad = 0;\n"
+        "  bad += classify_ptr(true, MEMTYPE_DEVICE, 0, 0) != PTR_DEVICE;\n"
+        "  bad += classify_ptr(true, MEMTYPE_DEVICE, 1, 0) != PTR_OTHER_DEVICE;\n"
+        "  bad += classify_ptr(true, MEMTYPE_DEVICE, 0, 3) != PTR_OTHER_DEVICE;\n"
+        "  bad += classify_ptr(true, MEMTYPE_MANAGED, 2, 0) != PTR_DEVICE;\n"
+        "  bad += classify_ptr(true, MEMTYPE_HOST, 0, 0) != PTR_HOST;\n"
+        "  bad += classify_ptr(true, MEMTYPE_UNREGISTERED, -2, 0) != PTR_HOST;\n"
+        "  bad += classify_ptr(false, 0, 0, 0) != PTR_HOST;\n"
+        '  std::printf("%d\\n", bad);\n  return bad;\n}\n')
+    exe = tmp_path / "ptr_rule"
+    inc = os.path.join(ROOT, "topopt-slp-3d_b200", "csrc")
+    subprocess.run(["g++", "-std=c++17", "-I" + inc, str(src), "-o", str(exe)], check=True)
+    r = subprocess.run([str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.strip() == "0", r.stdout

@@ -1,7 +1,7 @@
 """Build recipe for the tosp CUDA library (sm_100a) and the C oracle.
 
     python topopt-slp-3d_b200/build.py            # library only
-    python topopt-slp-3d_b200/build.py --oracle   # plus oracle/libkelem_omp.so
+    python topopt-slp-3d_b200/build.py --oracle   # plus the C oracle libraries in oracle/
 
 The library is compiled in-tree to ``topopt-slp-3d_b200/tosp/libtosp.so`` with
 ``nvcc -gencode arch=compute_100a,code=sm_100a -lineinfo``.  Objects are
@@ -63,17 +63,21 @@ def build_library(verbose_ptxas=False):
 
 
 def build_oracle():
-    src = os.path.join(ROOT, "oracle", "kelem_omp.c")
-    out = os.path.join(ROOT, "oracle", "libkelem_omp.so")
-    if not os.path.exists(src):
-        return None
-    if os.path.exists(out) and os.path.getmtime(out) >= os.path.getmtime(src):
-        return out
-    cmd = ["gcc", "-O3", "-march=x86-64-v3", "-fopenmp", "-shared", "-fPIC", src, "-o", out, "-lm"]
-    r = subprocess.run(cmd, capture_output=True, text=True)
-    if r.returncode != 0:
-        raise RuntimeError("gcc failed for the oracle:\n%s" % r.stderr)
-    return out
+    """The C restatements under oracle/ (test infrastructure, CPU baseline)."""
+    outs = []
+    for name in ("kelem_omp", "assembled_omp"):
+        src = os.path.join(ROOT, "oracle", name + ".c")
+        out = os.path.join(ROOT, "oracle", "lib%s.so" % name)
+        if not os.path.exists(src):
+            continue
+        outs.append(out)
+        if os.path.exists(out) and os.path.getmtime(out) >= os.path.getmtime(src):
+            continue
+        cmd = ["gcc", "-O3", "-march=x86-64-v3", "-fopenmp", "-shared", "-fPIC", src, "-o", out, "-lm"]
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode != 0:
+            raise RuntimeError("gcc failed for the oracle:\n%s" % r.stderr)
+    return outs
 
 
 if __name__ == "__main__":

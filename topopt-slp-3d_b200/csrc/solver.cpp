@@ -9,6 +9,7 @@
 #include <string>
 #include <vector>
 
+#include "ptr_kind.h"
 #include "tosp_internal.h"
 
 using namespace tosp;
@@ -152,14 +153,23 @@ int dalloc(tosp_handle *h, T **p, int64_t count) {
     return TOSP_OK;
 }
 
-bool is_device_ptr(const void *p) {
-    if (!p) return false;
+// *on_dev: whether argument `what` is memory the handle's kernels can use
+// directly (else it is host memory and gets staged).  Device memory of
+// another GPU is refused: the kernels would fault on it without peer access.
+int arg_location(tosp_handle *h, const void *p, const char *what, bool *on_dev) {
+    *on_dev = false;
+    if (!p) return TOSP_OK;
     cudaPointerAttributes a;
-    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-        cudaGetLastError();
-        return false;
+    const bool ok = cudaPointerGetAttributes(&a, p) == cudaSuccess;
+    if (!ok) cudaGetLastError();
+    const int k = classify_ptr(ok, ok ? (int)a.type : 0, ok ? a.device : -1, h->device);
+    if (k == PTR_OTHER_DEVICE) {
+        h->err = std::string(what) + " is device memory of GPU " + std::to_string(a.device) +
+                 ", but the handle lives on GPU " + std::to_string(h->device);
+        return TOSP_ERR_BAD_ARG;
     }
-    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+    *on_dev = k == PTR_DEVICE;
+    return TOSP_OK;
 }
 
 // Copy `count` doubles from a host or device pointer into device memory.
@@ -545,9 +555,11 @@ int ensure_stage(tosp_handle *h, int64_t len) {
 }
 
 // Free-dof vector (host or device) -> full-length device vector.
-int free_to_full(tosp_handle *h, const double *v, double *full) {
+int free_to_full(tosp_handle *h, const double *v, double *full, const char *what) {
     const double *src = v;
-    if (!is_device_ptr(v)) {
+    bool dev = false;
+    TRY(arg_location(h, v, what, &dev));
+    if (!dev) {
         TRY(ensure_stage(h, h->nfree));
         TRY(load_vec(h, h->d_stage_a, v, h->nfree));
         src = h->d_stage_a;
@@ -558,8 +570,10 @@ int free_to_full(tosp_handle *h, const double *v, double *full) {
     return TOSP_OK;
 }
 
-int full_to_free(tosp_handle *h, const double *full, double *v) {
-    if (is_device_ptr(v)) {
+int full_to_free(tosp_handle *h, const double *full, double *v, const char *what) {
+    bool dev = false;
+    TRY(arg_location(h, v, what, &dev));
+    if (dev) {
         launch_gather_free(full, h->d_freeidx, h->nfree, v, h->stream);
         CKL();
         return TOSP_OK;
@@ -1068,7 +1082,10 @@ int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
 // scratch (xfull, yfull: ndof doubles each); allocates nothing.
 int tosp::kelem_prod_with_scratch(tosp_handle *h, const double *x, double *y, int64_t nfree, double *xfull,
                                   double *yfull) {
-    if (!is_device_ptr(x) || !is_device_ptr(y)) {
+    bool xd = false, yd = false;
+    TRY(arg_location(h, x, "x", &xd));
+    TRY(arg_location(h, y, "y", &yd));
+    if (!xd || !yd) {
         h->err = "x and y must be device pointers (this entry point stages nothing)";
         return TOSP_ERR_BAD_ARG;
     }
@@ -1189,9 +1206,9 @@ int tosp_kelem_prod(tosp_handle *h, const double *x, double *y, int64_t nfree) {
     cudaSetDevice(h->device);
     TRY(check_len(h, nfree, h->nfree, "x"));
     TRY(need_setup(h));
-    TRY(free_to_full(h, x, h->cd));
+    TRY(free_to_full(h, x, h->cd, "x"));
     TRY(fine_apply64(h, h->cd, h->cq));
-    TRY(full_to_free(h, h->cq, y));
+    TRY(full_to_free(h, h->cq, y, "y"));
     return sync(h);
 }
 
@@ -1206,13 +1223,13 @@ int tosp_kelem_prod_mixed(tosp_handle *h, const double *x, double *y, int64_t nf
     TRY(need_setup(h));
     Level &F = h->lev[0];
     const int64_t nd = F.g.ndof;
-    TRY(free_to_full(h, x, h->cd));
+    TRY(free_to_full(h, x, h->cd, "x"));
     launch_convert<double, float>(h->cd, (float *)F.x, nd, h->stream);
     CKL();
     TRY(fine_apply<float>(h, (const float *)F.x, (float *)F.t));
     launch_convert<float, double>((const float *)F.t, h->cq, nd, h->stream);
     CKL();
-    TRY(full_to_free(h, h->cq, y));
+    TRY(full_to_free(h, h->cq, y, "y"));
     TRY(sync(h));
     return check_tc(h);
 }
@@ -1223,9 +1240,9 @@ int tosp_mg_cycle(tosp_handle *h, const double *r, double *s, int64_t nfree) {
     TRY(check_len(h, nfree, h->nfree, "r"));
     TRY(need_mg(h));
     TRY(need_setup(h));
-    TRY(free_to_full(h, r, h->cr));
+    TRY(free_to_full(h, r, h->cr, "r"));
     TRY(precondition(h, h->cr, h->cs));
-    TRY(full_to_free(h, h->cs, s));
+    TRY(full_to_free(h, h->cs, s, "s"));
     TRY(sync(h));
     return check_tc(h);
 }
@@ -1237,11 +1254,11 @@ int tosp_solve_mg(tosp_handle *h, double *x, const double *f, int64_t nfree, int
     TRY(need_mg(h));
     TRY(need_setup(h));
     CK(cudaEventRecord(h->ev0, h->stream));
-    TRY(free_to_full(h, x, h->cx));
-    TRY(free_to_full(h, f, h->cf));
+    TRY(free_to_full(h, x, h->cx, "x"));
+    TRY(free_to_full(h, f, h->cf, "f"));
     const int rc = solve_impl(h, it, relres);
     if (rc < 0) return rc;
-    TRY(full_to_free(h, h->cx, x));
+    TRY(full_to_free(h, h->cx, x, "x"));
     CK(cudaEventRecord(h->ev1, h->stream));
     TRY(sync(h));
     float ms = 0;
@@ -1254,7 +1271,9 @@ int tosp_apply_filter(tosp_handle *h, const double *x, double *y, int64_t ndens,
     if (!h || !x || !y) return TOSP_ERR_BAD_ARG;
     cudaSetDevice(h->device);
     TRY(check_len(h, ndens, h->dens.nelem, "x"));
-    const bool din = is_device_ptr(x), dout = is_device_ptr(y);
+    bool din = false, dout = false;
+    TRY(arg_location(h, x, "x", &din));
+    TRY(arg_location(h, y, "y", &dout));
     const double *src = x;
     if (!din) {
         TRY(load_vec(h, h->d_g0, x, ndens));
@@ -1291,13 +1310,15 @@ int tosp_grad(tosp_handle *h, const double *u, int64_t nfull, double *fgrad, dou
     TRY(check_len(h, ndens, h->dens.nelem, "fgrad"));
     TRY(need_setup(h));
     const double *du = u;
-    if (!is_device_ptr(u)) {
+    bool udev = false, dout = false;
+    TRY(arg_location(h, u, "u", &udev));
+    TRY(arg_location(h, fgrad, "fgrad", &dout));
+    if (!udev) {
         TRY(load_vec(h, h->d_ufull, u, nfull));
         du = h->d_ufull;
     }
     launch_grad(du, h->d_rho, h->d_free_elem, h->d_ke64, h->d_g0, h->fg, h->n, h->p, h->emin, h->E, h->stream);
     CKL();
-    const bool dout = is_device_ptr(fgrad);
     double *dst = dout ? fgrad : h->d_gf;
     if (h->opfilter == 0 || h->ntaps == 0) {
         CK(cudaMemcpyAsync(dst, h->d_g0, sizeof(double) * ndens, cudaMemcpyDeviceToDevice, h->stream));

@@ -8,8 +8,8 @@ code reads like the reference's ``StrSLP``; the heavy MATLAB arguments
 
 Indices crossing the ABI are 1-based like MATLAB; the Python layer takes the
 0-based arrays of :mod:`tosp.problems` and converts.  The CUDA library must be
-built (``python topopt-slp-3d_b200/build.py``); importing this module without
-it raises ``ImportError`` - there is no CPU fallback.
+built (``python topopt-slp-3d_b200/build.py``); without it the first call
+into the library raises ``ImportError`` - there is no CPU fallback.
 """
 import ctypes as C
 import os
@@ -110,12 +110,28 @@ def _load():
     return lib
 
 
-_lib = _load()
+class _LazyLib:
+    """The ctypes library, mapped on first use: importing ``tosp`` for its
+    problem builders or workloads loads no native code.  The first call raises
+    ImportError when the library is not built (there is no CPU fallback)."""
+
+    _lib = None
+
+    def loaded(self):
+        if _LazyLib._lib is None:
+            _LazyLib._lib = _load()
+        return _LazyLib._lib
+
+    def __getattr__(self, name):
+        return getattr(self.loaded(), name)
+
+
+_lib = _LazyLib()
 
 
 def exported_symbols():
     """Names of the entry points bound from the library."""
-    return [n for n in dir(_lib) if n.startswith("tosp_")]
+    return [n for n in dir(_lib.loaded()) if n.startswith("tosp_")]
 
 
 def kernel_launches():
