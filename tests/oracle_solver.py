@@ -37,3 +37,39 @@ class OracleSolver:
         g, _ = filt.grad(pb.nelx, pb.nely, pb.nelz, self.ks, u_full, self.dens, self.p, self.emin, self.W, self.w,
                          self.opfilter)
         return g
+
+
+class AssembledOracleSolver:
+    """The same interface on the C/OpenMP restatement of the assembled path
+    (oracle/cpu_assembled.py; V-cycle, reference beta), which
+    tests/test_cpu_port.py pins to the NumPy/SciPy oracle.  Fast enough for
+    benchmark-size meshes and whole SLP loops."""
+
+    def __init__(self, pb, n=1, ngrids=3, omega=0.6, tol=1e-8, maxiter=1000, p=3.0, emin=1e-9, opfilter=1,
+                 rmin=1.5, nthreads=0):
+        import os
+        from oracle.cpu_assembled import CpuAssembled
+        self.pb, self.tol, self.maxiter = pb, tol, maxiter
+        self.ca = CpuAssembled(pb, n, ngrids, omega, p=p, emin=emin, rmin=rmin, opfilter=opfilter,
+                               nthreads=nthreads or os.cpu_count())
+
+    def ApplyFilter(self, x, trans=False):
+        return self.ca.filter(x, trans)
+
+    def SetupGMG(self, xfil):
+        self.ca.setup(xfil)
+
+    def _full(self, v):
+        out = np.zeros(3 * self.pb.nnodes)
+        out[self.pb.freedofs] = v
+        return out
+
+    def KelemProd(self, x):
+        return self.ca.apply(0, self._full(x))[self.pb.freedofs]
+
+    def SolveMG(self, x, f):
+        u, it, nr = self.ca.solve(self._full(x), self._full(f), self.tol, self.maxiter)
+        return u[self.pb.freedofs], it, nr, 0
+
+    def Grad(self, u_full):
+        return self.ca.grad(u_full)[0]

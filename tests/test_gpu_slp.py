@@ -44,7 +44,9 @@ def test_slp_mixed_precision_same_designs(tosp_mod):
     t64 = slp.grad_proj(r64.xstar, np.ones(pb.nelem), prj, 0.3 * V, velem)
     tmx = slp.grad_proj(rmx.xstar, np.ones(pb.nelem), prj, 0.3 * V, velem)
     assert np.abs(r64.x - rmx.x).max() <= 1e-5
-    assert np.count_nonzero(t64 != tmx) <= 0.001 * t64.size
+    # GradProj's tie rule (inputs snapped to 2^-30 of their scale) makes the
+    # thresholded designs of the two precisions identical
+    assert np.array_equal(t64, tmx)
 
 
 def test_correct_function_value_matches_oracle(tosp_mod):

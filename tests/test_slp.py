@@ -125,3 +125,25 @@ def test_heaviside_projection_keeps_volume():
     assert abs((c + np.tanh(prj.beta * (0.0 - prj.eta))) * d) <= 1e-15
     assert abs((c + np.tanh(prj.beta * (1.0 - prj.eta))) * d - 1.0) <= 1e-15
     assert prj.beta == 64.0
+
+
+def test_two_oracle_paths_give_identical_thresholded_designs():
+    """The tie rule of GradProj: the same SLP loop on the NumPy/SciPy oracle
+    and on its C/OpenMP restatement (solutions equal to rounding) thresholds
+    to identical 0/1 designs."""
+    import os
+    import sys
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    pytest.importorskip("oracle.cpu_assembled")
+    from oracle_solver import AssembledOracleSolver, OracleSolver
+    from tosp import problems as P
+    pb = P.cantilever(16, 8, 8)
+    x0 = np.full(pb.nelem, 0.3)
+    params = slp.SlpParams(maxiter=6, lp="knapsack")
+    r1 = slp.str_slp(AssembledOracleSolver(pb, ngrids=3, omega=0.6, rmin=1.5, maxiter=5000, nthreads=4), pb, 0.3,
+                     x0, params, prj=slp.PrjParams(op=True))
+    r2 = slp.str_slp(OracleSolver(pb, ngrids=3, cycle=0, omega=0.6, rmin=1.5, maxiter=5000), pb, 0.3, x0, params,
+                     prj=slp.PrjParams(op=True))
+    assert [h["it"] for h in r1.history] == [h["it"] for h in r2.history]
+    assert abs(r1.F - r2.F) <= 1e-10 * abs(r2.F)
+    assert np.array_equal(r1.xstar, r2.xstar) and 0 < r1.xstar.sum() < r1.xstar.size

@@ -216,9 +216,25 @@ def heaviside_proj(x, prj, velem, scur, sdes, betaupd):
     return (c + np.tanh(prj.beta * (x - prj.eta))) * cd, prj
 
 
+def snap(v, scale=1.0):
+    """``v`` rounded to multiples of 2^-30 * scale, scale raised to a power of
+    two: values that agree up to the rounding of two solve paths (a GPU and a
+    CPU one, or two runs with different atomic orders) become exactly equal,
+    and ties then break by element index in the stable sorts."""
+    q = 2.0 ** (np.ceil(np.log2(scale)) - 30) if scale > 0 else 2.0 ** -30
+    return np.round(np.asarray(v, dtype=np.float64) / q) * q
+
+
 def grad_proj(x, g, prj, Vmax, velem):
-    """Rounding of the densities to 0/1 along -grad(Lag) (I/GradProj.m:1-124)."""
-    g = -np.asarray(g, dtype=np.float64)
+    """Rounding of the densities to 0/1 along -grad(Lag) (I/GradProj.m:1-124).
+
+    Tie rule (not in the reference, which runs one solve path): x and g are
+    snapped to 2^-30 of their scale first (:func:`snap`), so designs
+    thresholded from the GPU path and from the CPU oracle are identical
+    whenever the two inputs agree to rounding."""
+    x = snap(x)
+    g = np.asarray(g, dtype=np.float64)
+    g = -snap(g, float(np.abs(g).max()))
     gnorm = np.linalg.norm(g)
     coslim = np.cos(np.deg2rad(prj.maxang))
     gt = prj.gthresh * np.abs(g).max()
