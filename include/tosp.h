@@ -199,6 +199,20 @@ int64_t tosp_kernel_launches(void);
  * handles only).  Writes the mean device time per launch in ms. */
 int tosp_time_operator(tosp_handle *h, int32_t precision, int32_t reps, double *ms_per_launch);
 
+/* Fault injection for tests of the bounded device waits (no counterpart in
+ * the reference).  The next launches of the handle's persistent small-level
+ * cycle (mg.small_cycle_max > 0) give up a grid-barrier wait after `polls`
+ * polls (of 64 ns or more) instead of about 2^21, and when skip_block >= 0
+ * that block skips its first barrier arrival, so the other blocks' waits run
+ * out: the call then returns TOSP_ERR_TIMEOUT, the barrier state is reset and
+ * the handle works normally again (the knob is cleared with it).  Nothing
+ * faults, traps or waits without bound.  TOSP_ERR_STATE when the handle has
+ * no persistent cycle. */
+int tosp_inject_wait_fault(tosp_handle *h, int32_t polls, int32_t skip_block);
+
+/* Blocks of the handle's persistent small-level cycle (0 when it has none). */
+int tosp_small_cycle_blocks(const tosp_handle *h, int32_t *blocks);
+
 /* KelemProd for callers that cannot allocate device memory at call time: a
  * host whose GPU memory belongs to its own pooling allocator (a MATLAB
  * gpuArray session), pipelines with work in flight on several streams, which

@@ -108,3 +108,40 @@ def test_fallback_solver_keeps_converging_mixed_solves(tosp_mod):
     assert rc == 0 and rr <= 1e-8
     assert fs.fallbacks == 0 and fs.fp64 is None
     fs.close()
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+def test_bounded_wait_runs_out_and_the_handle_recovers(tosp_mod, prec):
+    """A bounded device wait that runs out: the persistent small-level cycle's
+    grid barrier gets a short poll limit and one block skips its first
+    arrival (tosp_inject_wait_fault), so the other blocks give up.  The cycle
+    returns TOSP_ERR_TIMEOUT; the barrier state is reset, and the same handle
+    then gives the same preconditioner output and solve as a handle that never
+    saw the fault.  No kernel waits without bound, traps or faults."""
+    import ctypes as C
+    pb = P.cantilever(32, 16, 16)
+    kw = dict(ngrids=4, cycle=0, omega=0.5, flexible=1 if prec else 0, maxiterMG=2000)
+    s = _solver(tosp_mod, pb, n=1, prec=prec, small_cycle_max=16384, **kw)
+    ref = _solver(tosp_mod, pb, n=1, prec=prec, small_cycle_max=16384, **kw)
+    dens = np.random.default_rng(3).uniform(0.2, 1.0, pb.nelem)
+    s.SetupGMG(dens)
+    ref.SetupGMG(dens)
+    nb = C.c_int32()
+    assert tosp_mod._lib.tosp_small_cycle_blocks(s.h, C.byref(nb)) == 0
+    assert nb.value >= 2, nb.value
+    r = np.random.default_rng(4).standard_normal(pb.freedofs.size)
+    assert tosp_mod._lib.tosp_inject_wait_fault(s.h, 4096, nb.value - 1) == 0
+    with pytest.raises(tosp_mod.TospError) as e:
+        s.MGCycle(r)
+    assert e.value.code == -8                                 # TOSP_ERR_TIMEOUT
+    assert "timed out" in str(e.value)
+    tol = 1e-12 if prec == 0 else 5e-5
+    assert rel_err(s.MGCycle(r), ref.MGCycle(r)) <= tol
+    u1, it1, rr1, rc1 = s.SolveMG(np.zeros(pb.f.size), pb.f)
+    u0, it0, rr0, rc0 = ref.SolveMG(np.zeros(pb.f.size), pb.f)
+    assert rc1 == rc0 == 0 and rr1 <= 1e-8
+    assert abs(pb.f @ u1 - pb.f @ u0) <= 1e-9 * abs(pb.f @ u0)
+
+
+def rel_err(a, b):
+    return np.abs(a - b).max() / np.abs(b).max()

@@ -184,6 +184,62 @@ __device__ __forceinline__ void brick_writeout_nodes(const T *ys, T *__restrict_
     }
 }
 
+// Node sums gathered from per-element corner outputs (eo4[a * BRICK_ELEMS + e]
+// = element e's values at its corner a, zero for elements outside the mesh)
+// and written out node by node.  Each node adds its contributions in corner
+// order 0..7, the order of brick_accumulate4, so the sums are the same; one
+// barrier (eo4 complete) replaces the eight of the corner passes.
+__device__ __forceinline__ void brick_gather_write(const float4 *eo4, float *__restrict__ y,
+                                                   const uint8_t *__restrict__ freemask, const Grid &g, int ex0,
+                                                   int ey0, int ez0, const int32_t *rel, const uint16_t *pk, int tid,
+                                                   bool check) {
+    const int64_t base = brick_base_dof(ex0, ey0, ez0, g);
+    const bool interior = brick_interior(ex0, ey0, ez0, g);
+    for (int ln = tid; ln < BRICK_NODES; ln += BRICK_ELEMS) {
+        const uint16_t p = pk[3 * ln];
+        if (!interior && !brick_slot_in(p, ex0, ey0, ez0, g)) continue;
+        const int ny_ = ln % NBY, nx_ = (ln / NBY) % NBX, nz_ = ln / (NBY * NBX);
+        float v0 = 0.f, v1 = 0.f, v2 = 0.f;
+#pragma unroll
+        for (int a = 0; a < 8; ++a) {
+            const int dx = (a >> 1) & 1, dy = a & 1, dz = (a >> 2) & 1;
+            const int lx = nx_ - dx, ly = ny_ - dy, lz = nz_ - dz;
+            if (lx >= 0 && lx < BX && ly >= 0 && ly < BY && lz >= 0 && lz < BZ) {
+                const float4 c = eo4[a * BRICK_ELEMS + (lz * BX + lx) * BY + ly];
+                v0 += c.x;
+                v1 += c.y;
+                v2 += c.z;
+            }
+        }
+        const int64_t dof = base + rel[3 * ln];
+        const float v[3] = {v0, v1, v2};
+        if (!check) {
+            // one 8-byte access for the two of the node's three values that
+            // share an 8-byte-aligned pair (decided from the address) and one
+            // 4-byte access for the third
+            float *a = y + dof;
+            const bool lo = (reinterpret_cast<uintptr_t>(a) & 7u) == 0;
+            float *pair = lo ? a : a + 1;
+            float *one = lo ? a + 2 : a;
+            const float p0 = lo ? v[0] : v[1], p1 = lo ? v[1] : v[2], s1 = lo ? v[2] : v[0];
+            if (p >> 10) {
+                asm volatile("st.global.v2.f32 [%0], {%1, %2};" ::"l"(pair), "f"(p0), "f"(p1) : "memory");
+                *one = s1;
+            } else {
+                asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(pair), "f"(p0), "f"(p1) : "memory");
+                atomicAdd(one, s1);
+            }
+            continue;
+        }
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            if (!freemask[dof + c]) continue;
+            if (p >> 10) y[dof + c] = v[c];
+            else atomicAdd(&y[dof + c], v[c]);
+        }
+    }
+}
+
 template <typename T>
 __device__ __forceinline__ void brick_writeout(const T *ys, T *__restrict__ y, const uint8_t *__restrict__ freemask,
                                                const Grid &g, int ex0, int ey0, int ez0, int tid) {

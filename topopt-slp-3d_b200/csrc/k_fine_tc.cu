@@ -67,6 +67,7 @@ constexpr int TC_IMG_BYTES = TC_B_BYTES + 16;             // + the block scale r
 constexpr int TC_A_TILE = BRICK_ELEMS / 8 * TC_GROUP;     // 4096 per A step
 constexpr int TC_A_BYTES = 3 * TC_A_TILE;
 constexpr int TC_XS_FLOATS = BRICK_NODES * 4;             // 900: nodes padded to float4
+constexpr int TC_EO_BYTES = 8 * BRICK_ELEMS * 16;         // element outputs: one float4 per corner
 constexpr int TC_W_BYTES = BRICK_ELEMS * 16;              // eight BF16 factors per element
 constexpr int TC_SLOTS_PAD = (BRICK_SLOTS + 3) / 4 * 4;   // slot table length
 constexpr int TC_CHUNK = 64;
@@ -164,15 +165,17 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&r)[64]) {
 }
 
 // Chunk C holds block rows 64C..64C+63: row n is entry i = n % 24 of
-// sub-cell s = n / 24.
+// sub-cell s = n / 24.  Columns t, t+1 (t even) are entries i, i+1 of the
+// same sub-cell, weighted by one packed FMA (two FP32 FMAs, same rounding).
 template <int C>
-__device__ __forceinline__ void consume_chunk(uint32_t taddr, const float (&ws)[8], float (&acc)[24]) {
+__device__ __forceinline__ void consume_chunk(uint32_t taddr, const float2 (&ws2)[8], float2 (&acc)[12]) {
     uint32_t r[64];
     tmem_ld64(taddr, r);
 #pragma unroll
-    for (int t = 0; t < TC_CHUNK; ++t) {
+    for (int t = 0; t < TC_CHUNK; t += 2) {
         const int n = C * TC_CHUNK + t;
-        acc[n % 24] = fmaf(ws[n / 24], __uint_as_float(r[t]), acc[n % 24]);
+        acc[(n % 24) / 2] = __ffma2_rn(ws2[n / 24], make_float2(__uint_as_float(r[t]), __uint_as_float(r[t + 1])),
+                                       acc[(n % 24) / 2]);
     }
 }
 
@@ -190,6 +193,9 @@ __device__ __forceinline__ void issue_chunk(int c, uint32_t tmem, uint32_t a_add
     mma_commit(mbar);
 }
 
+// Entry i of the 24 element outputs held as 12 pairs.
+__device__ __forceinline__ float acc_at(const float2 (&acc)[12], int i) { return (i & 1) ? acc[i >> 1].y : acc[i >> 1].x; }
+
 __device__ __forceinline__ uint32_t half2_bits(__half2 h) {
     uint32_t b;
     memcpy(&b, &h, 4);
@@ -204,12 +210,12 @@ __device__ __forceinline__ uint32_t half2_bits(__half2 h) {
 // address are static (8-byte aligned) shared variables.
 constexpr size_t TC_OFF_A = TC_B_BYTES;
 constexpr size_t TC_OFF_XS = TC_OFF_A + TC_A_BYTES;
-constexpr size_t TC_OFF_YS = TC_OFF_XS + sizeof(float) * TC_XS_FLOATS;
-constexpr size_t TC_OFF_W = TC_OFF_YS + sizeof(float) * TC_XS_FLOATS;
+constexpr size_t TC_OFF_EO = TC_OFF_XS + sizeof(float) * TC_XS_FLOATS;
+constexpr size_t TC_OFF_W = TC_OFF_EO + TC_EO_BYTES;
 constexpr size_t TC_OFF_REL = TC_OFF_W + TC_W_BYTES;
 constexpr size_t TC_OFF_PK = TC_OFF_REL + sizeof(int32_t) * TC_SLOTS_PAD;
 constexpr size_t TC_SMEM = (TC_OFF_PK + sizeof(uint16_t) * TC_SLOTS_PAD + 127) / 128 * 128;
-static_assert(TC_OFF_A % 16 == 0 && TC_OFF_XS % 16 == 0 && TC_OFF_YS % 16 == 0 && TC_OFF_W % 16 == 0,
+static_assert(TC_OFF_A % 16 == 0 && TC_OFF_XS % 16 == 0 && TC_OFF_EO % 16 == 0 && TC_OFF_W % 16 == 0,
               "operand alignment");
 static_assert(TC_OFF_REL % 4 == 0 && TC_OFF_PK % 2 == 0, "slot table alignment");
 static_assert(TC_NCHUNK * TC_CHUNK == TC_NROWS && TC_NCHUNK == 3, "three chunks through two buffers");
@@ -301,7 +307,7 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
                  int *__restrict__ err) {
     extern __shared__ __align__(128) unsigned char smem_raw[];
     float *xs = reinterpret_cast<float *>(smem_raw + TC_OFF_XS);          // staged nodal values
-    float *ys = reinterpret_cast<float *>(smem_raw + TC_OFF_YS);          // node sums
+    float4 *eo4 = reinterpret_cast<float4 *>(smem_raw + TC_OFF_EO);       // element outputs per corner
     unsigned char *abuf = smem_raw + TC_OFF_A;
     int32_t *rel = reinterpret_cast<int32_t *>(smem_raw + TC_OFF_REL);    // slot table
     uint16_t *pk = reinterpret_cast<uint16_t *>(smem_raw + TC_OFF_PK);
@@ -367,19 +373,20 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
         const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
         const bool valid = ex0 + lx < g.nelx && ey0 + ly < g.nely && ez0 + lz < g.nelz;
 
-        float ws[8], acc[24];
+        float2 ws2[8], acc[12];
         {
             const uint4 wv = *reinterpret_cast<const uint4 *>(smem_raw + TC_OFF_W + 16 * tid);
             const uint32_t wq[4] = {wv.x, wv.y, wv.z, wv.w};
             const float f = fsc * inv_ke;
 #pragma unroll
             for (int q = 0; q < 4; ++q) {
-                ws[2 * q] = __uint_as_float(wq[q] << 16) * f;
-                ws[2 * q + 1] = __uint_as_float(wq[q] & 0xFFFF0000u) * f;
+                const float w0 = __uint_as_float(wq[q] << 16) * f, w1 = __uint_as_float(wq[q] & 0xFFFF0000u) * f;
+                ws2[2 * q] = make_float2(w0, w0);
+                ws2[2 * q + 1] = make_float2(w1, w1);
             }
         }
 #pragma unroll
-        for (int i = 0; i < 24; ++i) acc[i] = 0.f;
+        for (int i = 0; i < 12; ++i) acc[i] = make_float2(0.f, 0.f);
 
         bool ok = true;
 #pragma unroll
@@ -392,9 +399,9 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
             if (got) {
                 fence_after();
                 const uint32_t taddr = tlane + (uint32_t)((c & 1) * TC_CHUNK);
-                if (c == 0) consume_chunk<0>(taddr, ws, acc);
-                else if (c == 1) consume_chunk<1>(taddr, ws, acc);
-                else consume_chunk<2>(taddr, ws, acc);
+                if (c == 0) consume_chunk<0>(taddr, ws2, acc);
+                else if (c == 1) consume_chunk<1>(taddr, ws2, acc);
+                else consume_chunk<2>(taddr, ws2, acc);
             }
             fence_before();
             if (__syncthreads_or(!got)) {   // buffer (c & 1) fully read
@@ -407,10 +414,6 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
                 // the same buffers
                 if (next < fg.nbricks) stage_brick(next, xs, smem_raw + TC_OFF_W, x, w, fg, rel, pk, tid);
                 cp_async_commit();
-                // and every thread has finished the previous brick's
-                // write-out; the sums start after later barriers
-                for (int i = tid; i < BRICK_NODES; i += BRICK_ELEMS)
-                    reinterpret_cast<float4 *>(ys)[i] = make_float4(0.f, 0.f, 0.f, 0.f);
                 if (tid == 0) {
                     fence_after();
                     issue_chunk(2, tmem, a_addr, b_addr, mbar0);
@@ -424,8 +427,16 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
             }
             break;
         }
+        // this element's corner outputs (zero outside the mesh); every thread
+        // finished the previous brick's gathers before the first chunk's barrier
+#pragma unroll
+        for (int a = 0; a < 8; ++a)
+            eo4[a * BRICK_ELEMS + tid] = valid ? make_float4(acc_at(acc, 3 * a), acc_at(acc, 3 * a + 1),
+                                                             acc_at(acc, 3 * a + 2), 0.f)
+                                               : make_float4(0.f, 0.f, 0.f, 0.f);
         // every MMA of this brick has completed: the A tiles are free.  The
-        // next brick's inputs are complete and visible after the barrier.
+        // next brick's inputs and the corner outputs are complete and visible
+        // after the barrier.
         cp_async_wait_0();
         __syncthreads();
         if (next < fg.nbricks) {
@@ -438,8 +449,7 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
             issue_chunk(0, tmem, a_addr, b_addr, mbar0);
             issue_chunk(1, tmem, a_addr, b_addr, mbar1);
         }
-        brick_accumulate4(reinterpret_cast<float4 *>(ys), acc, valid, ln0);
-        brick_writeout_nodes<float>(ys, y, freemask, g, ex0, ey0, ez0, rel, pk, tid, chk);
+        brick_gather_write(eo4, y, freemask, g, ex0, ey0, ez0, rel, pk, tid, chk);
     }
     cp_async_wait_0();
 

@@ -15,7 +15,9 @@
 // ld.global.cg (L2, coherent across the grid after the barrier's acquire);
 // stencils, diagonals, masks and the coarsest inverse are read-only for the
 // whole kernel.  The barrier's wait is bounded: on time-out it sets bar->err
-// and every block leaves the step loop.
+// and every block leaves the step loop.  The poll limit and one block that
+// skips its first arrival can be set from the host (tosp_inject_wait_fault),
+// so tests make the wait run out without faulting or hanging the GPU.
 #include "tosp_internal.h"
 
 namespace tosp {
@@ -39,10 +41,14 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
 }
 
 // Grid-wide barrier over the co-resident blocks of a cooperative launch.
-__device__ __forceinline__ bool grid_barrier(GridBarrier *bar, unsigned nblocks) {
+// limit: polls before the wait gives up; skip: this block does not arrive
+// (a fault injected by tests: the other blocks' waits then run out).
+__device__ __forceinline__ bool grid_barrier(GridBarrier *bar, unsigned nblocks, uint32_t limit, bool skip) {
     __shared__ int s_ok;
     __syncthreads();
-    if (threadIdx.x == 0) {
+    if (threadIdx.x == 0 && skip) {
+        s_ok = 1;
+    } else if (threadIdx.x == 0) {
         int ok = 1;
         const unsigned g = ld_acquire(&bar->gen);
         __threadfence();
@@ -53,7 +59,7 @@ __device__ __forceinline__ bool grid_barrier(GridBarrier *bar, unsigned nblocks)
         } else {
             uint32_t it = 0;
             while (ld_acquire(&bar->gen) == g) {
-                if (++it >= SMALL_WAIT_LIMIT) {
+                if (++it >= limit) {
                     atomicExch(&bar->err, 1);
                     ok = 0;
                     break;
@@ -217,6 +223,8 @@ k_small_cycle(const SmallStep<T> *__restrict__ steps, int nsteps, GridBarrier *b
     const int64_t nt = (int64_t)gridDim.x * blockDim.x;
     const int64_t warp = tid >> 5, nwarps = nt >> 5;
     const int lane = threadIdx.x & 31;
+    const uint32_t limit = bar->limit ? bar->limit : SMALL_WAIT_LIMIT;
+    const bool skip_first = bar->skip == (int)blockIdx.x + 1;
     for (int k = 0; k < nsteps; ++k) {
         const SmallStep<T> s = steps[k];
         switch (s.kind) {
@@ -239,7 +247,7 @@ k_small_cycle(const SmallStep<T> *__restrict__ steps, int nsteps, GridBarrier *b
             for (int64_t i = tid; i < s.g.ndof; i += nt) s.y[i] = s.x ? ldc(s.x + i) : T(0);
             break;
         }
-        if (k + 1 < nsteps && !grid_barrier(bar, gridDim.x)) return;
+        if (k + 1 < nsteps && !grid_barrier(bar, gridDim.x, limit, skip_first && k == 0)) return;
     }
 }
 

@@ -1397,6 +1397,32 @@ int tosp_time_operator(tosp_handle *h, int32_t precision, int32_t reps, double *
     return check_tc(h);
 }
 
+int tosp_inject_wait_fault(tosp_handle *h, int32_t polls, int32_t skip_block) {
+    if (!h || polls < 1 || skip_block < -1) return TOSP_ERR_BAD_ARG;
+    cudaSetDevice(h->device);
+    if (!h->d_bar || h->small_l < 0) {
+        h->err = "no persistent small-level cycle on this handle (set small_cycle_max and run tosp_setup_gmg)";
+        return TOSP_ERR_STATE;
+    }
+    if (skip_block >= h->small_blocks) {
+        h->err = "skip_block beyond the cycle's " + std::to_string(h->small_blocks) + " blocks";
+        return TOSP_ERR_BAD_ARG;
+    }
+    CK(cudaStreamSynchronize(h->stream));
+    GridBarrier b{};
+    CK(cudaMemcpy(&b, h->d_bar, sizeof b, cudaMemcpyDeviceToHost));
+    b.limit = (unsigned)polls;
+    b.skip = skip_block + 1;
+    CK(cudaMemcpy(h->d_bar, &b, sizeof b, cudaMemcpyHostToDevice));
+    return TOSP_OK;
+}
+
+int tosp_small_cycle_blocks(const tosp_handle *h, int32_t *blocks) {
+    if (!h || !blocks) return TOSP_ERR_BAD_ARG;
+    *blocks = h->small_l >= 0 ? h->small_blocks : 0;
+    return TOSP_OK;
+}
+
 int tosp_elem_stiff_mr(double el, double eh, double ew, double nu, int32_t n, double *kv) {
     if (!kv || n < 1 || n > 4 || !(el > 0) || !(eh > 0) || !(ew > 0)) return TOSP_ERR_BAD_ARG;
     std::vector<double> ks;

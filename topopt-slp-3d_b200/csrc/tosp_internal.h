@@ -213,7 +213,10 @@ struct SmallStep {
 };
 struct GridBarrier {
     unsigned count, gen;
-    int err, pad;
+    int err;
+    unsigned limit;   // polls before a wait gives up (0: SMALL_WAIT_LIMIT)
+    int skip;         // k > 0: block k - 1 skips its first arrival (fault injection for tests)
+    int pad;
 };
 // Largest grid of 256-thread blocks that can be co-resident (cooperative launch).
 int small_cycle_max_blocks(bool fp64);

@@ -92,6 +92,8 @@ def _load():
         "tosp_kernel_launches": (C.c_int64, []),
         "tosp_time_operator": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32, P(C.c_double)]),
         "tosp_kelem_prod_noalloc": (C.c_int, [C.c_void_p, d, d, C.c_int64]),
+        "tosp_inject_wait_fault": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
+        "tosp_small_cycle_blocks": (C.c_int, [C.c_void_p, P(C.c_int32)]),
         "tosp_server_create": (C.c_int, [C.c_int32, C.c_int64, P(C.c_void_p)]),
         "tosp_server_submit": (C.c_int, [C.c_void_p, P(_Problem), P(MgParams), C.c_int32, d, C.c_int64, d, C.c_int64,
                                          P(C.c_int64)]),
