@@ -657,8 +657,8 @@ def main():
                           "nominal_peak_tflops": 37.0}}
     rf32 = {"bound": "hbm", "achieved": round(ach32, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": round(ach32 / peaks["hbm_gbs"], 4), "traffic": traffic.get("fp32_operator_bytes_per_launch"),
-            "kernel": "k_fine_apply_tc2 (V-cycle operator, tcgen05 sub-cell block products)" if n == 2 else
-                      "k_fine_apply<float,bf16> (V-cycle operator)",
+            "kernel": f"k_fine_apply_tc<{n}> (V-cycle operator, tcgen05 sub-cell block products)"
+                      if (n * pb.nely) % 2 == 0 else "k_fine_apply<float,bf16> (V-cycle operator)",
             "algorithmic_bytes_per_launch": bytes32, "ms_per_launch": round(ms_op32, 4), "peak_source": peak_kind}
     # the dominant kernel of the timed step carries the contract's roofline
     roofline, roofline_other = (rf64, rf32) if share64 >= share32 else (rf32, rf64)

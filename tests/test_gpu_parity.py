@@ -69,12 +69,16 @@ def bf16_round(a):
 
 
 @pytest.mark.parametrize("dims,n", [((8, 4, 4), 2), ((10, 9, 3), 2), ((12, 16, 6), 2), ((4, 8, 12), 2),
-                                    ((6, 10, 2), 1), ((4, 4, 4), 3)])
+                                    ((6, 10, 2), 1), ((9, 6, 5), 1), ((16, 8, 8), 1),
+                                    ((4, 4, 4), 3), ((5, 6, 3), 3), ((8, 10, 4), 3),
+                                    ((5, 7, 3), 1), ((6, 5, 4), 3)])
 def test_mixed_operator_parity(tosp_mod, dims, n):
-    """The V-cycle's FP32/BF16 finest operator (tensor-core element matrices
-    for MR factor 2) against the FP64 oracle product with the same
-    BF16-rounded SIMP factors: max error <= 1e-5 of max |y| (FP32 vectors and
-    accumulation).  Ragged meshes leave partially filled element bricks."""
+    """The V-cycle's FP32/BF16 finest operator (tensor-core sub-cell block
+    products for MR factors 1, 2 and 3 when n * nely is even; the CUDA-core
+    kernel for the last two meshes, whose n * nely is odd) against the FP64
+    oracle product with the same BF16-rounded SIMP factors: max error <= 1e-5
+    of max |y| (FP32 vectors and accumulation).  Ragged meshes leave partially
+    filled element bricks."""
     pb = P.cantilever(*dims)
     dens = make(pb, n, seed=sum(dims) + 1)
     s = solver(tosp_mod, pb, n, prec=1)
@@ -301,3 +305,17 @@ def test_fixture_problem_solve(tosp_mod):
     u, it, rr, rc = s.SolveMG(np.zeros(pb.f.size), pb.f)
     assert abs(it - ito) <= 1
     assert abs(pb.f @ u - pb.f @ uo) <= 1e-9 * abs(pb.f @ uo)
+
+
+def test_coarsest_above_dense_limit_adds_a_grid(tosp_mod):
+    """A coarsest system between the dense direct solve's 24 576 dofs and
+    nmaxchol = 60 000 (here 28 611 dofs with 2 grids) gets one more grid, the
+    reference's own rule for systems above nmaxchol; the solve still reaches
+    the tolerance."""
+    pb = P.cantilever(64, 32, 32)
+    s = solver(tosp_mod, pb, 1, ngrids=2, nmaxchol=60000, maxiterMG=2000)
+    info = s.info()
+    assert info["ngrids"] == 3 and info["ncoarse"] == 3 * 17 * 9 * 9
+    s.SetupGMG(np.full(pb.nelem, 0.4))
+    u, it, rr, rc = s.SolveMG(np.zeros(pb.f.size), pb.f)
+    assert rc == 0 and rr <= 1e-8

@@ -1,17 +1,22 @@
-// Finest-level operator of the mixed-precision V-cycle, MR factor 2, on the
-// 5th-generation tensor cores.
+// Finest-level operator of the mixed-precision V-cycle on the 5th-generation
+// tensor cores, for multiresolution factors n = 1, 2 and 3.
 //
-// y_e = sum_s w_s KE_s u_e (I/WOK/KelemProd.m:57-100).  For a brick of 128
-// elements the products of the eight shared 24x24 sub-cell blocks with every
-// element's nodal vector are one GEMM (M = 128 elements, N = 8 x 24 = 192 block
-// rows, K = 24 element dofs, kind::f16, FP32 accumulator):
+// y_e = sum_s w_s KE_s u_e (I/WOK/KelemProd.m:57-100) over the n^3 density
+// sub-cells s of displacement element e.  For a brick of 128 elements the
+// products of the shared 24x24 sub-cell blocks with every element's nodal
+// vector are one GEMM (M = 128 elements, N = 24 n^3 block rows, K = 24 element
+// dofs, kind::f16, FP32 accumulator):
 //
 //     D[e][24 s + i] = sum_j KE_s[i][j] u_e[j],
 //
-// and each thread weights its element's 192 values with the element's eight
-// SIMP factors on the CUDA cores (192 FMAs per element):
+// and each thread weights its element's 24 n^3 values with the element's n^3
+// SIMP factors on the CUDA cores, two values per packed FMA (fma.rn.f32x2,
+// the rounding of two FP32 FMAs):
 //
 //     y_e[i] = sum_s w_s D[e][24 s + i].
+//
+// 24 n^3 FMAs per element instead of the 300 (n^3 + 2) of forming K_e on the
+// CUDA cores (n = 3: 648 against 8 700).
 //
 // FP16 operands carry each value in two pieces.  u_e is scaled by a power of
 // two per element (largest entry in [2^13, 2^14)) and split into hi + lo; the
@@ -30,24 +35,34 @@
 // so A holds three 16-wide tiles per element row and the B image five.  The
 // weights stay BF16 (exact in FP32), the same factors the coarse levels use.
 //
-// Pipelining inside a CTA: the 192 accumulator columns are produced in three
-// 64-column chunks through two tensor-memory buffers, so the MMAs of chunk
-// c+1 run while the threads consume chunk c.  Once the first chunk is read
-// (every thread then holds the brick's factors and the A tiles are built), the
-// next brick's nodal values and factors are staged with cp.async into the same
-// buffers; once the last chunk is read, the A tiles are rebuilt for the next
-// brick and that brick's first two chunks run during the current brick's node
-// sums and write-out.  Single node, factor and A buffers keep a CTA at 55 KB of
-// shared memory, so four CTAs (4 x 128 tensor-memory columns) share an SM.
-// Every wait on an MMA-completion barrier is bounded; a timeout sets *err,
-// leaves the brick loop and still frees the tensor memory.  Node sums and the
-// write-out are those of the CUDA-core kernels (brick.cuh).
+// Pipelining inside a CTA: the accumulator columns are produced in chunks
+// (64 columns; 32 for n = 1, whose 24 rows are one chunk) through two
+// tensor-memory buffers, so the MMAs of chunk c+2 are issued as soon as chunk c
+// is read and run while the threads consume chunk c+1.  Once the first chunk
+// is read (every thread then holds the brick's factors and the A tiles are
+// built), the next brick's nodal values and factors are staged with cp.async
+// into the same buffers; once the last chunk is read, each thread stores its
+// element's corner outputs, the A tiles are rebuilt for the next brick and
+// that brick's first two chunks run during the current brick's node gather
+// and write-out (brick.cuh: one node per thread sums the outputs of its up
+// to eight elements in corner order, then stores it, or adds it atomically on
+// the brick's faces).  Every wait on an MMA-completion barrier is bounded; a
+// timeout sets *err, leaves the brick loop and still frees the tensor memory.
+//
+// A CTA runs NB such bricks side by side (two; three for n = 3), four warps
+// each, so they share one copy of the B image (30 KB for n = 2, 103 KB for
+// n = 3): two CTAs of eight warps per SM for n = 2, one of twelve for n = 3.
+//
+// The factors are staged as the brick's slab of the density mesh (rows along
+// y of 8n BF16 values copied in 4-byte pieces), which needs n * nely even; the
+// host uses the CUDA-core kernel otherwise.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <utility>
 #include <vector>
 
 #include "brick.cuh"
@@ -58,24 +73,56 @@ namespace tosp {
 namespace {
 
 constexpr int TC_K = 16;                                  // K of every MMA (kind::f16)
-constexpr int TC_NROWS = 192;                             // B rows: 8 sub-cells x 24 block rows
 constexpr int TC_GROUP = 8 * TC_K * 2;                    // bytes of one 8-row group (256)
-constexpr int TC_B_TILE = TC_NROWS / 8 * TC_GROUP;        // 6144 per B step
 constexpr int TC_B_STEPS = 5;
-constexpr int TC_B_BYTES = TC_B_STEPS * TC_B_TILE;        // 30720
-constexpr int TC_IMG_BYTES = TC_B_BYTES + 16;             // + the block scale record
 constexpr int TC_A_TILE = BRICK_ELEMS / 8 * TC_GROUP;     // 4096 per A step
 constexpr int TC_A_BYTES = 3 * TC_A_TILE;
 constexpr int TC_XS_FLOATS = BRICK_NODES * 4;             // 900: nodes padded to float4
 constexpr int TC_EO_BYTES = 8 * BRICK_ELEMS * 16;         // element outputs: one float4 per corner
-constexpr int TC_W_BYTES = BRICK_ELEMS * 16;              // eight BF16 factors per element
 constexpr int TC_SLOTS_PAD = (BRICK_SLOTS + 3) / 4 * 4;   // slot table length
-constexpr int TC_CHUNK = 64;
-constexpr int TC_NCHUNK = TC_NROWS / TC_CHUNK;            // 3
-constexpr int TC_COLS = 2 * TC_CHUNK;                     // tensor-memory columns per CTA
-constexpr int TC_CTAS_PER_SM = 512 / TC_COLS;
 constexpr uint32_t TC_WAIT_LIMIT = 1u << 16;              // try_wait rounds before giving up
 constexpr uint32_t TC_SUSPEND_NS = 20000;                 // suspend-time hint of one try_wait round
+
+// Sizes of the kernel for MR factor N.
+template <int N>
+struct Tc {
+    static constexpr int NS = N * N * N;                  // sub-cells per element
+    static constexpr int NROWS = 24 * NS;                 // block rows (GEMM N)
+    static constexpr int NPAD = (NROWS + 15) / 16 * 16;   // padded to the MMA's N granularity
+    static constexpr int CH = N == 1 ? 32 : 64;           // accumulator columns per chunk
+    static constexpr int NCH = (NPAD + CH - 1) / CH;
+    static constexpr int COLS = 2 * CH;                   // tensor-memory columns per CTA
+    static constexpr int B_TILE = NPAD / 8 * TC_GROUP;    // bytes of one B step
+    static constexpr int B_BYTES = TC_B_STEPS * B_TILE;
+    static constexpr int IMG_BYTES = B_BYTES + 16;        // + the block scale record
+    static constexpr int WY = BY * N, WX = BX * N, WZ = BZ * N;   // factor slab (density cells)
+    static constexpr int W_BYTES = (WY * WX * WZ * 2 + 15) / 16 * 16;
+    static constexpr int UPR = WY / 2;                    // 4-byte pieces per slab row
+    // bricks processed side by side by one CTA, sharing the B image: four
+    // warps each, their own A tiles, staging, outputs, barriers and
+    // tensor-memory columns
+    static constexpr int NB = N == 3 ? 3 : 2;
+    static constexpr int THREADS = NB * BRICK_ELEMS;
+    static constexpr int TMEM_COLS = NB * COLS <= 64 ? 64 : (NB * COLS <= 128 ? 128 : (NB * COLS <= 256 ? 256 : 512));
+    // layout: B image, slot table, then one region per brick
+    static constexpr size_t OFF_REL = B_BYTES;
+    static constexpr size_t OFF_PK = OFF_REL + sizeof(int32_t) * TC_SLOTS_PAD;
+    static constexpr size_t OFF_G = (OFF_PK + sizeof(uint16_t) * TC_SLOTS_PAD + 127) / 128 * 128;
+    static constexpr size_t G_A = 0;                      // offsets inside a brick's region
+    static constexpr size_t G_XS = G_A + TC_A_BYTES;
+    static constexpr size_t G_EO = G_XS + sizeof(float) * TC_XS_FLOATS;
+    static constexpr size_t G_W = G_EO + TC_EO_BYTES;
+    static constexpr size_t G_BYTES = (G_W + W_BYTES + 127) / 128 * 128;
+    static constexpr size_t SMEM = OFF_G + NB * G_BYTES;
+    static constexpr int MINB = N == 3 ? 1 : (N == 2 ? 2 : 3);   // register cap: CTAs per SM aimed at
+    static_assert(B_TILE % 16 == 0 && OFF_G % 16 == 0 && G_BYTES % 16 == 0 && G_XS % 16 == 0 &&
+                      G_EO % 16 == 0 && G_W % 16 == 0, "operand alignment");
+    static_assert(OFF_REL % 4 == 0 && OFF_PK % 2 == 0, "slot table alignment");
+    static_assert(SMEM <= 227 * 1024, "shared memory per CTA");
+    static_assert(NB * COLS <= 512, "tensor memory of an SM");
+};
+
+__host__ __device__ constexpr int chunk_width(int npad, int ch, int c) { return npad - c * ch < ch ? npad - c * ch : ch; }
 
 // Canonical no-swizzle K-major layout with K = 16: 8-row x 16-byte core
 // matrices, the two core matrices of a row group 128 B apart (leading byte
@@ -98,7 +145,7 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr) {
 }
 
 // kind::f16 instruction descriptor: FP32 accumulator, FP16 A and B (format
-// code 0), both K-major, M = 128.
+// code 0), both K-major, M = 128, N = n (a multiple of 16, at most 256).
 __host__ __device__ constexpr uint32_t idesc_f16(int n) {
     return (1u << 4) | ((uint32_t)(n >> 3) << 17) | ((uint32_t)(128 >> 4) << 24);
 }
@@ -132,6 +179,24 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t phase) {
     return false;
 }
 
+// Barriers of one brick group (four warps, named barrier 1 + group; 0 is
+// __syncthreads).
+__device__ __forceinline__ void group_sync(int grp) {
+    asm volatile("bar.sync %0, %1;" ::"r"(1 + grp), "r"(BRICK_ELEMS) : "memory");
+}
+__device__ __forceinline__ bool group_sync_or(int grp, bool pred) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, %2, %3, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)pred), "r"(1 + grp), "r"(BRICK_ELEMS)
+        : "memory");
+    return r != 0;
+}
+
 __device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
@@ -144,8 +209,12 @@ __device__ __forceinline__ void cp_async4(void *dst, const void *src, int nbytes
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// 64 consecutive columns of this warp's 32 lanes (one column per register).
-__device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&r)[64]) {
+// W consecutive columns of this warp's 32 lanes (one column per register).
+template <int W>
+__device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t (&r)[W]);
+
+template <>
+__device__ __forceinline__ void tmem_ld<64>(uint32_t taddr, uint32_t (&r)[64]) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x64.b32 "
         "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
@@ -164,32 +233,72 @@ __device__ __forceinline__ void tmem_ld64(uint32_t taddr, uint32_t (&r)[64]) {
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
-// Chunk C holds block rows 64C..64C+63: row n is entry i = n % 24 of
-// sub-cell s = n / 24.  Columns t, t+1 (t even) are entries i, i+1 of the
-// same sub-cell, weighted by one packed FMA (two FP32 FMAs, same rounding).
-template <int C>
-__device__ __forceinline__ void consume_chunk(uint32_t taddr, const float2 (&ws2)[8], float2 (&acc)[12]) {
-    uint32_t r[64];
-    tmem_ld64(taddr, r);
+template <>
+__device__ __forceinline__ void tmem_ld<32>(uint32_t taddr, uint32_t (&r)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+template <>
+__device__ __forceinline__ void tmem_ld<16>(uint32_t taddr, uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+}
+
+// Chunk C holds block rows C*CH .. C*CH + width - 1: row r is entry
+// i = r % 24 of sub-cell s = r / 24 (rows from 24 n^3 on are padding).
+// Columns t, t+1 (t even) are entries i, i+1 of the same sub-cell, weighted
+// by one packed FMA.
+template <int N, int C>
+__device__ __forceinline__ void consume_chunk(uint32_t taddr, const float (&ws)[Tc<N>::NS], float2 (&acc)[12]) {
+    constexpr int W = chunk_width(Tc<N>::NPAD, Tc<N>::CH, C);
+    uint32_t r[W];
+    tmem_ld<W>(taddr, r);
 #pragma unroll
-    for (int t = 0; t < TC_CHUNK; t += 2) {
-        const int n = C * TC_CHUNK + t;
-        acc[(n % 24) / 2] = __ffma2_rn(ws2[n / 24], make_float2(__uint_as_float(r[t]), __uint_as_float(r[t + 1])),
-                                       acc[(n % 24) / 2]);
+    for (int t = 0; t < W; t += 2) {
+        const int row = C * Tc<N>::CH + t;
+        if (row < Tc<N>::NROWS) {
+            const float w = ws[row / 24];
+            acc[(row % 24) / 2] = __ffma2_rn(make_float2(w, w),
+                                             make_float2(__uint_as_float(r[t]), __uint_as_float(r[t + 1])),
+                                             acc[(row % 24) / 2]);
+        }
     }
+}
+
+// consume_chunk for a chunk index known after unrolling.
+template <int N, int... Cs>
+__device__ __forceinline__ void consume_any(int c, uint32_t taddr, const float (&ws)[Tc<N>::NS], float2 (&acc)[12],
+                                            std::integer_sequence<int, Cs...>) {
+    ((c == Cs ? consume_chunk<N, Cs>(taddr, ws, acc) : void()), ...);
 }
 
 // The five MMAs of chunk c into tensor-memory buffer (c & 1), then a commit to
 // its barrier.
+template <int N>
 __device__ __forceinline__ void issue_chunk(int c, uint32_t tmem, uint32_t a_addr, uint32_t b_addr, uint32_t mbar) {
-    const uint32_t d = tmem + (uint32_t)((c & 1) * TC_CHUNK);
-    const uint32_t boff = (uint32_t)(c * TC_CHUNK / 8 * TC_GROUP);
-    constexpr uint32_t id = idesc_f16(TC_CHUNK);
+    using K = Tc<N>;
+    const uint32_t d = tmem + (uint32_t)((c & 1) * K::CH);
+    const uint32_t boff = (uint32_t)(c * K::CH / 8 * TC_GROUP);
+    const uint32_t id = idesc_f16(chunk_width(K::NPAD, K::CH, c));
     mma_f16(d, smem_desc(a_addr), smem_desc(b_addr + boff), id, 0u);
-    mma_f16(d, smem_desc(a_addr + TC_A_TILE), smem_desc(b_addr + TC_B_TILE + boff), id, 1u);
-    mma_f16(d, smem_desc(a_addr + 2 * TC_A_TILE), smem_desc(b_addr + 2 * TC_B_TILE + boff), id, 1u);
-    mma_f16(d, smem_desc(a_addr), smem_desc(b_addr + 3 * TC_B_TILE + boff), id, 1u);
-    mma_f16(d, smem_desc(a_addr + TC_A_TILE), smem_desc(b_addr + 4 * TC_B_TILE + boff), id, 1u);
+    mma_f16(d, smem_desc(a_addr + TC_A_TILE), smem_desc(b_addr + K::B_TILE + boff), id, 1u);
+    mma_f16(d, smem_desc(a_addr + 2 * TC_A_TILE), smem_desc(b_addr + 2 * K::B_TILE + boff), id, 1u);
+    mma_f16(d, smem_desc(a_addr), smem_desc(b_addr + 3 * K::B_TILE + boff), id, 1u);
+    mma_f16(d, smem_desc(a_addr + TC_A_TILE), smem_desc(b_addr + 4 * K::B_TILE + boff), id, 1u);
     mma_commit(mbar);
 }
 
@@ -202,28 +311,13 @@ __device__ __forceinline__ uint32_t half2_bits(__half2 h) {
     return b;
 }
 
-}  // namespace
-
-// Dynamic shared memory: the B image, the A tiles, the staged nodal values,
-// the node sums, the factors and the brick slot table.  The MMA
-// operands need 16-byte aligned starts; the barriers and the tensor-memory
-// address are static (8-byte aligned) shared variables.
-constexpr size_t TC_OFF_A = TC_B_BYTES;
-constexpr size_t TC_OFF_XS = TC_OFF_A + TC_A_BYTES;
-constexpr size_t TC_OFF_EO = TC_OFF_XS + sizeof(float) * TC_XS_FLOATS;
-constexpr size_t TC_OFF_W = TC_OFF_EO + TC_EO_BYTES;
-constexpr size_t TC_OFF_REL = TC_OFF_W + TC_W_BYTES;
-constexpr size_t TC_OFF_PK = TC_OFF_REL + sizeof(int32_t) * TC_SLOTS_PAD;
-constexpr size_t TC_SMEM = (TC_OFF_PK + sizeof(uint16_t) * TC_SLOTS_PAD + 127) / 128 * 128;
-static_assert(TC_OFF_A % 16 == 0 && TC_OFF_XS % 16 == 0 && TC_OFF_EO % 16 == 0 && TC_OFF_W % 16 == 0,
-              "operand alignment");
-static_assert(TC_OFF_REL % 4 == 0 && TC_OFF_PK % 2 == 0, "slot table alignment");
-static_assert(TC_NCHUNK * TC_CHUNK == TC_NROWS && TC_NCHUNK == 3, "three chunks through two buffers");
-
-// Stage brick `brick` (nodal values, SIMP factors) with cp.async.
-__device__ __forceinline__ void stage_brick(int64_t brick, float *xs, unsigned char *wbuf, const float *__restrict__ x,
+// Stage brick `brick` (nodal values, and the brick's slab of SIMP factors on
+// the density mesh) with cp.async; absent nodes and cells read as zero.
+template <int N>
+__device__ __forceinline__ void stage_brick(int64_t brick, float *xs, uint16_t *wslab, const float *__restrict__ x,
                                             const __nv_bfloat16 *__restrict__ w, const FineGeom &fg,
                                             const int32_t *rel, const uint16_t *pk, int tid) {
+    using K = Tc<N>;
     const Grid &g = fg.g;
     int bbx, bby, bbz;
     brick_xyz(brick, fg, bbx, bby, bbz);
@@ -248,17 +342,18 @@ __device__ __forceinline__ void stage_brick(int64_t brick, float *xs, unsigned c
             cp_async4(dst + 2, in ? src + 2 : x, in ? 4 : 0);
         }
     }
-    const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
-    const int ex = ex0 + lx, ey = ey0 + ly, ez = ez0 + lz;
-    const bool valid = ex < g.nelx && ey < g.nely && ez < g.nelz;
-    unsigned char *wr = wbuf + 16 * tid;
-    const __nv_bfloat16 *wb = w + ((int64_t)(ez * 2) * fg.nelx_d + ex * 2) * fg.nely_d + ey * 2;
-#pragma unroll
-    for (int s = 0; s < 8; s += 2) {
-        // sub-cubes s and s+1 differ in y only: adjacent in the density mesh
-        const int sx = (s >> 1) & 1, sz = s >> 2;
-        const __nv_bfloat16 *src = valid ? wb + ((int64_t)sz * fg.nelx_d + sx) * fg.nely_d : w;
-        cp_async4(wr + 2 * s, src, valid ? 4 : 0);
+    // factor slab: rows along y of WY values, 4-byte pieces (two cells); the
+    // density mesh has n * nely cells along y, an even number, so a piece is
+    // wholly inside or wholly outside the mesh and 4-byte aligned
+    const int nelz_d = g.nelz * N;
+    const int xd0 = ex0 * N, yd0 = ey0 * N, zd0 = ez0 * N;
+    for (int u = tid; u < K::WZ * K::WX * K::UPR; u += BRICK_ELEMS) {
+        const int row = u / K::UPR, k = u - row * K::UPR;
+        const int rz = row / K::WX, rx = row - rz * K::WX;
+        const int zd = zd0 + rz, xd = xd0 + rx, yd = yd0 + 2 * k;
+        const bool in = zd < nelz_d && xd < fg.nelx_d && yd < fg.nely_d;
+        const __nv_bfloat16 *src = in ? w + ((int64_t)zd * fg.nelx_d + xd) * fg.nely_d + yd : w;
+        cp_async4(wslab + row * K::WY + 2 * k, src, in ? 4 : 0);
     }
 }
 
@@ -301,71 +396,92 @@ __device__ __forceinline__ float build_a(const float *xs, unsigned char *abuf, i
     return __uint_as_float((E - 13u) << 23);
 }
 
-__global__ void __launch_bounds__(BRICK_ELEMS, 4)
-k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_bfloat16 *__restrict__ w,
-                 const uint8_t *__restrict__ freemask, const uint4 *__restrict__ bimg, FineGeom fg,
-                 int *__restrict__ err) {
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    float *xs = reinterpret_cast<float *>(smem_raw + TC_OFF_XS);          // staged nodal values
-    float4 *eo4 = reinterpret_cast<float4 *>(smem_raw + TC_OFF_EO);       // element outputs per corner
-    unsigned char *abuf = smem_raw + TC_OFF_A;
-    int32_t *rel = reinterpret_cast<int32_t *>(smem_raw + TC_OFF_REL);    // slot table
-    uint16_t *pk = reinterpret_cast<uint16_t *>(smem_raw + TC_OFF_PK);
-    __shared__ __align__(8) uint64_t s_mbar[2];
-    __shared__ __align__(8) uint32_t s_tmem;
-    __shared__ int s_fail;
+}  // namespace
 
-    const int tid = threadIdx.x, warp = tid >> 5;
+// Dynamic shared memory: the B image and the brick slot table (shared by the
+// CTA's bricks), then per brick its A tiles, staged nodal values, element
+// outputs and factor slab.  The MMA operands need 16-byte aligned starts; the
+// barriers and the tensor-memory address are static (8-byte aligned) shared
+// variables.  Threads 128 g .. 128 g + 127 (warps 4g .. 4g+3) form brick group
+// g: bricks g, g + NB, ... of the CTA's share, with the group's own named
+// barrier, MMA-completion barriers and tensor-memory columns (lanes 0-127 of
+// columns COLS g .. COLS (g+1) - 1, which its warps reach as warps 0-3 would).
+template <int N>
+__global__ void __launch_bounds__(Tc<N>::THREADS, Tc<N>::MINB)
+k_fine_apply_tc(const float *__restrict__ x, float *__restrict__ y, const __nv_bfloat16 *__restrict__ w,
+                const uint8_t *__restrict__ freemask, const uint4 *__restrict__ bimg, FineGeom fg,
+                int *__restrict__ err) {
+    using K = Tc<N>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t s_mbar[2 * K::NB];
+    __shared__ __align__(8) uint32_t s_tmem;
+    __shared__ int s_fail[K::NB];
+
+    const int ttid = threadIdx.x;
+    const int grp = ttid / BRICK_ELEMS, tid = ttid - grp * BRICK_ELEMS;   // group, thread within it
+    const int warp = tid >> 5;                                           // warp within the group
     if (smem_u32(smem_raw) & 15u) {   // operand tiles need 16-byte aligned starts
-        if (tid == 0) atomicExch(err, 2);
+        if (ttid == 0) atomicExch(err, 2);
         return;
     }
+    int32_t *rel = reinterpret_cast<int32_t *>(smem_raw + K::OFF_REL);    // slot table
+    uint16_t *pk = reinterpret_cast<uint16_t *>(smem_raw + K::OFF_PK);
+    unsigned char *gbase = smem_raw + K::OFF_G + grp * K::G_BYTES;
+    unsigned char *abuf = gbase + K::G_A;
+    float *xs = reinterpret_cast<float *>(gbase + K::G_XS);              // staged nodal values
+    float4 *eo4 = reinterpret_cast<float4 *>(gbase + K::G_EO);           // element outputs per corner
+    uint16_t *wslab = reinterpret_cast<uint16_t *>(gbase + K::G_W);      // SIMP factors (BF16 bits)
+
     const Grid &g = fg.g;
-    for (int i = tid; i < TC_B_BYTES / 16; i += BRICK_ELEMS) reinterpret_cast<uint4 *>(smem_raw)[i] = bimg[i];
-    const float inv_ke = reinterpret_cast<const float *>(bimg)[TC_B_BYTES / 4];   // undoes the block scale
-    brick_slots_init(rel, pk, g, tid);
+    for (int i = ttid; i < K::B_BYTES / 16; i += K::THREADS) reinterpret_cast<uint4 *>(smem_raw)[i] = bimg[i];
+    const float inv_ke = reinterpret_cast<const float *>(bimg)[K::B_BYTES / 4];   // undoes the block scale
+    if (grp == 0) brick_slots_init(rel, pk, g, tid);
     if (tid == 0) {
-        s_fail = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar[0])) : "memory");
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar[1])) : "memory");
+        s_fail[grp] = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar[2 * grp])) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&s_mbar[2 * grp + 1])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 0) {
+    if (ttid < 32) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&s_tmem)),
-                     "r"(TC_COLS)
+                     "r"(K::TMEM_COLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     fence_before();
     __syncthreads();
     fence_after();
-    const uint32_t tmem = s_tmem;
-    const uint32_t tlane = tmem + ((uint32_t)(warp * 32) << 16);    // this warp's 32 lanes
-    const uint32_t mbar0 = smem_u32(&s_mbar[0]), mbar1 = smem_u32(&s_mbar[1]);
+    const uint32_t tmem = s_tmem + (uint32_t)(grp * K::COLS);           // this group's columns
+    const uint32_t tlane = tmem + ((uint32_t)(warp * 32) << 16);        // this warp's 32 lanes
+    const uint32_t mbar0 = smem_u32(&s_mbar[2 * grp]), mbar1 = smem_u32(&s_mbar[2 * grp + 1]);
     const uint32_t b_addr = smem_u32(smem_raw);
     const uint32_t a_addr = smem_u32(abuf);
     uint32_t ph0 = 0, ph1 = 0;
 
     const int ly = tid % BY, lx = (tid / BY) % BX, lz = tid / (BY * BX);
     const int ln0 = brick_base_node(tid);
+    const int64_t first = (int64_t)blockIdx.x * K::NB + grp, stride = (int64_t)gridDim.x * K::NB;
 
     // Prologue: the first brick's inputs and A tiles, then its first two
-    // chunks.  The grid never exceeds the brick count.
-    stage_brick(blockIdx.x, xs, smem_raw + TC_OFF_W, x, w, fg, rel, pk, tid);
-    cp_async_commit();
-    cp_async_wait_0();
-    __syncthreads();
-    float fsc = build_a(xs, abuf, ln0, tid);
-    fence_async_smem();
-    __syncthreads();
-    if (tid == 0) {
-        fence_after();
-        issue_chunk(0, tmem, a_addr, b_addr, mbar0);
-        issue_chunk(1, tmem, a_addr, b_addr, mbar1);
+    // chunks (a group without a brick skips the loop).
+    float fsc = 1.f;
+    if (first < fg.nbricks) {
+        stage_brick<N>(first, xs, wslab, x, w, fg, rel, pk, tid);
+        cp_async_commit();
+        cp_async_wait_0();
+        group_sync(grp);
+        fsc = build_a(xs, abuf, ln0, tid);
+        fence_async_smem();
+        group_sync(grp);
+        if (tid == 0) {
+            fence_after();
+            issue_chunk<N>(0, tmem, a_addr, b_addr, mbar0);
+            if (K::NCH > 1) issue_chunk<N>(1, tmem, a_addr, b_addr, mbar1);
+        }
     }
 
-    for (int64_t brick = blockIdx.x; brick < fg.nbricks; brick += gridDim.x) {
-        const int64_t next = brick + gridDim.x;
+    for (int64_t brick = first; brick < fg.nbricks; brick += stride) {
+        const int64_t next = brick + stride;
         const bool chk = brick_check_fixed(brick, fg);
 
         int bbx, bby, bbz;
@@ -373,24 +489,24 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
         const int ex0 = bbx * BX, ey0 = bby * BY, ez0 = bbz * BZ;
         const bool valid = ex0 + lx < g.nelx && ey0 + ly < g.nely && ez0 + lz < g.nelz;
 
-        float2 ws2[8], acc[12];
+        // this element's factors, with the two scale factors undone
+        float ws[K::NS];
         {
-            const uint4 wv = *reinterpret_cast<const uint4 *>(smem_raw + TC_OFF_W + 16 * tid);
-            const uint32_t wq[4] = {wv.x, wv.y, wv.z, wv.w};
             const float f = fsc * inv_ke;
 #pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const float w0 = __uint_as_float(wq[q] << 16) * f, w1 = __uint_as_float(wq[q] & 0xFFFF0000u) * f;
-                ws2[2 * q] = make_float2(w0, w0);
-                ws2[2 * q + 1] = make_float2(w1, w1);
+            for (int s = 0; s < K::NS; ++s) {
+                const int sy = s % N, sx = (s / N) % N, sz = s / (N * N);
+                const uint32_t b = wslab[((lz * N + sz) * K::WX + lx * N + sx) * K::WY + ly * N + sy];
+                ws[s] = __uint_as_float(b << 16) * f;
             }
         }
+        float2 acc[12];
 #pragma unroll
         for (int i = 0; i < 12; ++i) acc[i] = make_float2(0.f, 0.f);
 
         bool ok = true;
 #pragma unroll
-        for (int c = 0; c < TC_NCHUNK; ++c) {
+        for (int c = 0; c < K::NCH; ++c) {
             // warp-uniform, so that the collective tensor-memory loads below
             // are executed by all or none of a warp's threads
             const bool got = __all_sync(0xffffffffu, (c & 1) ? mbar_wait(mbar1, ph1) : mbar_wait(mbar0, ph0));
@@ -398,37 +514,36 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
             else ph0 ^= 1u;
             if (got) {
                 fence_after();
-                const uint32_t taddr = tlane + (uint32_t)((c & 1) * TC_CHUNK);
-                if (c == 0) consume_chunk<0>(taddr, ws2, acc);
-                else if (c == 1) consume_chunk<1>(taddr, ws2, acc);
-                else consume_chunk<2>(taddr, ws2, acc);
+                consume_any<N>(c, tlane + (uint32_t)((c & 1) * K::CH), ws, acc,
+                               std::make_integer_sequence<int, K::NCH>{});
             }
             fence_before();
-            if (__syncthreads_or(!got)) {   // buffer (c & 1) fully read
+            if (group_sync_or(grp, !got)) {   // buffer (c & 1) fully read
                 ok = false;
                 break;
             }
             if (c == 0) {
-                // past this barrier every thread has read this brick's factors
-                // and the A tiles were built: the next brick's inputs go into
-                // the same buffers
-                if (next < fg.nbricks) stage_brick(next, xs, smem_raw + TC_OFF_W, x, w, fg, rel, pk, tid);
+                // past this barrier every thread of the group has read this
+                // brick's factors and the A tiles were built: the next brick's
+                // inputs go into the same buffers
+                if (next < fg.nbricks) stage_brick<N>(next, xs, wslab, x, w, fg, rel, pk, tid);
                 cp_async_commit();
-                if (tid == 0) {
-                    fence_after();
-                    issue_chunk(2, tmem, a_addr, b_addr, mbar0);
-                }
+            }
+            if (tid == 0 && c + 2 < K::NCH) {
+                fence_after();
+                issue_chunk<N>(c + 2, tmem, a_addr, b_addr, (c & 1) ? mbar1 : mbar0);
             }
         }
         if (!ok) {
             if (tid == 0) {
-                s_fail = 1;
+                s_fail[grp] = 1;
                 atomicExch(err, 1);
             }
             break;
         }
         // this element's corner outputs (zero outside the mesh); every thread
-        // finished the previous brick's gathers before the first chunk's barrier
+        // of the group finished the previous brick's gathers before the first
+        // chunk's barrier
 #pragma unroll
         for (int a = 0; a < 8; ++a)
             eo4[a * BRICK_ELEMS + tid] = valid ? make_float4(acc_at(acc, 3 * a), acc_at(acc, 3 * a + 1),
@@ -438,16 +553,16 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
         // next brick's inputs and the corner outputs are complete and visible
         // after the barrier.
         cp_async_wait_0();
-        __syncthreads();
+        group_sync(grp);
         if (next < fg.nbricks) {
             fsc = build_a(xs, abuf, ln0, tid);
             fence_async_smem();
         }
-        __syncthreads();
+        group_sync(grp);
         if (tid == 0 && next < fg.nbricks) {
             fence_after();
-            issue_chunk(0, tmem, a_addr, b_addr, mbar0);
-            issue_chunk(1, tmem, a_addr, b_addr, mbar1);
+            issue_chunk<N>(0, tmem, a_addr, b_addr, mbar0);
+            if (K::NCH > 1) issue_chunk<N>(1, tmem, a_addr, b_addr, mbar1);
         }
         brick_gather_write(eo4, y, freemask, g, ex0, ey0, ez0, rel, pk, tid, chk);
     }
@@ -455,21 +570,22 @@ k_fine_apply_tc2(const float *__restrict__ x, float *__restrict__ y, const __nv_
 
     // MMAs still in flight after a timeout get one more bounded wait each
     // before their columns are released.
-    if (s_fail && tid == 0) {
+    if (tid == 0 && s_fail[grp]) {
         mbar_wait(mbar0, ph0);
-        mbar_wait(mbar1, ph1);
+        if (K::NCH > 1) mbar_wait(mbar1, ph1);
     }
     fence_before();
     __syncthreads();
     fence_after();
-    if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TC_COLS) : "memory");
+    if (ttid < 32)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(s_tmem), "r"(K::TMEM_COLS)
+                     : "memory");
 }
 
-// B image for MR factor 2: step tiles of the scaled blocks' FP16 hi and mid
-// pieces in the K order of the MMAs above (row n = 24 s + i, entry KE_s[i][j]
-// at k = j, j - 16 + 8 or j - 8 as the step requires), then the block scale
-// record: the float 2^-sc in the first four bytes.
+// B image: step tiles of the scaled blocks' FP16 hi and mid pieces in the K
+// order of the MMAs above (row r = 24 s + i, entry KE_s[i][j] at k = j,
+// j - 16 + 8 or j - 8 as the step requires; rows beyond 24 n^3 zero), then the
+// block scale record: the float 2^-sc in the first four bytes.
 static uint16_t f16_bits(float v) {
     const __half h = __float2half_rn(v);
     uint16_t b;
@@ -482,42 +598,51 @@ static double f16_value(uint16_t b) {
     return (double)__half2float(h);
 }
 
-void fine_tc_image(const std::vector<double> &packed_rowmajor, std::vector<uint16_t> &img) {
+template <int N>
+static void tc_image(const std::vector<double> &packed_rowmajor, std::vector<uint16_t> &img) {
+    using K = Tc<N>;
     auto ke = [&](int s, int i, int j) {
         const int a = i < j ? i : j, b = i < j ? j : i;
         return packed_rowmajor[(size_t)s * KE_PACK + pair_rowmajor(a, b)];
     };
     double kmax = 0.0;
-    for (int s = 0; s < 8; ++s)
+    for (int s = 0; s < K::NS; ++s)
         for (int t = 0; t < KE_PACK; ++t) kmax = fmax(kmax, fabs(packed_rowmajor[(size_t)s * KE_PACK + t]));
     int e = 0;
     frexp(kmax > 0.0 ? kmax : 1.0, &e);
     const int sc = 15 - e;   // kmax 2^sc in [2^14, 2^15)
-    img.assign(TC_IMG_BYTES / 2, 0);
-    auto put = [&](int step, int n, int k, uint16_t b) { img[(step * TC_B_TILE + tc_offset(n, k)) / 2] = b; };
-    for (int n = 0; n < TC_NROWS; ++n) {
-        const int s = n / 24, i = n % 24;
+    img.assign(K::IMG_BYTES / 2, 0);
+    auto put = [&](int step, int r, int k, uint16_t b) { img[(step * K::B_TILE + tc_offset(r, k)) / 2] = b; };
+    for (int r = 0; r < K::NROWS; ++r) {
+        const int s = r / 24, i = r % 24;
         for (int j = 0; j < 24; ++j) {
             const double v = ldexp(ke(s, i, j), sc);
             const uint16_t hi = f16_bits((float)v);
             const uint16_t mid = f16_bits((float)(v - f16_value(hi)));
-            if (j < 16) put(0, n, j, hi);
-            else put(1, n, j - 16, hi);
-            if (j < 8) put(1, n, j + 8, hi);
-            else put(2, n, j - 8, hi);
-            if (j < 16) put(3, n, j, mid);
-            else put(4, n, j - 16, mid);
+            if (j < 16) put(0, r, j, hi);
+            else put(1, r, j - 16, hi);
+            if (j < 8) put(1, r, j + 8, hi);
+            else put(2, r, j - 8, hi);
+            if (j < 16) put(3, r, j, mid);
+            else put(4, r, j - 16, mid);
         }
     }
     const float inv = (float)ldexp(1.0, -sc);
-    memcpy(&img[TC_B_BYTES / 2], &inv, sizeof(float));
+    memcpy(&img[K::B_BYTES / 2], &inv, sizeof(float));
 }
 
-size_t fine_tc_image_bytes() { return TC_IMG_BYTES; }
+bool fine_tc_supported(int n, int nely) { return n >= 1 && n <= 3 && (n * nely) % 2 == 0; }
+
+void fine_tc_image(const std::vector<double> &packed_rowmajor, int n, std::vector<uint16_t> &img) {
+    if (n == 1) tc_image<1>(packed_rowmajor, img);
+    else if (n == 2) tc_image<2>(packed_rowmajor, img);
+    else tc_image<3>(packed_rowmajor, img);
+}
 
 // Resident CTAs per SM from the device limits (shared memory with the
 // per-CTA reservation, registers at warp allocation granularity), capped by
 // the 512 tensor-memory columns.
+template <int N>
 static int tc_ctas_per_sm() {
     int dev = 0, smem_sm = 0, smem_res = 0, regs_sm = 0;
     cudaGetDevice(&dev);
@@ -525,17 +650,17 @@ static int tc_ctas_per_sm() {
     cudaDeviceGetAttribute(&smem_res, cudaDevAttrReservedSharedMemoryPerBlock, dev);
     cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
     cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, k_fine_apply_tc2) != cudaSuccess) {
+    if (cudaFuncGetAttributes(&fa, k_fine_apply_tc<N>) != cudaSuccess) {
         cudaGetLastError();
         return 1;
     }
-    const size_t per_cta = TC_SMEM + fa.sharedSizeBytes + (size_t)smem_res;
+    const size_t per_cta = Tc<N>::SMEM + fa.sharedSizeBytes + (size_t)smem_res;
     const int by_smem = (int)(smem_sm / per_cta);
     const int regs_warp = (fa.numRegs * 32 + 255) / 256 * 256;
-    const int by_regs = regs_sm / (regs_warp * (BRICK_ELEMS / 32));
-    int n = by_smem < by_regs ? by_smem : by_regs;
-    if (n > TC_CTAS_PER_SM) n = TC_CTAS_PER_SM;
-    return n < 1 ? 1 : n;
+    const int by_regs = regs_sm / (regs_warp * (Tc<N>::THREADS / 32));
+    int m = by_smem < by_regs ? by_smem : by_regs;
+    if (m > 512 / Tc<N>::TMEM_COLS) m = 512 / Tc<N>::TMEM_COLS;
+    return m < 1 ? 1 : m;
 }
 
 static int num_sms_tc() {
@@ -548,23 +673,33 @@ static int num_sms_tc() {
     return n;
 }
 
-void launch_fine_apply_tc(const float *x, float *y, const __nv_bfloat16 *w, const uint8_t *fm, const void *bimg,
-                          const FineGeom &fg, int *err, cudaStream_t st) {
+template <int N>
+static void launch_tc(const float *x, float *y, const __nv_bfloat16 *w, const uint8_t *fm, const void *bimg,
+                      const FineGeom &fg, int *err, cudaStream_t st) {
     static int attr_dev = -1, per_sm = 1;
     int dev = 0;
     cudaGetDevice(&dev);
     if (attr_dev != dev) {
-        cudaFuncSetAttribute(k_fine_apply_tc2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
-        cudaFuncSetAttribute(k_fine_apply_tc2, cudaFuncAttributePreferredSharedMemoryCarveout,
+        cudaFuncSetAttribute(k_fine_apply_tc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Tc<N>::SMEM);
+        cudaFuncSetAttribute(k_fine_apply_tc<N>, cudaFuncAttributePreferredSharedMemoryCarveout,
                              (int)cudaSharedmemCarveoutMaxShared);
-        per_sm = tc_ctas_per_sm();
+        per_sm = tc_ctas_per_sm<N>();
         attr_dev = dev;
     }
     int64_t grid = (int64_t)per_sm * num_sms_tc();
-    if (grid > fg.nbricks) grid = fg.nbricks;
+    const int64_t need = (fg.nbricks + Tc<N>::NB - 1) / Tc<N>::NB;   // NB bricks side by side per CTA
+    if (grid > need) grid = need;
     if (grid < 1) grid = 1;
-    k_fine_apply_tc2<<<(unsigned)grid, BRICK_ELEMS, TC_SMEM, st>>>(x, y, w, fm, (const uint4 *)bimg, fg, err);
+    k_fine_apply_tc<N><<<(unsigned)grid, Tc<N>::THREADS, Tc<N>::SMEM, st>>>(x, y, w, fm, (const uint4 *)bimg, fg,
+                                                                          err);
     count_launch();
+}
+
+void launch_fine_apply_tc(const float *x, float *y, const __nv_bfloat16 *w, const uint8_t *fm, const void *bimg,
+                          const FineGeom &fg, int n, int *err, cudaStream_t st) {
+    if (n == 1) launch_tc<1>(x, y, w, fm, bimg, fg, err, st);
+    else if (n == 2) launch_tc<2>(x, y, w, fm, bimg, fg, err, st);
+    else launch_tc<3>(x, y, w, fm, bimg, fg, err, st);
 }
 
 }  // namespace tosp

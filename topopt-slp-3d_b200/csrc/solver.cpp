@@ -58,7 +58,7 @@ struct tosp_handle {
     double *d_kt64 = nullptr;       // pair-major layout of the fine operator
     float *d_kt32 = nullptr;
     std::vector<double> ktab_c;     // MR 2: FP64 Walsh-Hadamard coefficients passed with each launch
-    uint16_t *d_tcimg = nullptr;    // mixed, MR 2: tensor-core B operand image of the blocks
+    uint16_t *d_tcimg = nullptr;    // mixed: tensor-core B operand image of the blocks (null: CUDA-core kernel)
     int *d_tcerr = nullptr;         // set by the tensor-core operator when an MMA wait times out
     // densities
     double *d_rho = nullptr, *d_w64 = nullptr;
@@ -189,7 +189,16 @@ int sync(tosp_handle *h) {
 }
 
 // ----- level rules (I/StartStrSLP.m:107-133) --------------------------------
+// Largest coarsest system of the direct solve: its explicit FP64 inverse
+// (npad^2 doubles, 4.8 GB here) is applied as one GEMV per cycle.
+constexpr int DENSE_MAX = 24576;
+
+// The reference adds grids while the coarsest system exceeds nmaxchol
+// (opchol = 0).  The same rule runs here against min(nmaxchol, DENSE_MAX): a
+// coarsest system between DENSE_MAX and nmaxchol, which the reference would
+// factor with sparse Cholesky, gets one more grid instead.
 int choose_levels(int nelx, int nely, int nelz, int ngrids, int nmaxchol, std::string &msg) {
+    const int cap = nmaxchol < DENSE_MAX ? nmaxchol : DENSE_MAX;
     auto divisible = [&](int k) {
         const int m = 1 << (k - 1);
         return nelx % m == 0 && nely % m == 0 && nelz % m == 0;
@@ -203,11 +212,14 @@ int choose_levels(int nelx, int nely, int nelz, int ngrids, int nmaxchol, std::s
     for (;;) {
         const double m = (double)(1 << (ng - 1));
         const double nc = (nelx / m + 1) * (nely / m + 1) * (nelz / m + 1) * 3;
-        if (nc <= nmaxchol) break;
+        if (nc <= cap) break;
         if (divisible(ng + 1)) ++ng;
         else {
-            msg = "coarsest system larger than nmaxchol and no further level possible "
-                  "(the reference switches to PCG on the coarsest grid, not provided)";
+            msg = nc <= nmaxchol
+                      ? "coarsest system of " + std::to_string((long long)nc) + " dofs exceeds the dense direct "
+                        "solve's " + std::to_string(DENSE_MAX) + " and no further level is possible"
+                      : "coarsest system larger than nmaxchol and no further level possible "
+                        "(the reference switches to PCG on the coarsest grid, not provided)";
             return -1;
         }
     }
@@ -230,7 +242,7 @@ int fine_apply(tosp_handle *h, const T *x, T *y) {
     if constexpr (sizeof(T) == 8) {
         launch_fine64(h, x, y);
     } else if (h->d_tcimg) {
-        launch_fine_apply_tc(x, y, h->d_wbf, h->lev[0].fm, h->d_tcimg, h->fg, h->d_tcerr, h->stream);
+        launch_fine_apply_tc(x, y, h->d_wbf, h->lev[0].fm, h->d_tcimg, h->fg, h->n, h->d_tcerr, h->stream);
     } else {
         launch_fine_apply<float, __nv_bfloat16>(x, y, h->d_wbf, h->lev[0].fm, h->d_kt32, h->fg, h->n, h->stream);
     }
@@ -699,7 +711,7 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
     h->dens = make_grid(pb->nelx * h->n, pb->nely * h->n, pb->nelz * h->n);
     h->ncoarse = h->mg_ok ? h->lev[ng - 1].g.ndof : 0;
     h->npad = (h->ncoarse + 31) / 32 * 32;
-    if (h->npad > 24576) {
+    if (h->npad > DENSE_MAX) {
         h->err = "coarsest system too large for the dense direct solve: " + std::to_string(h->ncoarse) +
                  " dofs; use more grids";
         return TOSP_ERR_UNSUPPORTED;
@@ -728,9 +740,9 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
         CK(cudaMemcpy(h->d_kt64, kt64.data(), sizeof(double) * kt64.size(), cudaMemcpyHostToDevice));
         CK(cudaMemcpy(h->d_kt32, kt32.data(), sizeof(float) * kt32.size(), cudaMemcpyHostToDevice));
     }
-    if (precision == TOSP_PREC_MIXED && h->n == 2) {
+    if (precision == TOSP_PREC_MIXED && fine_tc_supported(h->n, pb->nely)) {
         std::vector<uint16_t> img;
-        fine_tc_image(packed, img);
+        fine_tc_image(packed, h->n, img);
         TRY(dalloc(h, &h->d_tcimg, (int64_t)img.size()));
         CK(cudaMemcpy(h->d_tcimg, img.data(), sizeof(uint16_t) * img.size(), cudaMemcpyHostToDevice));
         TRY(dalloc(h, &h->d_tcerr, 1));
@@ -1378,8 +1390,8 @@ int tosp_time_operator(tosp_handle *h, int32_t precision, int32_t reps, double *
             CK(cudaMemsetAsync(F.t, 0, sizeof(float) * g0.ndof, h->stream));
             CK(cudaEventRecord(a, h->stream));
             if (h->d_tcimg)
-                launch_fine_apply_tc((const float *)F.x, (float *)F.t, h->d_wbf, F.fm, h->d_tcimg, h->fg, h->d_tcerr,
-                                     h->stream);
+                launch_fine_apply_tc((const float *)F.x, (float *)F.t, h->d_wbf, F.fm, h->d_tcimg, h->fg, h->n,
+                                     h->d_tcerr, h->stream);
             else
                 launch_fine_apply<float, __nv_bfloat16>((const float *)F.x, (float *)F.t, h->d_wbf, F.fm, h->d_kt32,
                                                         h->fg, h->n, h->stream);

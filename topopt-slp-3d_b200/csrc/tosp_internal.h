@@ -120,13 +120,14 @@ void fine_block_table(const std::vector<double> &packed_rowmajor, int n, int ele
 void fine_mr2_const_table(const std::vector<double> &kt_padded, int elem_bytes, std::vector<double> &out);
 void launch_fine_apply64_const(const double *x, double *y, const double *w, const uint8_t *freemask,
                                const double *ktab, const FineGeom &fg, cudaStream_t st);
-// Tensor-core finest operator of the mixed V-cycle (MR factor 2): B operand
-// image (FP16 pieces of the scaled blocks, canonical shared-memory layout,
-// then the block scale) and launch.
-void fine_tc_image(const std::vector<double> &packed_rowmajor, std::vector<uint16_t> &img);
-size_t fine_tc_image_bytes();
+// Tensor-core finest operator of the mixed V-cycle (MR factor n = 1, 2, 3):
+// whether the kernel serves the mesh (its factor staging needs n * nely even),
+// the B operand image (FP16 pieces of the scaled blocks, canonical
+// shared-memory layout, then the block scale) and the launch.
+bool fine_tc_supported(int n, int nely);
+void fine_tc_image(const std::vector<double> &packed_rowmajor, int n, std::vector<uint16_t> &img);
 void launch_fine_apply_tc(const float *x, float *y, const __nv_bfloat16 *w, const uint8_t *fm, const void *bimg,
-                          const FineGeom &fg, int *err, cudaStream_t st);
+                          const FineGeom &fg, int n, int *err, cudaStream_t st);
 
 // Sensitivities g0 (I/Grad.m:24-49), zero for elements not in freeDensG.
 void launch_grad(const double *u, const double *rho, const uint8_t *free_elem, const double *kepack,
