@@ -346,16 +346,22 @@ def run_serving(args):
         pb, n, x, ng = item
         # cycle and omega unspecified for the stream: the reference defaults
         mg = tosp.default_mg(ngrids=ng, cycle=1, omega=W.REF_OMEGA, tolMG=1e-8, maxiterMG=1000, flexible=1,
-                             maxstall=60)
+                             maxstall=60, small_cycle_max=args.small_levels)
         return srv.submit(pb, x, mg=mg, precision=tosp.PREC_MIXED, mr_n=n, p=3.0, emin=1e-9, opfilter=1,
                           rmin=1.0 if n > 1 else 1.5)
 
     out = []
     srv = tosp.Server(max_slots=args.slots, hbm_budget_bytes=int(args.budget_gb * (1 << 30)))
     seen = {}
-    for it in items:                                   # warm-up: one request per shape (handles, graphs)
+    for it in items:                                   # warm-up: handles per shape, one request each
         k = (id(it[0]), it[1])
         if k not in seen:
+            pb, n, x, ng = it
+            mg = tosp.default_mg(ngrids=ng, cycle=1, omega=W.REF_OMEGA, tolMG=1e-8, maxiterMG=1000, flexible=1,
+                                 maxstall=60, small_cycle_max=args.small_levels)
+            if args.prepare > 0:
+                srv.prepare(pb, count=args.prepare, mg=mg, precision=tosp.PREC_MIXED, mr_n=n,
+                            rmin=1.0 if n > 1 else 1.5)
             seen[k] = submit(srv, it)
     for rid in seen.values():
         srv.wait(rid)
@@ -390,17 +396,86 @@ def run_serving(args):
                     "all_converged": bool(all(st["relres"] <= 1e-8 for st in stats))})
         print(json.dumps(out[-1]), file=sys.stderr)
     clk = clocks.stop()
+    counters = srv.counters()
     srv.close()
     best = max(out, key=lambda r: r["solves_per_s"])
     line = {"metric": "serving stream: solves/s and p50/p99 latency (mixed MG-PCG to 1e-8 + Grad)",
             "value": best["solves_per_s"], "unit": "solves/s", "n_gpus": 1, "higher_is_better": True,
             "data": "synthetic", "dtype": "f64 outer CG / f32+bf16 V-cycle",
             "config": {"workload": "serving stream seed 7", "requests": len(items), "slots": args.slots,
-                       "hbm_budget_gb": args.budget_gb, "mesh_nx": list(W.SERVING_NX), "mr_n": [1, 2],
+                       "hbm_budget_gb": args.budget_gb, "small_levels": args.small_levels,
+                       "mesh_nx": list(W.SERVING_NX), "mr_n": [1, 2],
                        "cycle": "W", "omega": W.REF_OMEGA,
                        "bc": list(W.SERVING_BC)},
-            "rates": out, "clocks": clk}
+            "rates": out, "clocks": clk, "runner": counters}
     print(json.dumps(line))
+    return 0
+
+
+def run_sweep(args):
+    """Multigrid settings per precision on the benchmark workload: V/W cycle,
+    Jacobi sweeps, omega and grid count, each arm timed over a few solves
+    (setup + solve + Grad, device-resident inputs).  One JSON line with every
+    setting and each precision's fastest."""
+    import ctypes as C
+    import itertools
+    import torch
+    import tosp
+    from tosp.workloads import WORKLOADS, build_workload
+    torch.cuda.set_device(0)
+    spec = WORKLOADS[args.workload]
+    pb, n, xfil, spec = build_workload(args.workload, filter_fn=lambda x: x)
+    dev = torch.device("cuda", 0)
+    xfil_d = torch.tensor(xfil, dtype=torch.float64, device=dev)
+    f_d = torch.tensor(pb.f, dtype=torch.float64, device=dev)
+    u_d = torch.zeros(pb.freedofs.size, dtype=torch.float64, device=dev)
+    ufull_d = torch.zeros(3 * pb.nnodes, dtype=torch.float64, device=dev)
+    g_d = torch.zeros(xfil.size, dtype=torch.float64, device=dev)
+    fidx_d = torch.tensor(pb.freedofs, dtype=torch.int64, device=dev)
+    lib = tosp._lib
+    rows = []
+    grids = [int(v) for v in args.sweep_grids.split(",")]
+    for prec, cycle, (nu1, nu2), omega, ng in itertools.product(
+            (tosp.PREC_MIXED, tosp.PREC_FP64), (0, 1), ((1, 1), (1, 2), (2, 2), (3, 3)), (0.5, 0.6), grids):
+        mg = tosp.default_mg(ngrids=ng, cycle=cycle, omega=omega, smoothiter1=nu1, smoothiter2=nu2, tolMG=1e-8,
+                             maxiterMG=1000, flexible=1)
+        try:
+            s = tosp.Solver(pb, mg, precision=prec, mr_n=n, p=3.0, emin=1e-9, opfilter=1, rmin=spec["rmin"])
+        except tosp.TospError as e:
+            rows.append({"prec": "mixed" if prec else "fp64", "cycle": "VW"[cycle], "sweeps": [nu1, nu2],
+                         "omega": omega, "ngrids": ng, "error": str(e)[:120]})
+            continue
+
+        def step():
+            s.SetupGMG(xfil_d)
+            u_d.zero_()
+            it, rr = C.c_int32(), C.c_double()
+            rc = lib.tosp_solve_mg(s.h, u_d.data_ptr(), f_d.data_ptr(), u_d.numel(), C.byref(it), C.byref(rr))
+            ufull_d.zero_()
+            ufull_d[fidx_d] = u_d
+            lib.tosp_grad(s.h, ufull_d.data_ptr(), ufull_d.numel(), g_d.data_ptr(), None, g_d.numel())
+            return rc, it.value, rr.value
+        rc, it, rr = step()
+        for _ in range(2):
+            step()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.sweep_steps):
+            rc, it, rr = step()
+        e1.record()
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / args.sweep_steps
+        rows.append({"prec": "mixed" if prec else "fp64", "cycle": "VW"[cycle], "sweeps": [nu1, nu2], "omega": omega,
+                     "ngrids": s.info()["ngrids"], "status": rc, "it": it, "relres": rr, "ms": round(ms, 3),
+                     "solves_per_s": round(1000.0 / ms, 3) if rc == 0 else None})
+        print(json.dumps(rows[-1]), file=sys.stderr)
+        s.close()
+    ok = [r for r in rows if r.get("solves_per_s")]
+    best = {p: max((r for r in ok if r["prec"] == p), key=lambda r: r["solves_per_s"]) for p in ("mixed", "fp64")}
+    print(json.dumps({"metric": "multigrid settings sweep (solves/s, setup + solve to 1e-8 + Grad)",
+                      "workload": args.workload, "rows": rows, "best": best,
+                      "best_mixed_over_best_fp64": round(best["mixed"]["solves_per_s"] / best["fp64"]["solves_per_s"], 3)}))
     return 0
 
 
@@ -468,9 +543,17 @@ def main():
     ap.add_argument("--lp", default="", choices=["", "highs", "knapsack"], help="LP solver of the SLP loop")
     ap.add_argument("--serving", action="store_true",
                     help="serving stream (seed 7): Poisson arrivals at --rates, p50/p99 latency and solves/s")
+    ap.add_argument("--sweep", action="store_true",
+                    help="multigrid settings per precision (cycle, sweeps, omega, grids) on the workload")
+    ap.add_argument("--sweep-grids", default="4,5")
+    ap.add_argument("--sweep-steps", type=int, default=3)
     ap.add_argument("--rates", default="10,20,50,100,200,500")
     ap.add_argument("--serving-count", type=int, default=512)
     ap.add_argument("--slots", type=int, default=8)
+    ap.add_argument("--prepare", type=int, default=2, help="serving: idle handles created per shape before the stream")
+    ap.add_argument("--small-levels", type=int, default=0,
+                    help="serving: mg.small_cycle_max of the requests (0: off; k > 0: the levels with at most k "
+                         "nodes run as the persistent cycle, one launch per visit for a whole shape batch)")
     ap.add_argument("--budget-gb", type=float, default=64.0)
     ap.add_argument("--profile-solve", action="store_true",
                     help="with --profile-kernels: also one full mixed-precision solve (launch lists)")
@@ -490,6 +573,8 @@ def main():
         return profile_filter(args)
     if args.serving:
         return run_serving(args)
+    if args.sweep:
+        return run_sweep(args)
     if args.slp:
         return run_slp(args)
 

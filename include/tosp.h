@@ -232,11 +232,20 @@ int tosp_kelem_prod_noalloc(tosp_handle *h, const double *x, double *y, int64_t 
 /* ---- serving loop ------------------------------------------------------
  * A server runs many independent SetupGMG + SolveMG (zero start) + Grad
  * requests on the current device.  No counterpart in the reference (which
- * solves one problem per MATLAB process): requests are admitted in arrival
- * order as soon as one of `max_slots` slots is free and the request's
- * estimated device memory fits `hbm_budget_bytes`; each slot drives a solve
- * handle on its own CUDA stream, so concurrent requests overlap on the GPU;
- * handles are cached per problem shape and reused. */
+ * solves one problem per MATLAB process).  Requests are admitted in arrival
+ * order while fewer than `max_slots` are in flight and the request's device
+ * memory (the measured footprint of its shape once one handle of that shape
+ * exists, an estimate before) fits `hbm_budget_bytes`; handles are cached per
+ * problem shape and reused.  A worker sets an admitted request up (hierarchy,
+ * initial residual, first CG iteration); then the request joins the batch of
+ * in-flight requests of its shape (mesh, MR factor, grids, cycle, precision;
+ * supports and loads may differ), and a runner advances every batch one CG
+ * iteration per tick (each member's iteration is its handle's captured graph
+ * on its own stream, one host synchronisation per tick for the batch).  For
+ * requests with mg.small_cycle_max > 0 each visit to the levels with at most
+ * that many nodes is one persistent launch for all members of the batch (the
+ * member's graph is captured in segments around the visits).  A finished
+ * request leaves its batch at once and a worker computes its Grad. */
 typedef struct tosp_server tosp_server;
 
 #define TOSP_REQ_QUEUED     0
@@ -257,6 +266,11 @@ typedef struct tosp_request_stats {
 } tosp_request_stats;
 
 int tosp_server_create(int32_t max_slots, int64_t hbm_budget_bytes, tosp_server **out);
+/* Create `count` idle handles for the problem's shape ahead of its requests
+ * (within the budget; TOSP_ERR_OOM otherwise), so that the first requests of
+ * a shape do not wait for a handle's creation. */
+int tosp_server_prepare(tosp_server *s, const tosp_problem *prob, const tosp_mg_params *mg, int32_t precision,
+                        int32_t count);
 /* Copies the problem arrays, densities `xfil` (density mesh) and load `f`
  * (free dofs); TOSP_ERR_OOM if the request can never fit the budget. */
 int tosp_server_submit(tosp_server *s, const tosp_problem *prob, const tosp_mg_params *mg, int32_t precision,
@@ -273,6 +287,9 @@ int tosp_server_cancel(tosp_server *s, int64_t request_id);
 /* Forget a finished request and its results. */
 int tosp_server_release(tosp_server *s, int64_t request_id);
 int tosp_server_info(tosp_server *s, int32_t *active, int32_t *queued, int64_t *used_bytes, int64_t *cached_handles);
+/* Runner counters: ticks, member iterations run inside batch graphs, and the
+ * largest batch seen (instrumentation for tests and benchmarks). */
+int tosp_server_counters(tosp_server *s, int64_t *ticks, int64_t *batched_iterations, int64_t *max_batch);
 /* Cancels queued requests, waits for running ones, frees every handle. */
 int tosp_server_destroy(tosp_server *s);
 

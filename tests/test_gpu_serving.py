@@ -92,3 +92,42 @@ def test_admission_by_budget_and_cancel(tosp_mod):
     with pytest.raises(tosp_mod.TospError):      # can never fit
         srv2 = tosp_mod.Server(max_slots=1, hbm_budget_bytes=1 << 20)
         _submit(tosp_mod, srv2, pb, n, x, ng, 1)
+
+
+@pytest.mark.parametrize("small", [0, 65536])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batched_requests_match_standalone_solves(tosp_mod, precision, small):
+    """Requests of one shape in flight together run as one batch, one CG
+    iteration per tick; with mg.small_cycle_max > 0 every visit to the small
+    levels is one persistent launch for all of them.  Supports, loads and
+    densities differ between members; each result equals the standalone solve
+    of its request (same parameters) to the solve tolerance."""
+    pool = W.FieldPool(seed=5)
+    items = []
+    for k, bc in enumerate(("cantilever", "bridge", "torsion", "cantilever", "bridge", "torsion")):
+        pb = W.serving_problem(32, bc)
+        items.append((pb, pool.field(32, 1, k % 3, 0.45 + 0.02 * k)))
+    mg = tosp_mod.default_mg(ngrids=3, cycle=1, omega=0.5, tolMG=1e-8, maxiterMG=1000, flexible=1,
+                             small_cycle_max=small)
+    srv = tosp_mod.Server(max_slots=6, hbm_budget_bytes=8 << 30)
+    srv.prepare(items[0][0], count=6, mg=mg, precision=precision)
+    ids = [srv.submit(pb, x, mg=mg, precision=precision, mr_n=1, p=3.0, emin=1e-9, rmin=1.5) for pb, x in items]
+    res = []
+    for rid in ids:
+        srv.wait(rid)
+        res.append(srv.result(rid))
+    cnt = srv.counters()
+    srv.close()
+    assert cnt["max_batch"] >= 2, cnt
+    for (pb, x), (u, g, st) in zip(items, res):
+        s = tosp_mod.Solver(pb, mg, precision=precision, mr_n=1, p=3.0, emin=1e-9, opfilter=1, rmin=1.5)
+        s.SetupGMG(x)
+        u0, it0, rr0, rc0 = s.SolveMG(np.zeros(pb.f.size), pb.f)
+        uf = np.zeros(3 * pb.nnodes)
+        uf[pb.freedofs] = u0
+        g0 = s.Grad(uf)
+        s.close()
+        assert st["status"] == 0 and rc0 == 0 and st["relres"] <= 1e-8
+        assert abs(pb.f @ u - pb.f @ u0) <= 1e-7 * abs(pb.f @ u0)
+        assert np.linalg.norm(u - u0) <= 1e-5 * np.linalg.norm(u0)
+        assert np.abs(g - g0).max() <= 1e-5 * np.abs(g0).max()

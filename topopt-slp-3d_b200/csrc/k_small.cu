@@ -216,6 +216,53 @@ __device__ void step_dense(const SmallStep<T> &s, int64_t warp, int64_t nwarps, 
     }
 }
 
+// One step over threads tid of nt (a multiple of the warp size).
+template <typename T>
+__device__ __forceinline__ void run_step(const SmallStep<T> &s, int64_t tid, int64_t nt, int lane) {
+    const int64_t warp = tid >> 5, nwarps = nt >> 5;
+    switch (s.kind) {
+    case SS_STENCIL:
+        step_stencil(s, warp, nwarps, lane);
+        break;
+    case SS_RESTRICT:
+        step_restrict(s, tid, nt);
+        break;
+    case SS_PROLONG:
+        step_prolong(s, tid, nt);
+        break;
+    case SS_JACOBI0:
+        for (int64_t i = tid; i < s.g.ndof; i += nt) s.y[i] = __ldg(s.invd + i) * ldc(s.b + i);
+        break;
+    case SS_DENSE:
+        step_dense(s, warp, nwarps, lane);
+        break;
+    default:   // SS_COPY
+        for (int64_t i = tid; i < s.g.ndof; i += nt) s.y[i] = s.x ? ldc(s.x + i) : T(0);
+        break;
+    }
+}
+
+// The small-level cycles of several solves of one shape (the serving loop's
+// batch): member m owns blocks block0 .. block0 + nblocks - 1 and its own
+// step list; step k of every member runs between the same two grid barriers,
+// so one launch per visit serves the whole batch.
+template <typename T>
+__global__ void __launch_bounds__(SMALL_THREADS)
+k_small_cycle_batch(const SmallBatchEntry *__restrict__ ent, int nmem, int maxsteps, GridBarrier *bar) {
+    int m = 0;
+    while (m + 1 < nmem && (int)blockIdx.x >= ent[m + 1].block0) ++m;
+    const SmallBatchEntry me = ent[m];
+    const SmallStep<T> *steps = reinterpret_cast<const SmallStep<T> *>(me.steps);
+    const int64_t tid = (int64_t)(blockIdx.x - me.block0) * blockDim.x + threadIdx.x;
+    const int64_t nt = (int64_t)me.nblocks * blockDim.x;
+    const int lane = threadIdx.x & 31;
+    const uint32_t limit = bar->limit ? bar->limit : SMALL_WAIT_LIMIT;
+    for (int k = 0; k < maxsteps; ++k) {
+        if (k < me.nsteps) run_step(steps[k], tid, nt, lane);
+        if (k + 1 < maxsteps && !grid_barrier(bar, gridDim.x, limit, false)) return;
+    }
+}
+
 template <typename T>
 __global__ void __launch_bounds__(SMALL_THREADS)
 k_small_cycle(const SmallStep<T> *__restrict__ steps, int nsteps, GridBarrier *bar) {
@@ -268,6 +315,21 @@ int small_cycle_max_blocks(bool fp64) {
     return per_sm * sms;
 }
 
+int small_cycle_batch_max_blocks(bool fp64) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const cudaError_t e = fp64 ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_small_cycle_batch<double>,
+                                                                                SMALL_THREADS, 0)
+                               : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_small_cycle_batch<float>,
+                                                                                SMALL_THREADS, 0);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return per_sm * sms;
+}
+
 template <typename T>
 void launch_small_cycle(const SmallStep<T> *steps_dev, int nsteps, GridBarrier *bar, int blocks, cudaStream_t st) {
     cudaLaunchConfig_t cfg = {};
@@ -285,5 +347,24 @@ void launch_small_cycle(const SmallStep<T> *steps_dev, int nsteps, GridBarrier *
 }
 template void launch_small_cycle<double>(const SmallStep<double> *, int, GridBarrier *, int, cudaStream_t);
 template void launch_small_cycle<float>(const SmallStep<float> *, int, GridBarrier *, int, cudaStream_t);
+
+template <typename T>
+void launch_small_cycle_batch(const SmallBatchEntry *ent_dev, int nmem, int maxsteps, GridBarrier *bar, int blocks,
+                              cudaStream_t st) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)blocks);
+    cfg.blockDim = dim3(SMALL_THREADS);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    cudaLaunchKernelEx(&cfg, k_small_cycle_batch<T>, ent_dev, nmem, maxsteps, bar);
+    count_launch();
+}
+template void launch_small_cycle_batch<double>(const SmallBatchEntry *, int, int, GridBarrier *, int, cudaStream_t);
+template void launch_small_cycle_batch<float>(const SmallBatchEntry *, int, int, GridBarrier *, int, cudaStream_t);
 
 }  // namespace tosp

@@ -105,6 +105,18 @@ struct tosp_handle {
     double *d_ufull = nullptr, *d_g0 = nullptr, *d_gf = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     tosp_solve_stats stats{};
+    SolveState st{};                // loop state of the current solve
+    // one CG iteration (it >= 2) per parity as graph segments split at the
+    // visits to the persistent small-level cycle (serving-loop batches run
+    // those visits batched across requests); seg_capture is set while the
+    // segments are captured
+    static constexpr int MAXSEG = 64;
+    cudaGraphExec_t seg_graph[2][MAXSEG] = {};
+    int nseg[2] = {0, 0};
+    int seg_variant[MAXSEG] = {};   // small-cycle variant of visit i (the same for both parities)
+    bool seg_failed = false, seg_capture = false;
+    int seg_count = 0;
+    std::vector<cudaGraph_t> seg_pending;
     int64_t bytes = 0;
     std::vector<void *> allocs;
 };
@@ -462,8 +474,22 @@ int build_small(tosp_handle *h) {
     return TOSP_OK;
 }
 
+// While an iteration is captured as segments, a visit to the small levels
+// closes the current segment (its graph is kept) and opens the next; the
+// visit itself is left to the caller of the segments.
+int segment_break(tosp_handle *h, int variant) {
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamEndCapture(h->stream, &g));
+    h->seg_pending.push_back(g);
+    if (h->seg_count < tosp_handle::MAXSEG) h->seg_variant[h->seg_count] = variant;
+    h->seg_count++;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    return TOSP_OK;
+}
+
 template <typename T>
 int small_cycle(tosp_handle *h, int variant) {
+    if (h->seg_capture) return segment_break(h, variant);
     const SmallStep<T> *steps = reinterpret_cast<const SmallStep<T> *>(h->d_steps) + (size_t)variant * SMALL_MAX_STEPS;
     launch_small_cycle<T>(steps, h->small_n[variant], h->d_bar, h->small_blocks, h->stream);
     CKL();
@@ -1015,9 +1041,10 @@ void capture_iteration(tosp_handle *h, int parity) {
     if (g) cudaGraphDestroy(g);
 }
 
-int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
+// r = f - K x and the norms of I/SolveMG.m:27-29; from a zero start (K 0 = 0
+// exactly) r = f without the product.  Starts the loop state.
+int solve_init(tosp_handle *h) {
     const int64_t nd = h->lev[0].g.ndof;
-    // r = f - K x; from a zero start (K 0 = 0 exactly) r = f without the product
     launch_dot(h->cx, h->cx, nd, h->d_partials, h->d_scal + 3, h->stream);
     CKL();
     TRY(read_scalars(h));
@@ -1032,60 +1059,89 @@ int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
     launch_dot(h->cr, h->cr, nd, h->d_partials, h->d_scal + 3, h->stream);
     CKL();
     TRY(read_scalars(h));
-    const double nf = std::sqrt(h->h_scal[4]);
-    double nr = std::sqrt(h->h_scal[3]) / nf;
-    int it = 1;
-    int rc = TOSP_OK;
-    double best = nr;
-    int best_it = 1;
-    while (nr > h->mg.tolMG && it <= h->mg.maxiterMG) {
-        if (it == 1) {
-            TRY(cg_iteration(h, 1, it));
-        } else {
-            const int par = it & 1;
-            if (!h->iter_graph[par] && !h->graph_failed) capture_iteration(h, par);
-            if (h->iter_graph[par]) {
-                CK(cudaGraphLaunch(h->iter_graph[par], h->stream));
-            } else {
-                TRY(cg_iteration(h, h->mg.flexible ? 2 : 0, it));
-            }
-        }
-        TRY(sync(h));
-        const double rho = h->h_scal[0], dq = h->h_scal[2], rr = h->h_scal[3];
-        // r'M^{-1}r may turn negative when the smoother is not convergent for
-        // the chosen omega (the V-cycle is then indefinite); the reference
-        // PCG carries on in that case, so only d'Kd <= 0 and non-finite
-        // values stop the iteration.
-        if (!(dq > 0.0) || !std::isfinite(rho) || !std::isfinite(rr)) {
-            h->err = "CG breakdown: r'M^{-1}r = " + std::to_string(rho) + ", d'q = " + std::to_string(dq) +
-                     ", r'r = " + std::to_string(rr);
-            rc = TOSP_ERR_BREAKDOWN;
-            break;
-        }
-        nr = std::sqrt(rr) / nf;
-        ++it;
-        if (nr <= 0.5 * best) {
-            best = nr;
-            best_it = it;
-        }
-        if (h->mg.maxstall > 0 && nr > h->mg.tolMG && it - best_it >= h->mg.maxstall) {
-            h->err = "CG stalled: relative residual not halved in " + std::to_string(h->mg.maxstall) + " iterations";
-            rc = TOSP_NOT_CONVERGED;
-            break;
-        }
+    SolveState &S = h->st;
+    S.nf = std::sqrt(h->h_scal[4]);
+    S.nr = std::sqrt(h->h_scal[3]) / S.nf;
+    S.it = 1;
+    S.rc = TOSP_OK;
+    S.best = S.nr;
+    S.best_it = 1;
+    S.done = !(S.nr > h->mg.tolMG && S.it <= h->mg.maxiterMG);
+    return TOSP_OK;
+}
+
+// Queue iteration S.it of I/SolveMG.m:30-52 on the handle's stream (the
+// first one launched kernel by kernel, the others as the captured graph of
+// their parity).
+int solve_launch_iteration(tosp_handle *h) {
+    const int it = h->st.it;
+    if (it == 1) return cg_iteration(h, 1, it);
+    const int par = it & 1;
+    if (!h->iter_graph[par] && !h->graph_failed) capture_iteration(h, par);
+    if (h->iter_graph[par]) {
+        CK(cudaGraphLaunch(h->iter_graph[par], h->stream));
+        return TOSP_OK;
     }
-    // the last iteration's x += alpha d (the others ride on the direction update)
-    if (it > 1) {
-        launch_pcg_finish(h->cx, h->cd, h->d_scal, nd, h->stream);
+    return cg_iteration(h, h->mg.flexible ? 2 : 0, it);
+}
+
+// Loop bookkeeping after an iteration whose scalars reached h_scal: the
+// breakdown test, the relative residual, the iteration counter, the stall
+// test and the loop condition of I/SolveMG.m:30.
+void solve_account(tosp_handle *h) {
+    SolveState &S = h->st;
+    const double rho = h->h_scal[0], dq = h->h_scal[2], rr = h->h_scal[3];
+    // r'M^{-1}r may turn negative when the smoother is not convergent for
+    // the chosen omega (the V-cycle is then indefinite); the reference
+    // PCG carries on in that case, so only d'Kd <= 0 and non-finite
+    // values stop the iteration.
+    if (!(dq > 0.0) || !std::isfinite(rho) || !std::isfinite(rr)) {
+        h->err = "CG breakdown: r'M^{-1}r = " + std::to_string(rho) + ", d'q = " + std::to_string(dq) +
+                 ", r'r = " + std::to_string(rr);
+        S.rc = TOSP_ERR_BREAKDOWN;
+        S.done = true;
+        return;
+    }
+    S.nr = std::sqrt(rr) / S.nf;
+    ++S.it;
+    if (S.nr <= 0.5 * S.best) {
+        S.best = S.nr;
+        S.best_it = S.it;
+    }
+    if (h->mg.maxstall > 0 && S.nr > h->mg.tolMG && S.it - S.best_it >= h->mg.maxstall) {
+        h->err = "CG stalled: relative residual not halved in " + std::to_string(h->mg.maxstall) + " iterations";
+        S.rc = TOSP_NOT_CONVERGED;
+        S.done = true;
+        return;
+    }
+    S.done = !(S.nr > h->mg.tolMG && S.it <= h->mg.maxiterMG);
+}
+
+// The last iteration's x += alpha d (the others ride on the direction
+// update), the final status and the statistics.
+int solve_finish(tosp_handle *h, int32_t *it_out, double *relres_out) {
+    SolveState &S = h->st;
+    if (S.it > 1) {
+        launch_pcg_finish(h->cx, h->cd, h->d_scal, h->lev[0].g.ndof, h->stream);
         CKL();
     }
-    if (rc == TOSP_OK && nr > h->mg.tolMG && it > h->mg.maxiterMG) rc = TOSP_NOT_CONVERGED;
-    if (it_out) *it_out = it;
-    if (relres_out) *relres_out = nr;
-    h->stats.it = it;
-    h->stats.relres = nr;
+    if (S.rc == TOSP_OK && S.nr > h->mg.tolMG && S.it > h->mg.maxiterMG) S.rc = TOSP_NOT_CONVERGED;
+    if (it_out) *it_out = S.it;
+    if (relres_out) *relres_out = S.nr;
+    h->stats.it = S.it;
+    h->stats.relres = S.nr;
     TRY(check_tc(h));
-    return rc;
+    return S.rc;
+}
+
+int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
+    TRY(solve_init(h));
+    while (!h->st.done) {
+        TRY(solve_launch_iteration(h));
+        TRY(sync(h));
+        solve_account(h);
+    }
+    return solve_finish(h, it_out, relres_out);
 }
 
 }  // namespace
@@ -1112,8 +1168,208 @@ int tosp::kelem_prod_with_scratch(tosp_handle *h, const double *x, double *y, in
     return sync(h);
 }
 
+// ----- serving-loop batches ----------------------------------------------------
+#define CK_E(call, err)                                                  \
+    do {                                                                 \
+        cudaError_t e_ = (call);                                         \
+        if (e_ != cudaSuccess) {                                         \
+            err = std::string("CUDA error: ") + cudaGetErrorString(e_); \
+            return TOSP_ERR_CUDA;                                        \
+        }                                                                \
+    } while (0)
+
+int tosp::solve_start(tosp_handle *h, const double *x, const double *f) {
+    TRY(need_mg(h));
+    TRY(need_setup(h));
+    TRY(free_to_full(h, x, h->cx, "x"));
+    TRY(free_to_full(h, f, h->cf, "f"));
+    TRY(solve_init(h));
+    if (!h->st.done) {
+        TRY(solve_launch_iteration(h));
+        TRY(sync(h));
+        solve_account(h);
+    }
+    return TOSP_OK;
+}
+
+void tosp::solve_step_account(tosp_handle *h) { solve_account(h); }
+
+int tosp::solve_step(tosp_handle *h) {
+    TRY(solve_launch_iteration(h));
+    TRY(sync(h));
+    solve_account(h);
+    return TOSP_OK;
+}
+
+const SolveState &tosp::solve_state(const tosp_handle *h) { return h->st; }
+
+int tosp::solve_stop(tosp_handle *h, double *x, int32_t *it, double *relres) {
+    const int rc = solve_finish(h, it, relres);
+    if (rc < 0) return rc;
+    TRY(full_to_free(h, h->cx, x, "x"));
+    TRY(sync(h));
+    return rc;
+}
+
+std::string tosp::batch_key(const tosp_handle *h) {
+    std::string k;
+    auto add = [&](const void *p, size_t n) { k.append(static_cast<const char *>(p), n); };
+    add(&h->fg.g.nelx, sizeof(int) * 3);
+    add(&h->n, sizeof(int));
+    add(&h->precision, sizeof(int));
+    add(&h->ngrids, sizeof(int));
+    add(&h->small_l, sizeof(int));
+    add(&h->small_n[0], sizeof(int) * 3);
+    add(&h->mg.cycle, sizeof(int32_t));
+    add(&h->mg.smoothiter1, sizeof(int32_t) * 2);
+    add(&h->mg.flexible, sizeof(int32_t));
+    return k;
+}
+
+int tosp::batch_prepare(BatchPlan &plan, cudaStream_t st, std::string &err) {
+    const int nmem = (int)plan.mem.size();
+    if (nmem < 1) {
+        err = "empty batch";
+        return TOSP_ERR_BAD_ARG;
+    }
+    tosp_handle *h0 = plan.mem[0];
+    plan.fp64 = h0->precision == TOSP_PREC_FP64;
+    for (int v = 0; v < 3; ++v) plan.maxsteps[v] = h0->small_l >= 0 ? h0->small_n[v] : 0;
+    if (h0->small_l < 0) {
+        plan.blocks = 0;   // no small levels: members' launches only
+        return TOSP_OK;
+    }
+    for (tosp_handle *h : plan.mem)
+        if (batch_key(h) != batch_key(h0)) {
+            err = "batch members of different shapes";
+            return TOSP_ERR_BAD_ARG;
+        }
+    // at most one block per SM: the launch then leaves room for the other
+    // batches' kernels (a cooperative launch waits until all its blocks fit)
+    int sms = 0;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, h0->device);
+    const int maxb = std::min(small_cycle_batch_max_blocks(plan.fp64), std::max(sms, 1));
+    if (maxb < nmem) {
+        err = "too many batch members for one cooperative launch";
+        return TOSP_ERR_UNSUPPORTED;
+    }
+    // each member keeps its own launch size, scaled down to what is co-resident
+    std::vector<int> nb(nmem);
+    int64_t total = 0;
+    for (int m = 0; m < nmem; ++m) total += nb[m] = std::max(1, plan.mem[m]->small_blocks);
+    if (total > maxb) {
+        const int64_t want = total;
+        total = 0;
+        for (int m = 0; m < nmem; ++m) total += nb[m] = (int)std::max<int64_t>(1, (int64_t)nb[m] * maxb / want);
+    }
+    while (total > maxb) {
+        for (int m = 0; m < nmem && total > maxb; ++m)
+            if (nb[m] > 1) --nb[m], --total;
+    }
+    std::vector<SmallBatchEntry> ent((size_t)3 * nmem);
+    const size_t step_bytes = plan.fp64 ? sizeof(SmallStep<double>) : sizeof(SmallStep<float>);
+    for (int v = 0; v < 3; ++v) {
+        int b0 = 0;
+        for (int m = 0; m < nmem; ++m) {
+            SmallBatchEntry &e = ent[(size_t)v * nmem + m];
+            e.steps = static_cast<const unsigned char *>(plan.mem[m]->d_steps) + step_bytes * (size_t)v * SMALL_MAX_STEPS;
+            e.nsteps = plan.mem[m]->small_n[v];
+            e.block0 = b0;
+            e.nblocks = nb[m];
+            e.pad = 0;
+            b0 += nb[m];
+        }
+    }
+    plan.blocks = (int)total;
+    cudaError_t e = cudaMemcpyAsync(plan.d_ent, ent.data(), sizeof(SmallBatchEntry) * ent.size(),
+                                    cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaMemsetAsync(plan.d_bar, 0, sizeof(GridBarrier), st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+        err = std::string("batch tables: ") + cudaGetErrorString(e);
+        return TOSP_ERR_CUDA;
+    }
+    return TOSP_OK;
+}
+
+// Capture the generic iteration of one parity as segments (once per handle:
+// the buffers never move).
+int capture_segments(tosp_handle *h, int parity) {
+    h->seg_pending.clear();
+    h->seg_count = 0;
+    h->seg_capture = true;
+    cudaError_t e = cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal);
+    int rc = e == cudaSuccess ? cg_iteration(h, h->mg.flexible ? 2 : 0, parity) : TOSP_ERR_CUDA;
+    cudaGraph_t last = nullptr;
+    const cudaError_t e2 = cudaStreamEndCapture(h->stream, &last);
+    h->seg_capture = false;
+    if (last) h->seg_pending.push_back(last);
+    bool ok = rc == TOSP_OK && e == cudaSuccess && e2 == cudaSuccess && last &&
+              (int)h->seg_pending.size() <= tosp_handle::MAXSEG;
+    for (size_t i = 0; i < h->seg_pending.size(); ++i) {
+        if (ok && cudaGraphInstantiate(&h->seg_graph[parity][i], h->seg_pending[i], 0) != cudaSuccess) ok = false;
+        if (h->seg_pending[i]) cudaGraphDestroy(h->seg_pending[i]);
+    }
+    const int nseg = (int)h->seg_pending.size();
+    h->seg_pending.clear();
+    if (!ok) {
+        cudaGetLastError();
+        for (auto &g : h->seg_graph[parity])
+            if (g) {
+                cudaGraphExecDestroy(g);
+                g = nullptr;
+            }
+        h->seg_failed = true;
+        h->err = "iteration segments could not be captured";
+        return TOSP_ERR_CUDA;
+    }
+    h->nseg[parity] = nseg;
+    return TOSP_OK;
+}
+
+int tosp::batch_tick(const BatchPlan &plan, cudaStream_t main, cudaEvent_t *ev_mem, cudaEvent_t ev_small,
+                     std::string &err) {
+    const int nmem = (int)plan.mem.size();
+    int nseg = -1;
+    for (tosp_handle *h : plan.mem) {
+        const int par = h->st.it & 1;
+        if (!h->seg_graph[par][0] && !h->seg_failed) capture_segments(h, par);
+        if (h->seg_failed) {
+            err = h->err;
+            return TOSP_ERR_CUDA;
+        }
+        if (nseg < 0) nseg = h->nseg[par];
+        if (h->nseg[par] != nseg) {
+            err = "batch members with different iteration structures";
+            return TOSP_ERR_STATE;
+        }
+    }
+    tosp_handle *h0 = plan.mem[0];
+    for (int i = 0; i < nseg; ++i) {
+        for (tosp_handle *h : plan.mem) CK_E(cudaGraphLaunch(h->seg_graph[h->st.it & 1][i], h->stream), err);
+        if (i + 1 == nseg) break;
+        // visit i of every member: one batched persistent launch
+        for (int m = 0; m < nmem; ++m) {
+            CK_E(cudaEventRecord(ev_mem[m], plan.mem[m]->stream), err);
+            CK_E(cudaStreamWaitEvent(main, ev_mem[m], 0), err);
+        }
+        const int v = h0->seg_variant[i];
+        if (plan.fp64)
+            launch_small_cycle_batch<double>(plan.d_ent + (size_t)v * nmem, nmem, plan.maxsteps[v], plan.d_bar,
+                                             plan.blocks, main);
+        else
+            launch_small_cycle_batch<float>(plan.d_ent + (size_t)v * nmem, nmem, plan.maxsteps[v], plan.d_bar,
+                                            plan.blocks, main);
+        CK_E(cudaGetLastError(), err);
+        CK_E(cudaEventRecord(ev_small, main), err);
+        for (tosp_handle *h : plan.mem) CK_E(cudaStreamWaitEvent(h->stream, ev_small, 0), err);
+    }
+    return TOSP_OK;
+}
+
 int64_t tosp::handle_ndof(const tosp_handle *h) { return h->fg.g.ndof; }
 int tosp::handle_device(const tosp_handle *h) { return h->device; }
+cudaStream_t tosp::handle_stream(const tosp_handle *h) { return h->stream; }
 void tosp::set_handle_error(tosp_handle *h, const std::string &msg) { h->err = msg; }
 
 // =============================================================================
@@ -1166,6 +1422,9 @@ int tosp_destroy(tosp_handle *h) {
     if (h->stream) cudaStreamSynchronize(h->stream);
     for (cudaGraphExec_t gx : h->iter_graph)
         if (gx) cudaGraphExecDestroy(gx);
+    for (auto &row : h->seg_graph)
+        for (cudaGraphExec_t gx : row)
+            if (gx) cudaGraphExecDestroy(gx);
     for (void *p : h->allocs) cudaFree(p);
     if (h->h_scal) cudaFreeHost(h->h_scal);
     if (h->ev0) cudaEventDestroy(h->ev0);

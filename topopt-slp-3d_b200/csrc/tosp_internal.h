@@ -219,8 +219,18 @@ struct GridBarrier {
     int skip;         // k > 0: block k - 1 skips its first arrival (fault injection for tests)
     int pad;
 };
+// One member of a batched small-level cycle: its step list (SmallStep of the
+// cycle precision), and the blocks of the launch that run it.
+struct SmallBatchEntry {
+    const void *steps;
+    int32_t nsteps, block0, nblocks, pad;
+};
+template <typename T>
+void launch_small_cycle_batch(const SmallBatchEntry *ent_dev, int nmem, int maxsteps, GridBarrier *bar, int blocks,
+                              cudaStream_t st);
 // Largest grid of 256-thread blocks that can be co-resident (cooperative launch).
 int small_cycle_max_blocks(bool fp64);
+int small_cycle_batch_max_blocks(bool fp64);
 template <typename T>
 void launch_small_cycle(const SmallStep<T> *steps_dev, int nsteps, GridBarrier *bar, int blocks, cudaStream_t st);
 
@@ -255,11 +265,48 @@ void launch_pcg_update(double *r, const double *q, double *scal, double *partial
                        float *b0 = nullptr, const float *invd0 = nullptr, float *x0 = nullptr);
 void launch_set_scalar(double *dst, const double *src, cudaStream_t st);
 
+// Loop state of an MG-preconditioned CG solve (I/SolveMG.m:26-53).
+struct SolveState {
+    int it = 0;             // the reference's `it` (iterations + 1)
+    double nr = 0, nf = 0;  // relative residual, ||f||
+    double best = 0;        // the stall test's best residual and its iteration
+    int best_it = 0;
+    int rc = 0;             // TOSP_OK, TOSP_NOT_CONVERGED or TOSP_ERR_BREAKDOWN
+    bool done = false;      // the loop condition no longer holds
+};
+
+// Serving-loop batches (solver.cpp): a solve's steps, and one CG iteration of
+// several handles of one shape captured as a single graph.
+int solve_start(tosp_handle *h, const double *x, const double *f);   // loads, r, norms, first iteration
+void solve_step_account(tosp_handle *h);                              // after a batch iteration's sync
+int solve_step(tosp_handle *h);                                       // one iteration on the handle's stream
+const SolveState &solve_state(const tosp_handle *h);
+int solve_stop(tosp_handle *h, double *x, int32_t *it, double *relres);  // final update, x to the host
+// Batch key: handles with equal keys can share a batch graph (same grids,
+// cycle and precision; supports and loads may differ).
+std::string batch_key(const tosp_handle *h);
+// A batch of handles of one shape (batch_key) stepping together: each
+// member's iteration runs as its captured segments on its own stream, and
+// every visit to the small levels between two segments is one persistent
+// launch over all members (tables and barrier from batch_prepare).
+struct BatchPlan {
+    std::vector<tosp_handle *> mem;
+    SmallBatchEntry *d_ent = nullptr;   // 3 variants x nmem entries (device)
+    GridBarrier *d_bar = nullptr;
+    int blocks = 0, maxsteps[3] = {0, 0, 0};
+    bool fp64 = false;
+};
+int batch_prepare(BatchPlan &plan, cudaStream_t st, std::string &err);   // fills d_ent (allocated by the caller)
+// Queue one CG iteration of every member (each at its own iteration number);
+// ev_mem: one event per member; the caller synchronises the members' streams.
+int batch_tick(const BatchPlan &plan, cudaStream_t main, cudaEvent_t *ev_mem, cudaEvent_t ev_small, std::string &err);
+
 // Handle internals used by entry points that live outside solver.cpp.
 int kelem_prod_with_scratch(tosp_handle *h, const double *x, double *y, int64_t nfree, double *xfull,
                             double *yfull);
 int64_t handle_ndof(const tosp_handle *h);
 int handle_device(const tosp_handle *h);
+cudaStream_t handle_stream(const tosp_handle *h);
 void set_handle_error(tosp_handle *h, const std::string &msg);
 
 }  // namespace tosp

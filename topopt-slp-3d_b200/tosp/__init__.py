@@ -95,6 +95,7 @@ def _load():
         "tosp_inject_wait_fault": (C.c_int, [C.c_void_p, C.c_int32, C.c_int32]),
         "tosp_small_cycle_blocks": (C.c_int, [C.c_void_p, P(C.c_int32)]),
         "tosp_server_create": (C.c_int, [C.c_int32, C.c_int64, P(C.c_void_p)]),
+        "tosp_server_prepare": (C.c_int, [C.c_void_p, P(_Problem), P(MgParams), C.c_int32, C.c_int32]),
         "tosp_server_submit": (C.c_int, [C.c_void_p, P(_Problem), P(MgParams), C.c_int32, d, C.c_int64, d, C.c_int64,
                                          P(C.c_int64)]),
         "tosp_server_poll": (C.c_int, [C.c_void_p, C.c_int64, P(C.c_int32)]),
@@ -104,6 +105,7 @@ def _load():
         "tosp_server_release": (C.c_int, [C.c_void_p, C.c_int64]),
         "tosp_server_info": (C.c_int, [C.c_void_p, P(C.c_int32), P(C.c_int32), P(C.c_int64), P(C.c_int64)]),
         "tosp_server_destroy": (C.c_int, [C.c_void_p]),
+        "tosp_server_counters": (C.c_int, [C.c_void_p, P(C.c_int64), P(C.c_int64), P(C.c_int64)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -444,6 +446,15 @@ class Server:
         self.meta[rid.value] = (f.size, xfil.size)
         return rid.value
 
+    def prepare(self, pb, count=1, mg=None, precision=PREC_MIXED, mr_n=1, p=3.0, emin=1e-9, opfilter=1, rmin=1.5):
+        """Create `count` idle handles for the problem's shape ahead of its
+        requests."""
+        mg = mg if mg is not None else default_mg()
+        prob, keep = _problem_struct(pb, mr_n, p, emin, opfilter, rmin)
+        rc = _lib.tosp_server_prepare(self.h, C.byref(prob), C.byref(mg), precision, count)
+        if rc != TOSP_OK:
+            raise TospError(rc, "tosp_server_prepare")
+
     def state(self, rid):
         st = C.c_int32()
         rc = _lib.tosp_server_poll(self.h, rid, C.byref(st))
@@ -477,6 +488,11 @@ class Server:
         a, q, b, c = C.c_int32(), C.c_int32(), C.c_int64(), C.c_int64()
         _lib.tosp_server_info(self.h, C.byref(a), C.byref(q), C.byref(b), C.byref(c))
         return {"active": a.value, "queued": q.value, "used_bytes": b.value, "cached_handles": c.value}
+
+    def counters(self):
+        t, b, m = C.c_int64(), C.c_int64(), C.c_int64()
+        _lib.tosp_server_counters(self.h, C.byref(t), C.byref(b), C.byref(m))
+        return {"ticks": t.value, "batched_iterations": b.value, "max_batch": m.value}
 
     def close(self):
         if getattr(self, "h", None):
