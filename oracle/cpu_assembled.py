@@ -4,7 +4,8 @@
 Restates ``I/GlobalStiffMatrix.m:16-65`` (K on the free dofs),
 ``I/SetupGMG.m:16-77`` (A{l+1} = P'A{l}P, M{l} = diag(A{l})/omega, Cholesky
 of the coarsest matrix), ``I/SolveMG.m:26-53`` (PCG, the reference's beta),
-``I/VCycle.m:23-43`` / ``I/Smooth.m:14-17`` (V-cycle, damped Jacobi),
+``I/VCycle.m:23-43`` / ``I/WCycle.m:23-44`` / ``I/Smooth.m:14-17`` (V- and
+W-cycles, damped Jacobi),
 ``I/Grad.m:18-62`` (sensitivities, transposed filter) and
 ``I/ApplyFilter.m:74-81`` on top of the C/OpenMP kernels of
 ``assembled_omp.c`` and ``kelem_omp.c``.  The sparse matrices are stored as
@@ -52,8 +53,10 @@ def _p(a):
 
 
 class CpuAssembled:
-    def __init__(self, pb, n, ngrids, omega, nu1=1, nu2=1, p=3.0, emin=1e-9, rmin=1.5, opfilter=1, nthreads=0):
+    def __init__(self, pb, n, ngrids, omega, nu1=1, nu2=1, p=3.0, emin=1e-9, rmin=1.5, opfilter=1, nthreads=0,
+                 cycle=0):
         self.pb, self.n, self.ng, self.omega, self.nu1, self.nu2 = pb, n, ngrids, omega, nu1, nu2
+        self.cycle = cycle   # 0 VCycle (I/VCycle.m), 1 WCycle (I/WCycle.m)
         self.p, self.emin, self.nt, self.opfilter = p, emin, nthreads, opfilter
         self.dims = [(pb.nelx >> l, pb.nely >> l, pb.nelz >> l) for l in range(ngrids)]
         self.ndof = [3 * (a + 1) * (b + 1) * (c + 1) for a, b, c in self.dims]
@@ -113,15 +116,21 @@ class CpuAssembled:
         lib().stencil_apply(nx, ny, nz, _p(self.st[l]), _p(x), _p(b), _p(self.minv[l]), _p(y), mode, self.nt)
         return y
 
-    def vcycle(self, l, b):
-        """VCycle (I/VCycle.m:23-43) from a zero iterate."""
+    def vcycle(self, l, b, x0=None):
+        """VCycle (I/VCycle.m:23-43) or, with cycle = 1, WCycle
+        (I/WCycle.m:23-44: two recursive calls, the second warm-started); from
+        a zero iterate unless x0 is given."""
         L, W = lib(), cpu_wok.lib()
-        x = np.empty(self.ndof[l])
-        if self.nu1 >= 1:
-            L.vec_mul(x.size, _p(self.minv[l]), _p(b), _p(x), self.nt)
+        if x0 is None:
+            x = np.empty(self.ndof[l])
+            if self.nu1 >= 1:
+                L.vec_mul(x.size, _p(self.minv[l]), _p(b), _p(x), self.nt)
+            else:
+                x[:] = 0.0
+            first = 1
         else:
-            x[:] = 0.0
-        for _ in range(1, self.nu1):
+            x, first = x0, 0
+        for _ in range(first, self.nu1):
             x = self.apply(l, x, b, 2)
         r = self.apply(l, x, b, 1)
         cx, cy, cz = self.dims[l + 1]
@@ -131,6 +140,8 @@ class CpuAssembled:
             eH = sla.cho_solve(self.chol, rH)
         else:
             eH = self.vcycle(l + 1, rH)
+            if self.cycle == 1:
+                eH = self.vcycle(l + 1, rH, eH)
         W.prolong_full(cx, cy, cz, _p(np.ascontiguousarray(eH)), _p(x), _p(self.fm[l]), 1, self.nt)
         for _ in range(self.nu2):
             x = self.apply(l, x, b, 2)

@@ -82,3 +82,20 @@ def test_assembled_port_matches_oracle(case):
     assert np.abs(g - go).max() <= 1e-12 * np.abs(go).max()
     xr = np.random.default_rng(4).uniform(0, 1, dens.size)
     assert np.abs(ca.filter(xr) - filt.apply_filter(xr, W, w, 1, False)).max() <= 1e-14
+
+
+def test_assembled_port_w_cycle_matches_oracle(case):
+    """The C/OpenMP assembled path's WCycle (I/WCycle.m) against the SciPy
+    oracle's: one preconditioner application and a full solve."""
+    from oracle.cpu_assembled import CpuAssembled
+    pb, n, dens, ks, K, H, cw = case
+    ca = CpuAssembled(pb, n, 3, 0.6, rmin=1.0, nthreads=4, cycle=1)
+    ca.setup(dens)
+    x = np.random.default_rng(5).standard_normal(pb.freedofs.size)
+    xf = np.zeros(3 * pb.nnodes)
+    xf[pb.freedofs] = x
+    s = gmg.precondition(H, x, 1, 1, 1)
+    assert np.abs(ca.vcycle(0, xf)[pb.freedofs] - s).max() <= 1e-11 * np.abs(s).max()
+    uo, ito = gmg.solve_mg(H, np.zeros(pb.f.size), pb.f, 1, 1, 1, 1e-8, 500)
+    u, it, nr = ca.solve(np.zeros(3 * pb.nnodes), pb.f_full(), 1e-8, 500)
+    assert it == ito and abs(pb.f_full() @ u - pb.f @ uo) <= 1e-10 * abs(pb.f @ uo)

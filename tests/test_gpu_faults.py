@@ -145,3 +145,35 @@ def test_bounded_wait_runs_out_and_the_handle_recovers(tosp_mod, prec):
 
 def rel_err(a, b):
     return np.abs(a - b).max() / np.abs(b).max()
+
+
+def test_metrics_lines_and_nvtx_ranges(tmp_path):
+    """With TOSP_METRICS set, every solve and every served request appends one
+    JSON line (iterations, residual, times, status); the entry points' NVTX
+    ranges cost nothing without a profiler.  Run in a child process, since the
+    library reads the variable once."""
+    import json
+    import os
+    import subprocess
+    import sys
+    log = tmp_path / "metrics.jsonl"
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = (
+        "import sys; sys.path[:0] = [%r, %r]\n"
+        "import numpy as np, tosp\n"
+        "from tosp import problems as P\n"
+        "pb = P.cantilever(16, 8, 8)\n"
+        "s = tosp.Solver(pb, tosp.default_mg(ngrids=3, cycle=0, omega=0.6), mr_n=1)\n"
+        "s.SetupGMG(np.full(pb.nelem, 0.5)); s.SolveMG(np.zeros(pb.f.size), pb.f)\n"
+        "srv = tosp.Server(max_slots=2, hbm_budget_bytes=1 << 30)\n"
+        "rid = srv.submit(pb, np.full(pb.nelem, 0.5), mg=tosp.default_mg(ngrids=3, cycle=0, omega=0.6))\n"
+        "srv.wait(rid); srv.result(rid); srv.close()\n") % (root, os.path.join(root, "topopt-slp-3d_b200"))
+    env = dict(os.environ, TOSP_METRICS=str(log))
+    subprocess.run([sys.executable, "-c", code], check=True, env=env, timeout=300)
+    lines = [json.loads(l) for l in log.read_text().splitlines()]
+    events = [l["event"] for l in lines]
+    assert "solve" in events and "request" in events
+    solve = lines[events.index("solve")]
+    assert solve["status"] == 0 and solve["relres"] <= 1e-8 and solve["it"] > 1
+    req = lines[events.index("request")]
+    assert req["status"] == 0 and req["mesh"] == [16, 8, 8] and req["ms_latency"] >= req["ms_run"]

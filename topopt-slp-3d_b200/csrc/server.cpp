@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "tosp_internal.h"
+#include "trace.h"
 
 namespace {
 
@@ -229,6 +230,7 @@ void batch_main(tosp_server *s, Batch *b);
 
 // Setup and the first CG iteration of an admitted request (worker thread).
 void start_request(tosp_server *s, const std::shared_ptr<Request> &r) {
+    tosp::TraceRange trace_("serving request start");
     r->t_start = Clock::now();
     tosp_handle *h = r->h;
     int rc = tosp_setup_gmg(h, r->xfil.data(), (int64_t)r->xfil.size());
@@ -258,6 +260,7 @@ void start_request(tosp_server *s, const std::shared_ptr<Request> &r) {
 
 // Final update, u to the host, Grad, statistics (worker thread).
 void finish_request(tosp_server *s, Request &r) {
+    tosp::TraceRange trace_("serving request finish");
     tosp_handle *h = r.h;
     int32_t it = 0;
     double rr = 0;
@@ -286,6 +289,16 @@ void finish_request(tosp_server *s, Request &r) {
     r.st.ms_latency = std::chrono::duration<double, std::milli>(t1 - r.t_submit).count();
     r.st.ms_queue = r.st.ms_latency - r.st.ms_run;
     r.st.precision = r.precision;
+    if (tosp::metrics_on()) {
+        char buf[320];
+        std::snprintf(buf, sizeof buf,
+                      "{\"event\": \"request\", \"id\": %lld, \"mesh\": [%d, %d, %d], \"mr_n\": %d, "
+                      "\"precision\": %d, \"it\": %d, \"relres\": %.6e, \"ms_latency\": %.3f, "
+                      "\"ms_queue\": %.3f, \"ms_run\": %.3f, \"status\": %d}",
+                      (long long)r.id, r.pb.nelx, r.pb.nely, r.pb.nelz, r.pb.mr_n, r.precision, it, rr,
+                      r.st.ms_latency, r.st.ms_queue, r.st.ms_run, rc);
+        tosp::metrics_line(buf);
+    }
     (void)s;
 }
 
@@ -416,6 +429,7 @@ void batch_main(tosp_server *s, Batch *b) {
             b->join_q.clear();
         }
         if (b->dirty) batch_rebuild(*b);
+        tosp::TraceRange trace_("serving batch tick");
         if (!b->unbatched) {
             std::string err;
             if (tosp::batch_tick(b->plan, b->stream, b->ev_mem.data(), b->ev_small, err) != TOSP_OK) {

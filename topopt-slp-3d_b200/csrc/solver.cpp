@@ -11,6 +11,7 @@
 
 #include "ptr_kind.h"
 #include "tosp_internal.h"
+#include "trace.h"
 
 using namespace tosp;
 
@@ -1397,6 +1398,7 @@ void tosp_default_mg_params(tosp_mg_params *mg) {
 }
 
 int tosp_create(const tosp_problem *prob, const tosp_mg_params *mg, int32_t precision, tosp_handle **out) {
+    TraceRange trace_("tosp_create");
     if (!out) {
         g_create_error = "null output handle pointer";
         return TOSP_ERR_BAD_ARG;
@@ -1451,6 +1453,7 @@ int tosp_set_freedofs(tosp_handle *h, const int64_t *freedofs, int64_t nfree) {
 }
 
 int tosp_setup_gmg(tosp_handle *h, const double *xfil, int64_t ndens) {
+    TraceRange trace_("SetupGMG");
     if (!h || !xfil) return TOSP_ERR_BAD_ARG;
     cudaSetDevice(h->device);
     TRY(check_len(h, ndens, h->dens.nelem, "densities"));
@@ -1473,6 +1476,7 @@ int tosp_setup_gmg(tosp_handle *h, const double *xfil, int64_t ndens) {
 }
 
 int tosp_kelem_prod(tosp_handle *h, const double *x, double *y, int64_t nfree) {
+    TraceRange trace_("KelemProd");
     if (!h || !x || !y) return TOSP_ERR_BAD_ARG;
     cudaSetDevice(h->device);
     TRY(check_len(h, nfree, h->nfree, "x"));
@@ -1484,6 +1488,7 @@ int tosp_kelem_prod(tosp_handle *h, const double *x, double *y, int64_t nfree) {
 }
 
 int tosp_kelem_prod_mixed(tosp_handle *h, const double *x, double *y, int64_t nfree) {
+    TraceRange trace_("KelemProdMixed");
     if (!h || !x || !y) return TOSP_ERR_BAD_ARG;
     cudaSetDevice(h->device);
     if (h->precision != TOSP_PREC_MIXED) {
@@ -1506,6 +1511,7 @@ int tosp_kelem_prod_mixed(tosp_handle *h, const double *x, double *y, int64_t nf
 }
 
 int tosp_mg_cycle(tosp_handle *h, const double *r, double *s, int64_t nfree) {
+    TraceRange trace_("MGCycle");
     if (!h || !r || !s) return TOSP_ERR_BAD_ARG;
     cudaSetDevice(h->device);
     TRY(check_len(h, nfree, h->nfree, "r"));
@@ -1519,6 +1525,7 @@ int tosp_mg_cycle(tosp_handle *h, const double *r, double *s, int64_t nfree) {
 }
 
 int tosp_solve_mg(tosp_handle *h, double *x, const double *f, int64_t nfree, int32_t *it, double *relres) {
+    TraceRange trace_("SolveMG");
     if (!h || !x || !f) return TOSP_ERR_BAD_ARG;
     cudaSetDevice(h->device);
     TRY(check_len(h, nfree, h->nfree, "x/f"));
@@ -1535,10 +1542,19 @@ int tosp_solve_mg(tosp_handle *h, double *x, const double *f, int64_t nfree, int
     float ms = 0;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     h->stats.ms_solve = ms;
+    if (metrics_on()) {
+        char buf[256];
+        std::snprintf(buf, sizeof buf,
+                      "{\"event\": \"solve\", \"ndof\": %lld, \"precision\": %d, \"it\": %d, \"relres\": %.6e, "
+                      "\"ms\": %.3f, \"status\": %d}",
+                      (long long)h->fg.g.ndof, h->precision, h->st.it, h->st.nr, ms, rc);
+        metrics_line(buf);
+    }
     return rc;
 }
 
 int tosp_apply_filter(tosp_handle *h, const double *x, double *y, int64_t ndens, int32_t trans) {
+    TraceRange trace_("ApplyFilter");
     if (!h || !x || !y) return TOSP_ERR_BAD_ARG;
     cudaSetDevice(h->device);
     TRY(check_len(h, ndens, h->dens.nelem, "x"));
@@ -1575,6 +1591,7 @@ int tosp_filter_weights(tosp_handle *h, double *w, int64_t ndens) {
 }
 
 int tosp_grad(tosp_handle *h, const double *u, int64_t nfull, double *fgrad, double *fgrad0, int64_t ndens) {
+    TraceRange trace_("Grad");
     if (!h || !u || !fgrad) return TOSP_ERR_BAD_ARG;
     cudaSetDevice(h->device);
     TRY(check_len(h, nfull, h->lev[0].g.ndof, "u"));
