@@ -57,6 +57,12 @@ WORKLOADS = {
     "cantilever96x48x48_mr2": dict(dims=(96, 48, 48), n=2, density="uniform_filtered", ngrids=4, rmin=1.0,
                                    omega=REF_OMEGA),
     "cantilever48x24x24": dict(dims=(48, 24, 24), n=1, density="const0.3", ngrids=3, rmin=1.5, omega=0.6),
+    # smaller cases of the same kernels (profiler captures)
+    "cantilever128x64x64_mr2": dict(dims=(128, 64, 64), n=2, density="grf", ngrids=4, rmin=1.0, omega=REF_OMEGA),
+    "cantilever128x64x64": dict(dims=(128, 64, 64), n=1, density="grf", ngrids=4, rmin=1.5, omega=REF_OMEGA),
+    # the 160 x 40 x 80 bridge of the MR-3 SLP loop (reference axes: height 80)
+    "bridge160x80x40_mr3": dict(dims=(160, 80, 40), n=3, density="grf", ngrids=4, rmin=2.5 / 3, omega=REF_OMEGA,
+                                problem="bridge"),
 }
 
 
@@ -66,7 +72,7 @@ def build_workload(name, filter_fn=None):
     spec = WORKLOADS[name]
     nelx, nely, nelz = spec["dims"]
     n = spec["n"]
-    pb = problems.cantilever(nelx, nely, nelz)
+    pb = getattr(problems, spec.get("problem", "cantilever"))(nelx, nely, nelz)
     nd = pb.nelem * n ** 3
     if spec["density"] == "grf":
         xfil = grf_heaviside(nelx * n, nely * n, nelz * n, seed=1)
