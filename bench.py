@@ -446,15 +446,20 @@ def run_sweep(args):
     lib = tosp._lib
     rows = []
     grids = [int(v) for v in args.sweep_grids.split(",")]
-    for prec, cycle, (nu1, nu2), omega, ng in itertools.product(
-            (tosp.PREC_MIXED, tosp.PREC_FP64), (0, 1), ((1, 1), (1, 2), (2, 2), (3, 3)), (0.5, 0.6), grids):
+    # arms: (name, precision, cg_product, replace_drop)
+    arms = [("mixed_cg64", tosp.PREC_MIXED, 0, 0.1), ("fp64", tosp.PREC_FP64, 0, 0.1)]
+    arms += [("mixed_cg32", tosp.PREC_MIXED, 1, float(d)) for d in args.sweep_drops.split(",")]
+    for (arm, prec, cgp, drop), cycle, (nu1, nu2), omega, ng in itertools.product(
+            arms, (0, 1), ((1, 1), (1, 2), (2, 2), (3, 3)), (0.5, 0.6), grids):
         mg = tosp.default_mg(ngrids=ng, cycle=cycle, omega=omega, smoothiter1=nu1, smoothiter2=nu2, tolMG=1e-8,
-                             maxiterMG=1000, flexible=1)
+                             maxiterMG=1000, flexible=1, cg_product=cgp, replace_drop=drop)
+        tag = {"prec": arm, "cycle": "VW"[cycle], "sweeps": [nu1, nu2], "omega": omega}
+        if cgp:
+            tag["replace_drop"] = drop
         try:
             s = tosp.Solver(pb, mg, precision=prec, mr_n=n, p=3.0, emin=1e-9, opfilter=1, rmin=spec["rmin"])
         except tosp.TospError as e:
-            rows.append({"prec": "mixed" if prec else "fp64", "cycle": "VW"[cycle], "sweeps": [nu1, nu2],
-                         "omega": omega, "ngrids": ng, "error": str(e)[:120]})
+            rows.append(dict(tag, ngrids=ng, error=str(e)[:120]))
             continue
 
         def step():
@@ -477,16 +482,18 @@ def run_sweep(args):
         e1.record()
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1) / args.sweep_steps
-        rows.append({"prec": "mixed" if prec else "fp64", "cycle": "VW"[cycle], "sweeps": [nu1, nu2], "omega": omega,
-                     "ngrids": s.info()["ngrids"], "status": rc, "it": it, "relres": rr, "ms": round(ms, 3),
-                     "solves_per_s": round(1000.0 / ms, 3) if rc == 0 else None})
+        rows.append(dict(tag, ngrids=s.info()["ngrids"], status=rc, it=it, relres=rr, ms=round(ms, 3),
+                         solves_per_s=round(1000.0 / ms, 3) if rc == 0 else None,
+                         replacements=s.stats()["replacements"]))
         print(json.dumps(rows[-1]), file=sys.stderr)
         s.close()
     ok = [r for r in rows if r.get("solves_per_s")]
-    best = {p: max((r for r in ok if r["prec"] == p), key=lambda r: r["solves_per_s"]) for p in ("mixed", "fp64")}
+    best = {p: max((r for r in ok if r["prec"] == p), key=lambda r: r["solves_per_s"])
+            for p in ("mixed_cg64", "mixed_cg32", "fp64")}
     print(json.dumps({"metric": "multigrid settings sweep (solves/s, setup + solve to 1e-8 + Grad)",
                       "workload": args.workload, "rows": rows, "best": best,
-                      "best_mixed_over_best_fp64": round(best["mixed"]["solves_per_s"] / best["fp64"]["solves_per_s"], 3)}))
+                      "best_over_best_fp64": {p: round(best[p]["solves_per_s"] / best["fp64"]["solves_per_s"], 3)
+                                              for p in ("mixed_cg64", "mixed_cg32")}}))
     return 0
 
 
@@ -546,6 +553,9 @@ def main():
     ap.add_argument("--no-w-cycle", action="store_true", help="skip the secondary W-cycle measurement")
     ap.add_argument("--ngrids", type=int, default=0, help="override the workload's grid count")
     ap.add_argument("--flexible", type=int, default=1, help="flexible (Polak-Ribiere) CG beta in both arms")
+    ap.add_argument("--cg-product", type=int, default=1, choices=[0, 1],
+                    help="mg.cg_product of the headline mixed arm (the other value is timed beside it): 0 FP64 "
+                         "product every CG iteration, 1 tensor-core product with FP64 residual replacement")
     ap.add_argument("--slp", default="", choices=["", "config0", "config3"],
                     help="full SLP loop: config0 = 48x24x24 cantilever, FP64, 20 iterations; config3 = 160x80x40 "
                          "bridge (reference axes), MR 3, mixed precision, 100 iterations + GradProj")
@@ -557,6 +567,7 @@ def main():
     ap.add_argument("--sweep", action="store_true",
                     help="multigrid settings per precision (cycle, sweeps, omega, grids) on the workload")
     ap.add_argument("--sweep-grids", default="4,5")
+    ap.add_argument("--sweep-drops", default="0.1", help="sweep: replace_drop values of the cg_product 1 arm")
     ap.add_argument("--sweep-steps", type=int, default=3)
     ap.add_argument("--rates", default="10,20,50,100,200,500")
     ap.add_argument("--serving-count", type=int, default=512)
@@ -624,7 +635,13 @@ def main():
     holder["s64"] = tosp.Solver(pb0, mg, precision=tosp.PREC_FP64, **kw)
     pb, n, xfil, spec = build_workload(args.workload, filter_fn=gpu_filter)
     s64 = holder["s64"]
-    smx = tosp.Solver(pb, mg, precision=tosp.PREC_MIXED, **kw)
+    mg_cg = {}
+    for cgp in (0, 1):
+        mg_cg[cgp] = tosp.MgParams.from_buffer_copy(mg)
+        mg_cg[cgp].cg_product = cgp
+    arm_name = {0: "mixed_cg64", 1: "mixed_cg32"}
+    smx = tosp.Solver(pb, mg_cg[args.cg_product], precision=tosp.PREC_MIXED, **kw)
+    smx_alt = tosp.Solver(pb, mg_cg[1 - args.cg_product], precision=tosp.PREC_MIXED, **kw)
     dev = torch.device("cuda", local)
     xfil_d = torch.tensor(xfil, dtype=torch.float64, device=dev)
     f_d = torch.tensor(pb.f, dtype=torch.float64, device=dev)
@@ -675,13 +692,18 @@ def main():
     fp64_steps = args.fp64_steps or args.steps
     per_64, its_64, _ = timed(s64, fp64_steps, args.warmup)
     total64 = max_over_ranks(sum(per_64))
-    # solutions of both arms (outside the timed regions) for the true residuals
-    # and the mixed-vs-FP64 errors
+    # the other mixed arm (cg_product), same steps
+    per_alt, its_alt, _ = timed(smx_alt, args.steps, args.warmup)
+    total_alt = max_over_ranks(sum(per_alt))
+    # solutions of every arm (outside the timed regions) for the true residuals
+    # and the errors against FP64
     sol = {}
-    for key, s in (("mixed", smx), ("fp64", s64)):
+    replacements = {}
+    for key, s in ((arm_name[args.cg_product], smx), (arm_name[1 - args.cg_product], smx_alt), ("fp64", s64)):
         step_dev(s)
         g_full = g_d.cpu().numpy().copy()
         sol[key] = (u_d.cpu().numpy().copy(), g_full)
+        replacements[key] = s.stats()["replacements"]
     stats_mx = smx.stats()
 
     # ---- end to end through the C ABI with pinned host buffers ------------------
@@ -725,24 +747,34 @@ def main():
 
     # ---- kernel roofline (finest-level operators) ---------------------------------
     peaks, peak_kind = load_peaks()
+    s_cg32 = smx if args.cg_product == 1 else smx_alt
     ms_op32 = smx.time_operator(tosp.PREC_MIXED, reps=10)
     ms_op64 = smx.time_operator(tosp.PREC_FP64, reps=10)
+    ms_opcg = s_cg32.time_operator(2, reps=10)
     ndof, nsub, nel = 3 * pb.nnodes, xfil.size, pb.nelem
     bytes32 = 4 * ndof + 4 * ndof + 2 * nsub + ndof      # x, y fp32, SIMP bf16, free mask
+    bytescg = 4 * ndof + 4 * ndof + 4 * nsub + ndof      # x, y fp32, SIMP fp32, free mask
     bytes64 = 8 * ndof + 8 * ndof + 8 * nsub + ndof
     flops = nel * n ** 3 * 1200                           # 576 FMA + 24 scalings per sub-block
     it_mx = its_mx[-1][0]
     applies32 = 2 * (it_mx - 1)                           # residual + post-smooth per V-cycle
-    applies64 = it_mx                                     # initial residual + one per iteration
+    if args.cg_product == 1:
+        appliescg = it_mx - 1                             # the CG's product, every iteration
+        applies64 = stats_mx["replacements"]              # residual replacements
+    else:
+        appliescg = 0
+        applies64 = it_mx - 1                             # the CG's product, every iteration
     traffic = {}
     tp = os.path.join(ROOT, "profiles", "operator_traffic.json")
     if os.path.exists(tp):
         traffic = json.load(open(tp)).get(args.workload, {})
     ach32 = bytes32 / (ms_op32 * 1e-3) / 1e9
+    achcg = bytescg / (ms_opcg * 1e-3) / 1e9
     ach64 = bytes64 / (ms_op64 * 1e-3) / 1e9
     ach64_tf = flops / (ms_op64 * 1e-3) / 1e12
     fma_exec = nel * (2148 if n == 2 else 300 * (n ** 3 + 2))      # FMAs the FP64 kernel executes per launch
     share32 = applies32 * ms_op32 / (total_ms / args.steps)
+    sharecg = appliescg * ms_opcg / (total_ms / args.steps)
     share64 = applies64 * ms_op64 / (total_ms / args.steps)
     rf64 = {"bound": "hbm", "achieved": round(ach64, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": round(ach64 / peaks["hbm_gbs"], 4), "traffic": traffic.get("fp64_operator_bytes_per_launch"),
@@ -756,11 +788,18 @@ def main():
             "kernel": f"k_fine_apply_tc<{n}> (V-cycle operator, tcgen05 sub-cell block products)"
                       if (n * pb.nely) % 2 == 0 else "k_fine_apply<float,bf16> (V-cycle operator)",
             "algorithmic_bytes_per_launch": bytes32, "ms_per_launch": round(ms_op32, 4), "peak_source": peak_kind}
+    rfcg = {"bound": "hbm", "achieved": round(achcg, 1), "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": round(achcg / peaks["hbm_gbs"], 4), "traffic": traffic.get("cg32_operator_bytes_per_launch"),
+            "kernel": f"k_fine_apply_tc<{n},float> (CG product of cg_product 1, FP32 factors)",
+            "algorithmic_bytes_per_launch": bytescg, "ms_per_launch": round(ms_opcg, 4), "peak_source": peak_kind}
     # the dominant kernel of the timed step carries the contract's roofline
-    roofline, roofline_other = (rf64, rf32) if share64 >= share32 else (rf32, rf64)
+    ranked = sorted([(share64, rf64), (share32, rf32), (sharecg, rfcg)], key=lambda t: -t[0])
+    roofline, roofline_other = ranked[0][1], [r for _, r in ranked[1:]]
     kernels = {
         "fine_op_fp32": {"ms": round(ms_op32, 4), "GBps": round(ach32, 1), "per_solve": applies32,
                          "share_of_step": round(share32, 3)},
+        "fine_op_cg32": {"ms": round(ms_opcg, 4), "GBps": round(achcg, 1), "per_solve": appliescg,
+                         "share_of_step": round(sharecg, 3)},
         "fine_op_fp64": {"ms": round(ms_op64, 4), "TFLOPs_fp64_dense_formula": round(ach64_tf, 2),
                          "GBps": round(ach64, 1), "per_solve": applies64, "share_of_step": round(share64, 3)},
     }
@@ -774,12 +813,20 @@ def main():
         "data": "synthetic",
         "config": bench_config(args, spec0, pb, n, ngrids, world),
         "latency_ms": {"p50": round(float(np.percentile(lat, 50)), 3), "p99": round(float(np.percentile(lat, 99)), 3)},
-        "pcg_iterations": {"mixed": it_mx, "fp64": its_64[-1][0]},
-        "relres": {"mixed": its_mx[-1][1], "fp64": its_64[-1][1]},
+        "mixed_arm": arm_name[args.cg_product],
+        "pcg_iterations": {arm_name[args.cg_product]: it_mx, arm_name[1 - args.cg_product]: its_alt[-1][0],
+                           "fp64": its_64[-1][0]},
+        "relres": {arm_name[args.cg_product]: its_mx[-1][1], arm_name[1 - args.cg_product]: its_alt[-1][1],
+                   "fp64": its_64[-1][1]},
         "relres_true": relres_true,
-        "cg": "flexible beta r'(s - s_old)/rho_old in both arms" if args.flexible else "reference beta",
+        "residual_replacements": replacements,
+        "cg": "flexible beta r'(s - s_old)/rho_old in every arm" if args.flexible else "reference beta",
         "fp64": {"value": round(world * fp64_steps / (total64 * 1e-3), 4), "unit": "solves/s",
                  "ms_per_step": round(total64 / fp64_steps, 3), "steps": fp64_steps},
+        arm_name[1 - args.cg_product]: {
+            "value": round(world * args.steps / (total_alt * 1e-3), 4), "unit": "solves/s",
+            "ms_per_step": round(total_alt / args.steps, 3), "steps": args.steps,
+            "over_fp64": round((args.steps / total_alt) / (fp64_steps / total64), 3)},
         "mixed_over_fp64": round((args.steps / total_ms) / (fp64_steps / total64), 3),
         "setup_ms": round(stats_mx["ms_setup"], 3),
         "e2e": {"value": round(world * e2e_steps / e2e_s, 4), "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
@@ -793,10 +840,12 @@ def main():
     if not args.no_w_cycle:
         # the reference's default cycle (W, I/TopOpt3D.m:172-174) on the same
         # workload, both arms, as a secondary figure
-        mgw = tosp.MgParams.from_buffer_copy(mg)
+        mgw = tosp.MgParams.from_buffer_copy(mg_cg[args.cg_product])
         mgw.cycle = 1
+        mgw64 = tosp.MgParams.from_buffer_copy(mgw)
+        mgw64.cg_product = 0
         smw = tosp.Solver(pb, mgw, precision=tosp.PREC_MIXED, **kw)
-        s6w = tosp.Solver(pb, mgw, precision=tosp.PREC_FP64, **kw)
+        s6w = tosp.Solver(pb, mgw64, precision=tosp.PREC_FP64, **kw)
         per_w, its_w, _ = timed(smw, 3, 3)
         per_w64, its_w64, _ = timed(s6w, 3, 3)
         tw, tw64 = max_over_ranks(sum(per_w)), max_over_ranks(sum(per_w64))
@@ -835,6 +884,7 @@ def main():
     if rank == 0:
         print(json.dumps(line))
     smx.close()
+    smx_alt.close()
     s64.close()
     if world > 1:
         dist.destroy_process_group()

@@ -98,14 +98,27 @@ typedef struct tosp_mg_params {
                               (one launch per visit instead of one per sweep and transfer).
                               Measured slower than the graph-replayed launches on a B200, so
                               off by default.  A tuning knob with no reference counterpart.   */
+    int32_t cg_product;    /* product K d of the CG recurrence (I/SolveMG.m:37-38):
+                              0: FP64 operator every iteration (default, the reference's PCG);
+                              1 (TOSP_PREC_MIXED with the tensor-core operator, n * nely even):
+                              the tensor-core operator with FP32 SIMP factors (about 22
+                              significant bits), every CG vector, dot and update still FP64;
+                              the recurrence residual is replaced by the FP64 residual
+                              f - K u (FP64 operator) whenever its norm has fallen by the
+                              factor replace_drop since the last replacement, and before
+                              convergence is accepted, so the tolerance holds for the true
+                              residual.  Ignored by the serving loop.                          */
+    double  replace_drop;  /* replacement factor of cg_product 1, in (0, 1); 0: 0.1            */
 } tosp_mg_params;
 
 /* Statistics of the last tosp_solve_mg call. */
 typedef struct tosp_solve_stats {
     int32_t it;            /* the reference's `it` (iterations + 1)                   */
-    double  relres;        /* final ||f - K u|| / ||f|| as tracked by CG              */
+    double  relres;        /* final ||f - K u|| / ||f|| as tracked by CG (cg_product 1:
+                              computed with the FP64 operator)                        */
     double  ms_setup;      /* device time of the last setup (tosp_setup_gmg)          */
     double  ms_solve;      /* device time of the last solve                           */
+    int32_t replacements;  /* cg_product 1: residual replacements (FP64 products)     */
 } tosp_solve_stats;
 
 /* Library version string. */
@@ -150,11 +163,19 @@ int tosp_setup_gmg(tosp_handle *h, const double *xfil, int64_t ndens);
 int tosp_kelem_prod(tosp_handle *h, const double *x, double *y, int64_t nfree);
 
 /* y = K(rho) x evaluated by the finest-level operator of the mixed V-cycle
- * (FP32 vectors, BF16 SIMP factors; for MR factor 2 the element matrices are
- * formed on the tensor cores).  No counterpart in the reference: it exposes
- * the preconditioner's operator for inspection and tests.  TOSP_PREC_MIXED
- * handles only (TOSP_ERR_STATE otherwise); x and y are FP64 on the free dofs. */
+ * (FP32 vectors, BF16 SIMP factors; sub-cell block products on the tensor
+ * cores when n * nely is even, CUDA cores otherwise).  No counterpart in the
+ * reference: it exposes the preconditioner's operator for inspection and
+ * tests.  TOSP_PREC_MIXED handles only (TOSP_ERR_STATE otherwise); x and y are
+ * FP64 on the free dofs. */
 int tosp_kelem_prod_mixed(tosp_handle *h, const double *x, double *y, int64_t nfree);
+
+/* y = K(rho) x by the product of the CG recurrence of mg.cg_product 1: the
+ * tensor-core operator with FP32 SIMP factors and FP32 vectors.  No
+ * counterpart in the reference (inspection and tests); handles created with
+ * cg_product 1 only (TOSP_ERR_STATE otherwise); x and y are FP64 on the free
+ * dofs. */
+int tosp_kelem_prod_cg32(tosp_handle *h, const double *x, double *y, int64_t nfree);
 
 /* One preconditioner application s = cycle(r) (VCycle/WCycle/FMVCycle,
  * I/VCycle.m:1, I/WCycle.m:1, I/FMVCycle.m:1) on free-dof vectors. */
@@ -196,7 +217,9 @@ int64_t tosp_kernel_launches(void);
  * stream with CUDA events bracketing each launch (inputs are the handle's
  * current vectors): `precision` TOSP_PREC_FP64 times the FP64 kernel of the
  * outer CG, TOSP_PREC_MIXED the FP32/BF16 kernel of the V-cycle (mixed
- * handles only).  Writes the mean device time per launch in ms. */
+ * handles only), 2 the tensor-core kernel with FP32 factors of the CG's
+ * product (cg_product 1 handles only).  Writes the mean device time per launch
+ * in ms. */
 int tosp_time_operator(tosp_handle *h, int32_t precision, int32_t reps, double *ms_per_launch);
 
 /* Fault injection for tests of the bounded device waits (no counterpart in

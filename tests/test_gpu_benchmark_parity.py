@@ -7,11 +7,12 @@
 * 96x48x48 MR 2 (FP64 drop-in workload): GPU FP64 against the oracle's C/OpenMP
   restatement of the assembled path on the same densities: `it` within one,
   u and dF/drho to 1e-8 relative, F to 1e-9, true residual <= 1e-8.
-* 192x96x96 MR 2 (mixed-precision workload, 5.4 M dofs): the mixed and the
-  FP64 GPU solves against the CPU oracle's FP64 solve: true residuals
-  ||f - K u||/||f|| of both GPU solutions with the oracle's operator
-  <= 1e-8 (to rounding of the residual itself), and the errors of u, F and
-  dF/drho against the oracle <= 1e-6 relative (printed).
+* 192x96x96 MR 2 (mixed-precision workload, 5.4 M dofs): the mixed solves
+  (FP64 CG product every iteration, and the tensor-core CG product with
+  residual replacement) and the FP64 GPU solve against the CPU oracle's FP64
+  solve: true residuals ||f - K u||/||f|| of the GPU solutions with the
+  oracle's operator <= 1e-8 (to rounding of the residual itself), and the
+  errors of u, F and dF/drho against the oracle <= 1e-6 relative (printed).
 * 48x24x24 SLP loop (20 iterations, knapsack LP, GradProj at the end): GPU
   FP64 against the same loop on the oracle: identical accept/reject sequence,
   compliance history within 1e-9, identical thresholded designs.
@@ -51,9 +52,9 @@ def full(pb, u):
     return out
 
 
-def gpu_solver(tosp, pb, n, prec, ngrids, omega, rmin, flexible=0, maxiter=1000):
+def gpu_solver(tosp, pb, n, prec, ngrids, omega, rmin, flexible=0, maxiter=1000, cg_product=0):
     mg = tosp.default_mg(ngrids=ngrids, cycle=0, omega=omega, smoothiter1=1, smoothiter2=1, tolMG=1e-8,
-                         maxiterMG=maxiter, flexible=flexible)
+                         maxiterMG=maxiter, flexible=flexible, cg_product=cg_product)
     return tosp.Solver(pb, mg, precision=prec, mr_n=n, p=P_SIMP, emin=EMIN, opfilter=1, rmin=rmin)
 
 
@@ -120,8 +121,9 @@ def test_config2_mixed_and_fp64_against_oracle(tosp_mod):
     pb, n, xfil, spec = build_workload("cantilever192x96x96_mr2")
     ngrids, omega, rmin = spec["ngrids"], spec["omega"], spec["rmin"]
     res = {}
-    for key, prec in (("mixed", tosp_mod.PREC_MIXED), ("fp64", tosp_mod.PREC_FP64)):
-        s = gpu_solver(tosp_mod, pb, n, prec, ngrids, omega, rmin, flexible=1)
+    for key, prec, cgp in (("mixed", tosp_mod.PREC_MIXED, 0), ("mixed_cg32", tosp_mod.PREC_MIXED, 1),
+                           ("fp64", tosp_mod.PREC_FP64, 0)):
+        s = gpu_solver(tosp_mod, pb, n, prec, ngrids, omega, rmin, flexible=1, cg_product=cgp)
         s.SetupGMG(xfil)
         u, it, rr, rc = s.SolveMG(np.zeros(pb.f.size), pb.f)
         g = s.Grad(full(pb, u))

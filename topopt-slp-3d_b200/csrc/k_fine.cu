@@ -599,12 +599,14 @@ __device__ __forceinline__ double powp(double x, double p) {
 }
 
 // wq (optional) receives the BF16-rounded factors widened back to FP64, so
-// that the mixed V-cycle's Galerkin hierarchy matches its finest operator.
-__global__ void k_simp(const double *rho, double *w64, __nv_bfloat16 *wbf, double *wq, int64_t n, double p,
-                       double emin, double E) {
+// that the mixed V-cycle's Galerkin hierarchy matches its finest operator;
+// w32 (optional) the factors rounded to FP32 (the CG's tensor-core product).
+__global__ void k_simp(const double *rho, double *w64, __nv_bfloat16 *wbf, double *wq, float *w32, int64_t n,
+                       double p, double emin, double E) {
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const double w = emin + (E - emin) * powp(rho[i], p);
         w64[i] = w;
+        if (w32) w32[i] = (float)w;
         if (wbf) {
             const __nv_bfloat16 b = __double2bfloat16(w);
             wbf[i] = b;
@@ -613,11 +615,11 @@ __global__ void k_simp(const double *rho, double *w64, __nv_bfloat16 *wbf, doubl
     }
 }
 
-void launch_simp(const double *rho, double *w64, __nv_bfloat16 *wbf, double *wq, int64_t n, double p, double emin,
-                 double E, cudaStream_t st) {
+void launch_simp(const double *rho, double *w64, __nv_bfloat16 *wbf, double *wq, float *w32, int64_t n, double p,
+                 double emin, double E, cudaStream_t st) {
     int64_t blocks = (n + 255) / 256;
     if (blocks > 4096) blocks = 4096;
-    k_simp<<<(unsigned)blocks, 256, 0, st>>>(rho, w64, wbf, wq, n, p, emin, E); count_launch();
+    k_simp<<<(unsigned)blocks, 256, 0, st>>>(rho, w64, wbf, wq, w32, n, p, emin, E); count_launch();
 }
 
 // ---------------------------------------------------------------------------

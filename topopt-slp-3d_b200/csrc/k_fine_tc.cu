@@ -56,6 +56,12 @@
 // The factors are staged as the brick's slab of the density mesh (rows along
 // y of 8n BF16 values copied in 4-byte pieces), which needs n * nely even; the
 // host uses the CUDA-core kernel otherwise.
+//
+// The same kernel with FP32 factors (one cell per 4-byte piece) and the blocks
+// in three FP16 pieces (two more MMA steps, hi + mid + lo against u_hi) is the
+// product of the FP64 CG recurrence when the caller asks for it (cg_product 1).
+// Its larger B image is shared by four bricks per CTA at one CTA per SM (one
+// brick for n = 3), which keeps 16 warps per SM for n = 1, 2.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -74,7 +80,6 @@ namespace {
 
 constexpr int TC_K = 16;                                  // K of every MMA (kind::f16)
 constexpr int TC_GROUP = 8 * TC_K * 2;                    // bytes of one 8-row group (256)
-constexpr int TC_B_STEPS = 5;
 constexpr int TC_A_TILE = BRICK_ELEMS / 8 * TC_GROUP;     // 4096 per A step
 constexpr int TC_A_BYTES = 3 * TC_A_TILE;
 constexpr int TC_XS_FLOATS = BRICK_NODES * 4;             // 900: nodes padded to float4
@@ -83,8 +88,9 @@ constexpr int TC_SLOTS_PAD = (BRICK_SLOTS + 3) / 4 * 4;   // slot table length
 constexpr uint32_t TC_WAIT_LIMIT = 1u << 16;              // try_wait rounds before giving up
 constexpr uint32_t TC_SUSPEND_NS = 20000;                 // suspend-time hint of one try_wait round
 
-// Sizes of the kernel for MR factor N.
-template <int N>
+// Sizes of the kernel for MR factor N and SIMP factors of type WT (BF16 for
+// the V-cycle, FP32 for the CG's product).
+template <int N, typename WT = __nv_bfloat16>
 struct Tc {
     static constexpr int NS = N * N * N;                  // sub-cells per element
     static constexpr int NROWS = 24 * NS;                 // block rows (GEMM N)
@@ -93,15 +99,20 @@ struct Tc {
     static constexpr int NCH = (NPAD + CH - 1) / CH;
     static constexpr int COLS = 2 * CH;                   // tensor-memory columns per CTA
     static constexpr int B_TILE = NPAD / 8 * TC_GROUP;    // bytes of one B step
-    static constexpr int B_BYTES = TC_B_STEPS * B_TILE;
-    static constexpr int IMG_BYTES = B_BYTES + 16;        // + the block scale record
+    // blocks in two FP16 pieces (hi + mid, five MMA steps) for the V-cycle's
+    // BF16-factor kernel, three (hi + mid + lo, eight steps) for the CG's
+    // FP32-factor kernel
+    static constexpr bool K3 = sizeof(WT) == 4;
+    static constexpr int B_STEPS = K3 ? 8 : 5;
+    static constexpr int B_BYTES = B_STEPS * B_TILE;
     static constexpr int WY = BY * N, WX = BX * N, WZ = BZ * N;   // factor slab (density cells)
-    static constexpr int W_BYTES = (WY * WX * WZ * 2 + 15) / 16 * 16;
-    static constexpr int UPR = WY / 2;                    // 4-byte pieces per slab row
+    static constexpr int CPP = 4 / (int)sizeof(WT);       // cells per 4-byte piece
+    static constexpr int W_BYTES = (WY * WX * WZ * (int)sizeof(WT) + 15) / 16 * 16;
+    static constexpr int UPR = WY / CPP;                  // 4-byte pieces per slab row
     // bricks processed side by side by one CTA, sharing the B image: four
     // warps each, their own A tiles, staging, outputs, barriers and
     // tensor-memory columns
-    static constexpr int NB = N == 3 ? 3 : 2;
+    static constexpr int NB = K3 ? (N == 3 ? 1 : 4) : (N == 3 ? 3 : 2);
     static constexpr int THREADS = NB * BRICK_ELEMS;
     static constexpr int TMEM_COLS = NB * COLS <= 64 ? 64 : (NB * COLS <= 128 ? 128 : (NB * COLS <= 256 ? 256 : 512));
     // layout: B image, slot table, then one region per brick
@@ -114,11 +125,12 @@ struct Tc {
     static constexpr size_t G_W = G_EO + TC_EO_BYTES;
     static constexpr size_t G_BYTES = (G_W + W_BYTES + 127) / 128 * 128;
     static constexpr size_t SMEM = OFF_G + NB * G_BYTES;
-    static constexpr int MINB = N == 3 ? 1 : (N == 2 ? 2 : 3);   // register cap: CTAs per SM aimed at
+    static constexpr int MINB = K3 || N == 3 ? 1 : (N == 2 ? 2 : 3);   // register cap: CTAs per SM aimed at
     static_assert(B_TILE % 16 == 0 && OFF_G % 16 == 0 && G_BYTES % 16 == 0 && G_XS % 16 == 0 &&
                       G_EO % 16 == 0 && G_W % 16 == 0, "operand alignment");
     static_assert(OFF_REL % 4 == 0 && OFF_PK % 2 == 0, "slot table alignment");
     static_assert(SMEM <= 227 * 1024, "shared memory per CTA");
+    static_assert(sizeof(WT) == 2 || sizeof(WT) == 4, "BF16 or FP32 factors");
     static_assert(NB * COLS <= 512, "tensor memory of an SM");
 };
 
@@ -286,19 +298,24 @@ __device__ __forceinline__ void consume_any(int c, uint32_t taddr, const float (
     ((c == Cs ? consume_chunk<N, Cs>(taddr, ws, acc) : void()), ...);
 }
 
-// The five MMAs of chunk c into tensor-memory buffer (c & 1), then a commit to
-// its barrier.
-template <int N>
+// A tile of MMA step t: steps 0-2 run A tiles 0, 1, 2 ([u_hi u_lo]) against
+// the hi piece of the blocks; steps 3-4 (two-piece image) run tiles 0, 1
+// (u_hi) against the mid piece; in the three-piece image steps 3-5 run tiles
+// 0, 1, 2 against the mid piece and steps 6-7 tiles 0, 1 against the lo piece.
+__host__ __device__ constexpr int step_a_tile(int t) { return t < 6 ? t % 3 : t - 6; }
+
+// The B_STEPS MMAs of chunk c into tensor-memory buffer (c & 1), then a commit
+// to its barrier.
+template <int N, typename WT>
 __device__ __forceinline__ void issue_chunk(int c, uint32_t tmem, uint32_t a_addr, uint32_t b_addr, uint32_t mbar) {
-    using K = Tc<N>;
+    using K = Tc<N, WT>;
     const uint32_t d = tmem + (uint32_t)((c & 1) * K::CH);
     const uint32_t boff = (uint32_t)(c * K::CH / 8 * TC_GROUP);
     const uint32_t id = idesc_f16(chunk_width(K::NPAD, K::CH, c));
-    mma_f16(d, smem_desc(a_addr), smem_desc(b_addr + boff), id, 0u);
-    mma_f16(d, smem_desc(a_addr + TC_A_TILE), smem_desc(b_addr + K::B_TILE + boff), id, 1u);
-    mma_f16(d, smem_desc(a_addr + 2 * TC_A_TILE), smem_desc(b_addr + 2 * K::B_TILE + boff), id, 1u);
-    mma_f16(d, smem_desc(a_addr), smem_desc(b_addr + 3 * K::B_TILE + boff), id, 1u);
-    mma_f16(d, smem_desc(a_addr + TC_A_TILE), smem_desc(b_addr + 4 * K::B_TILE + boff), id, 1u);
+#pragma unroll
+    for (int t = 0; t < K::B_STEPS; ++t)
+        mma_f16(d, smem_desc(a_addr + step_a_tile(t) * TC_A_TILE), smem_desc(b_addr + t * K::B_TILE + boff), id,
+                t ? 1u : 0u);
     mma_commit(mbar);
 }
 
@@ -311,13 +328,16 @@ __device__ __forceinline__ uint32_t half2_bits(__half2 h) {
     return b;
 }
 
+__device__ __forceinline__ float factor_value(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ float factor_value(float v) { return v; }
+
 // Stage brick `brick` (nodal values, and the brick's slab of SIMP factors on
 // the density mesh) with cp.async; absent nodes and cells read as zero.
-template <int N>
-__device__ __forceinline__ void stage_brick(int64_t brick, float *xs, uint16_t *wslab, const float *__restrict__ x,
-                                            const __nv_bfloat16 *__restrict__ w, const FineGeom &fg,
+template <int N, typename WT>
+__device__ __forceinline__ void stage_brick(int64_t brick, float *xs, WT *wslab, const float *__restrict__ x,
+                                            const WT *__restrict__ w, const FineGeom &fg,
                                             const int32_t *rel, const uint16_t *pk, int tid) {
-    using K = Tc<N>;
+    using K = Tc<N, WT>;
     const Grid &g = fg.g;
     int bbx, bby, bbz;
     brick_xyz(brick, fg, bbx, bby, bbz);
@@ -342,18 +362,19 @@ __device__ __forceinline__ void stage_brick(int64_t brick, float *xs, uint16_t *
             cp_async4(dst + 2, in ? src + 2 : x, in ? 4 : 0);
         }
     }
-    // factor slab: rows along y of WY values, 4-byte pieces (two cells); the
-    // density mesh has n * nely cells along y, an even number, so a piece is
-    // wholly inside or wholly outside the mesh and 4-byte aligned
+    // factor slab: rows along y of WY values, 4-byte pieces (two BF16 cells
+    // or one FP32 cell); with BF16 the density mesh has n * nely cells along
+    // y, an even number, so a piece is wholly inside or wholly outside the
+    // mesh and 4-byte aligned
     const int nelz_d = g.nelz * N;
     const int xd0 = ex0 * N, yd0 = ey0 * N, zd0 = ez0 * N;
     for (int u = tid; u < K::WZ * K::WX * K::UPR; u += BRICK_ELEMS) {
         const int row = u / K::UPR, k = u - row * K::UPR;
         const int rz = row / K::WX, rx = row - rz * K::WX;
-        const int zd = zd0 + rz, xd = xd0 + rx, yd = yd0 + 2 * k;
+        const int zd = zd0 + rz, xd = xd0 + rx, yd = yd0 + K::CPP * k;
         const bool in = zd < nelz_d && xd < fg.nelx_d && yd < fg.nely_d;
-        const __nv_bfloat16 *src = in ? w + ((int64_t)zd * fg.nelx_d + xd) * fg.nely_d + yd : w;
-        cp_async4(wslab + row * K::WY + 2 * k, src, in ? 4 : 0);
+        const WT *src = in ? w + ((int64_t)zd * fg.nelx_d + xd) * fg.nely_d + yd : w;
+        cp_async4(wslab + row * K::WY + K::CPP * k, src, in ? 4 : 0);
     }
 }
 
@@ -406,12 +427,12 @@ __device__ __forceinline__ float build_a(const float *xs, unsigned char *abuf, i
 // g: bricks g, g + NB, ... of the CTA's share, with the group's own named
 // barrier, MMA-completion barriers and tensor-memory columns (lanes 0-127 of
 // columns COLS g .. COLS (g+1) - 1, which its warps reach as warps 0-3 would).
-template <int N>
-__global__ void __launch_bounds__(Tc<N>::THREADS, Tc<N>::MINB)
-k_fine_apply_tc(const float *__restrict__ x, float *__restrict__ y, const __nv_bfloat16 *__restrict__ w,
+template <int N, typename WT>
+__global__ void __launch_bounds__(Tc<N, WT>::THREADS, Tc<N, WT>::MINB)
+k_fine_apply_tc(const float *__restrict__ x, float *__restrict__ y, const WT *__restrict__ w,
                 const uint8_t *__restrict__ freemask, const uint4 *__restrict__ bimg, FineGeom fg,
                 int *__restrict__ err) {
-    using K = Tc<N>;
+    using K = Tc<N, WT>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t s_mbar[2 * K::NB];
     __shared__ __align__(8) uint32_t s_tmem;
@@ -430,7 +451,7 @@ k_fine_apply_tc(const float *__restrict__ x, float *__restrict__ y, const __nv_b
     unsigned char *abuf = gbase + K::G_A;
     float *xs = reinterpret_cast<float *>(gbase + K::G_XS);              // staged nodal values
     float4 *eo4 = reinterpret_cast<float4 *>(gbase + K::G_EO);           // element outputs per corner
-    uint16_t *wslab = reinterpret_cast<uint16_t *>(gbase + K::G_W);      // SIMP factors (BF16 bits)
+    WT *wslab = reinterpret_cast<WT *>(gbase + K::G_W);                  // SIMP factors
 
     const Grid &g = fg.g;
     for (int i = ttid; i < K::B_BYTES / 16; i += K::THREADS) reinterpret_cast<uint4 *>(smem_raw)[i] = bimg[i];
@@ -466,7 +487,7 @@ k_fine_apply_tc(const float *__restrict__ x, float *__restrict__ y, const __nv_b
     // chunks (a group without a brick skips the loop).
     float fsc = 1.f;
     if (first < fg.nbricks) {
-        stage_brick<N>(first, xs, wslab, x, w, fg, rel, pk, tid);
+        stage_brick<N, WT>(first, xs, wslab, x, w, fg, rel, pk, tid);
         cp_async_commit();
         cp_async_wait_0();
         group_sync(grp);
@@ -475,8 +496,8 @@ k_fine_apply_tc(const float *__restrict__ x, float *__restrict__ y, const __nv_b
         group_sync(grp);
         if (tid == 0) {
             fence_after();
-            issue_chunk<N>(0, tmem, a_addr, b_addr, mbar0);
-            if (K::NCH > 1) issue_chunk<N>(1, tmem, a_addr, b_addr, mbar1);
+            issue_chunk<N, WT>(0, tmem, a_addr, b_addr, mbar0);
+            if (K::NCH > 1) issue_chunk<N, WT>(1, tmem, a_addr, b_addr, mbar1);
         }
     }
 
@@ -496,8 +517,7 @@ k_fine_apply_tc(const float *__restrict__ x, float *__restrict__ y, const __nv_b
 #pragma unroll
             for (int s = 0; s < K::NS; ++s) {
                 const int sy = s % N, sx = (s / N) % N, sz = s / (N * N);
-                const uint32_t b = wslab[((lz * N + sz) * K::WX + lx * N + sx) * K::WY + ly * N + sy];
-                ws[s] = __uint_as_float(b << 16) * f;
+                ws[s] = factor_value(wslab[((lz * N + sz) * K::WX + lx * N + sx) * K::WY + ly * N + sy]) * f;
             }
         }
         float2 acc[12];
@@ -526,12 +546,12 @@ k_fine_apply_tc(const float *__restrict__ x, float *__restrict__ y, const __nv_b
                 // past this barrier every thread of the group has read this
                 // brick's factors and the A tiles were built: the next brick's
                 // inputs go into the same buffers
-                if (next < fg.nbricks) stage_brick<N>(next, xs, wslab, x, w, fg, rel, pk, tid);
+                if (next < fg.nbricks) stage_brick<N, WT>(next, xs, wslab, x, w, fg, rel, pk, tid);
                 cp_async_commit();
             }
             if (tid == 0 && c + 2 < K::NCH) {
                 fence_after();
-                issue_chunk<N>(c + 2, tmem, a_addr, b_addr, (c & 1) ? mbar1 : mbar0);
+                issue_chunk<N, WT>(c + 2, tmem, a_addr, b_addr, (c & 1) ? mbar1 : mbar0);
             }
         }
         if (!ok) {
@@ -561,8 +581,8 @@ k_fine_apply_tc(const float *__restrict__ x, float *__restrict__ y, const __nv_b
         group_sync(grp);
         if (tid == 0 && next < fg.nbricks) {
             fence_after();
-            issue_chunk<N>(0, tmem, a_addr, b_addr, mbar0);
-            if (K::NCH > 1) issue_chunk<N>(1, tmem, a_addr, b_addr, mbar1);
+            issue_chunk<N, WT>(0, tmem, a_addr, b_addr, mbar0);
+            if (K::NCH > 1) issue_chunk<N, WT>(1, tmem, a_addr, b_addr, mbar1);
         }
         brick_gather_write(eo4, y, freemask, g, ex0, ey0, ez0, rel, pk, tid, chk);
     }
@@ -582,10 +602,19 @@ k_fine_apply_tc(const float *__restrict__ x, float *__restrict__ y, const __nv_b
                      : "memory");
 }
 
-// B image: step tiles of the scaled blocks' FP16 hi and mid pieces in the K
-// order of the MMAs above (row r = 24 s + i, entry KE_s[i][j] at k = j,
-// j - 16 + 8 or j - 8 as the step requires; rows beyond 24 n^3 zero), then the
-// block scale record: the float 2^-sc in the first four bytes.
+// B image: step tiles of the scaled blocks' FP16 pieces in the K order of the
+// MMAs above (row r = 24 s + i, entry KE_s[i][j] at k = j, j - 16 + 8 or j - 8
+// as the step requires; rows beyond 24 n^3 zero), then the block scale record:
+// the float 2^-sc in the first four bytes.  Steps 0-2 hold the hi piece against
+// A = [u_hi u_lo].  Two-piece image: steps 3-4 the mid piece against u_hi
+// (step 4: entries j >= 16 only).  Three-piece image: steps 3-5 the mid piece
+// against [u_hi u_lo], steps 6-7 the lo piece (the rest v - hi - mid, rounded)
+// against u_hi.  Two pieces carry about 22 bits of each block entry relative
+// to the largest; that truncation, and the dropped u_lo * mid product, change
+// the operator by about 2^-22 |KE| |u_e|, which slows a CG whose recurrence
+// uses it (110 -> 173 iterations on the 192 x 96 x 96 MR-2 workload; the
+// V-cycle tolerates it), so the CG's kernel takes three pieces and five
+// products (hi*hi, lo*hi, hi*mid, lo*mid, hi*lo).
 static uint16_t f16_bits(float v) {
     const __half h = __float2half_rn(v);
     uint16_t b;
@@ -598,9 +627,9 @@ static double f16_value(uint16_t b) {
     return (double)__half2float(h);
 }
 
-template <int N>
+template <int N, typename WT>
 static void tc_image(const std::vector<double> &packed_rowmajor, std::vector<uint16_t> &img) {
-    using K = Tc<N>;
+    using K = Tc<N, WT>;
     auto ke = [&](int s, int i, int j) {
         const int a = i < j ? i : j, b = i < j ? j : i;
         return packed_rowmajor[(size_t)s * KE_PACK + pair_rowmajor(a, b)];
@@ -611,7 +640,7 @@ static void tc_image(const std::vector<double> &packed_rowmajor, std::vector<uin
     int e = 0;
     frexp(kmax > 0.0 ? kmax : 1.0, &e);
     const int sc = 15 - e;   // kmax 2^sc in [2^14, 2^15)
-    img.assign(K::IMG_BYTES / 2, 0);
+    img.assign((K::B_BYTES + 16) / 2, 0);   // + the block scale record
     auto put = [&](int step, int r, int k, uint16_t b) { img[(step * K::B_TILE + tc_offset(r, k)) / 2] = b; };
     for (int r = 0; r < K::NROWS; ++r) {
         const int s = r / 24, i = r % 24;
@@ -623,8 +652,18 @@ static void tc_image(const std::vector<double> &packed_rowmajor, std::vector<uin
             else put(1, r, j - 16, hi);
             if (j < 8) put(1, r, j + 8, hi);
             else put(2, r, j - 8, hi);
-            if (j < 16) put(3, r, j, mid);
-            else put(4, r, j - 16, mid);
+            if (!K::K3) {
+                if (j < 16) put(3, r, j, mid);
+                else put(4, r, j - 16, mid);
+            } else {
+                if (j < 16) put(3, r, j, mid);
+                else put(4, r, j - 16, mid);
+                if (j < 8) put(4, r, j + 8, mid);
+                else put(5, r, j - 8, mid);
+                const uint16_t lo = f16_bits((float)(v - f16_value(hi) - f16_value(mid)));
+                if (j < 16) put(6, r, j, lo);
+                else put(7, r, j - 16, lo);
+            }
         }
     }
     const float inv = (float)ldexp(1.0, -sc);
@@ -634,15 +673,21 @@ static void tc_image(const std::vector<double> &packed_rowmajor, std::vector<uin
 bool fine_tc_supported(int n, int nely) { return n >= 1 && n <= 3 && (n * nely) % 2 == 0; }
 
 void fine_tc_image(const std::vector<double> &packed_rowmajor, int n, std::vector<uint16_t> &img) {
-    if (n == 1) tc_image<1>(packed_rowmajor, img);
-    else if (n == 2) tc_image<2>(packed_rowmajor, img);
-    else tc_image<3>(packed_rowmajor, img);
+    if (n == 1) tc_image<1, __nv_bfloat16>(packed_rowmajor, img);
+    else if (n == 2) tc_image<2, __nv_bfloat16>(packed_rowmajor, img);
+    else tc_image<3, __nv_bfloat16>(packed_rowmajor, img);
+}
+
+void fine_tc_image_w32(const std::vector<double> &packed_rowmajor, int n, std::vector<uint16_t> &img) {
+    if (n == 1) tc_image<1, float>(packed_rowmajor, img);
+    else if (n == 2) tc_image<2, float>(packed_rowmajor, img);
+    else tc_image<3, float>(packed_rowmajor, img);
 }
 
 // Resident CTAs per SM from the device limits (shared memory with the
 // per-CTA reservation, registers at warp allocation granularity), capped by
 // the 512 tensor-memory columns.
-template <int N>
+template <int N, typename WT>
 static int tc_ctas_per_sm() {
     int dev = 0, smem_sm = 0, smem_res = 0, regs_sm = 0;
     cudaGetDevice(&dev);
@@ -650,16 +695,17 @@ static int tc_ctas_per_sm() {
     cudaDeviceGetAttribute(&smem_res, cudaDevAttrReservedSharedMemoryPerBlock, dev);
     cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev);
     cudaFuncAttributes fa{};
-    if (cudaFuncGetAttributes(&fa, k_fine_apply_tc<N>) != cudaSuccess) {
+    if (cudaFuncGetAttributes(&fa, k_fine_apply_tc<N, WT>) != cudaSuccess) {
         cudaGetLastError();
         return 1;
     }
-    const size_t per_cta = Tc<N>::SMEM + fa.sharedSizeBytes + (size_t)smem_res;
+    using K = Tc<N, WT>;
+    const size_t per_cta = K::SMEM + fa.sharedSizeBytes + (size_t)smem_res;
     const int by_smem = (int)(smem_sm / per_cta);
     const int regs_warp = (fa.numRegs * 32 + 255) / 256 * 256;
-    const int by_regs = regs_sm / (regs_warp * (Tc<N>::THREADS / 32));
+    const int by_regs = regs_sm / (regs_warp * (K::THREADS / 32));
     int m = by_smem < by_regs ? by_smem : by_regs;
-    if (m > 512 / Tc<N>::TMEM_COLS) m = 512 / Tc<N>::TMEM_COLS;
+    if (m > 512 / K::TMEM_COLS) m = 512 / K::TMEM_COLS;
     return m < 1 ? 1 : m;
 }
 
@@ -673,30 +719,39 @@ static int num_sms_tc() {
     return n;
 }
 
-template <int N>
-static void launch_tc(const float *x, float *y, const __nv_bfloat16 *w, const uint8_t *fm, const void *bimg,
+template <int N, typename WT>
+static void launch_tc(const float *x, float *y, const WT *w, const uint8_t *fm, const void *bimg,
                       const FineGeom &fg, int *err, cudaStream_t st) {
+    using K = Tc<N, WT>;
     static int attr_dev = -1, per_sm = 1;
     int dev = 0;
     cudaGetDevice(&dev);
     if (attr_dev != dev) {
-        cudaFuncSetAttribute(k_fine_apply_tc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Tc<N>::SMEM);
-        cudaFuncSetAttribute(k_fine_apply_tc<N>, cudaFuncAttributePreferredSharedMemoryCarveout,
+        cudaFuncSetAttribute(k_fine_apply_tc<N, WT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)K::SMEM);
+        cudaFuncSetAttribute(k_fine_apply_tc<N, WT>, cudaFuncAttributePreferredSharedMemoryCarveout,
                              (int)cudaSharedmemCarveoutMaxShared);
-        per_sm = tc_ctas_per_sm<N>();
+        per_sm = tc_ctas_per_sm<N, WT>();
         attr_dev = dev;
     }
     int64_t grid = (int64_t)per_sm * num_sms_tc();
-    const int64_t need = (fg.nbricks + Tc<N>::NB - 1) / Tc<N>::NB;   // NB bricks side by side per CTA
+    const int64_t need = (fg.nbricks + K::NB - 1) / K::NB;   // NB bricks side by side per CTA
     if (grid > need) grid = need;
     if (grid < 1) grid = 1;
-    k_fine_apply_tc<N><<<(unsigned)grid, Tc<N>::THREADS, Tc<N>::SMEM, st>>>(x, y, w, fm, (const uint4 *)bimg, fg,
-                                                                          err);
+    k_fine_apply_tc<N, WT><<<(unsigned)grid, K::THREADS, K::SMEM, st>>>(x, y, w, fm, (const uint4 *)bimg, fg, err);
     count_launch();
 }
 
 void launch_fine_apply_tc(const float *x, float *y, const __nv_bfloat16 *w, const uint8_t *fm, const void *bimg,
                           const FineGeom &fg, int n, int *err, cudaStream_t st) {
+    if (n == 1) launch_tc<1>(x, y, w, fm, bimg, fg, err, st);
+    else if (n == 2) launch_tc<2>(x, y, w, fm, bimg, fg, err, st);
+    else launch_tc<3>(x, y, w, fm, bimg, fg, err, st);
+}
+
+bool fine_tc_w32_supported(int n) { return n >= 1 && n <= 3; }
+
+void launch_fine_apply_tc_w32(const float *x, float *y, const float *w, const uint8_t *fm, const void *bimg,
+                              const FineGeom &fg, int n, int *err, cudaStream_t st) {
     if (n == 1) launch_tc<1>(x, y, w, fm, bimg, fg, err, st);
     else if (n == 2) launch_tc<2>(x, y, w, fm, bimg, fg, err, st);
     else launch_tc<3>(x, y, w, fm, bimg, fg, err, st);

@@ -80,11 +80,12 @@ __device__ __forceinline__ double sum_partials(const double *partials, int np, d
     return block_sum(s, sh);
 }
 
-__global__ void k_dot_partial(const double *a, const double *b, int64_t n, double *partials, double *out) {
+template <typename TB>
+__global__ void k_dot_partial(const double *a, const TB *b, int64_t n, double *partials, double *out) {
     __shared__ double sh[32];
     double s = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        s += a[i] * b[i];
+        s += a[i] * (double)b[i];
     s = block_sum(s, sh);
     if (threadIdx.x == 0) partials[blockIdx.x] = s;
     if (last_block(red_counter(partials))) {
@@ -94,7 +95,10 @@ __global__ void k_dot_partial(const double *a, const double *b, int64_t n, doubl
 }
 
 void launch_dot(const double *a, const double *b, int64_t n, double *partials, double *out, cudaStream_t st) {
-    k_dot_partial<<<RED_BLOCKS, 256, 0, st>>>(a, b, n, partials, out); count_launch();
+    k_dot_partial<double><<<RED_BLOCKS, 256, 0, st>>>(a, b, n, partials, out); count_launch();
+}
+void launch_dot(const double *a, const float *b, int64_t n, double *partials, double *out, cudaStream_t st) {
+    k_dot_partial<float><<<RED_BLOCKS, 256, 0, st>>>(a, b, n, partials, out); count_launch();
 }
 
 // a'b and a'c in one pass over a (partials: 2 * RED_BLOCKS).
@@ -181,25 +185,28 @@ template void launch_jacobi_out_dot<double>(double *, const double *, const doub
 // iteration's s_old).  The iterate update of the previous iteration,
 // x += alpha d (I/SolveMG.m:40), is done here, while d is read anyway, before
 // d is replaced (modes 0 and 2); launch_pcg_finish applies the last one.
+// d32 (optional) receives the new d in FP32, the input of the tensor-core
+// product.
 __global__ void k_pcg_direction(double *d, const double *s, double *sold, const double *scal, int64_t n, int mode,
-                                double *x) {
+                                double *x, float *d32) {
     const double beta = mode == 1 ? 0.0 : (mode == 2 ? (scal[0] - scal[5]) / scal[1] : scal[0] / scal[1]);
     const double alpha = scal[6];
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const double si = s[i];
-        if (mode == 1) {
-            d[i] = si;
-        } else {
+        double dn = si;
+        if (mode != 1) {
             const double di = d[i];
             x[i] += alpha * di;
-            d[i] = beta * di + si;
+            dn = beta * di + si;
         }
+        d[i] = dn;
+        if (d32) d32[i] = (float)dn;
         if (sold) sold[i] = si;
     }
 }
 void launch_pcg_direction(double *d, const double *s, double *sold, const double *scal, int64_t n, int mode,
-                          double *x, cudaStream_t st) {
-    k_pcg_direction<<<gridv(n), 256, 0, st>>>(d, s, sold, scal, n, mode, x); count_launch();
+                          double *x, cudaStream_t st, float *d32) {
+    k_pcg_direction<<<gridv(n), 256, 0, st>>>(d, s, sold, scal, n, mode, x, d32); count_launch();
 }
 
 // x += alpha d with the last iteration's alpha (slot 6).
@@ -217,13 +224,14 @@ void launch_pcg_finish(double *x, const double *d, const double *scal, int64_t n
 // given) it also writes the next cycle's FP32 right-hand side b0 = r and, when
 // x0 is given, its first Jacobi iterate x0 = invd0 b0 (the sweep from a zero
 // guess).
-__global__ void k_pcg_update(double *r, const double *q, double *scal, int64_t n, double *partials, float *b0,
+template <typename TQ>
+__global__ void k_pcg_update(double *r, const TQ *q, double *scal, int64_t n, double *partials, float *b0,
                              const float *invd0, float *x0) {
     __shared__ double sh[32];
     const double alpha = scal[0] / scal[2];
     double s = 0.0;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double ri = r[i] - alpha * q[i];
+        const double ri = r[i] - alpha * (double)q[i];
         r[i] = ri;
         s += ri * ri;
         if (b0) {
@@ -246,7 +254,40 @@ __global__ void k_pcg_update(double *r, const double *q, double *scal, int64_t n
 
 void launch_pcg_update(double *r, const double *q, double *scal, double *partials, int64_t n, cudaStream_t st,
                        float *b0, const float *invd0, float *x0) {
-    k_pcg_update<<<RED_BLOCKS, 256, 0, st>>>(r, q, scal, n, partials, b0, invd0, x0); count_launch();
+    k_pcg_update<double><<<RED_BLOCKS, 256, 0, st>>>(r, q, scal, n, partials, b0, invd0, x0); count_launch();
+}
+void launch_pcg_update(double *r, const float *q, double *scal, double *partials, int64_t n, cudaStream_t st,
+                       float *b0, const float *invd0, float *x0) {
+    k_pcg_update<float><<<RED_BLOCKS, 256, 0, st>>>(r, q, scal, n, partials, b0, invd0, x0); count_launch();
+}
+
+// Residual replacement: r = f - t (t = K x by the FP64 operator), r'r into
+// slot 3 (last block) and, for the mixed V-cycle (b0 given), the next cycle's
+// FP32 right-hand side and first Jacobi iterate as in k_pcg_update.
+__global__ void k_replace_residual(const double *f, const double *t, double *r, double *scal, int64_t n,
+                                   double *partials, float *b0, const float *invd0, float *x0) {
+    __shared__ double sh[32];
+    double s = 0.0;
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const double ri = f[i] - t[i];
+        r[i] = ri;
+        s += ri * ri;
+        if (b0) {
+            const float bi = (float)ri;
+            b0[i] = bi;
+            if (x0) x0[i] = invd0[i] * bi;
+        }
+    }
+    s = block_sum(s, sh);
+    if (threadIdx.x == 0) partials[blockIdx.x] = s;
+    if (last_block(red_counter(partials))) {
+        const double t2 = sum_partials(partials, gridDim.x, sh);
+        if (threadIdx.x == 0) scal[3] = t2;
+    }
+}
+void launch_replace_residual(const double *f, const double *t, double *r, double *scal, double *partials, int64_t n,
+                             cudaStream_t st, float *b0, const float *invd0, float *x0) {
+    k_replace_residual<<<RED_BLOCKS, 256, 0, st>>>(f, t, r, scal, n, partials, b0, invd0, x0); count_launch();
 }
 
 __global__ void k_set_scalar(double *dst, const double *src) { *dst = *src; }

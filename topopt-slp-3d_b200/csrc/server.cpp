@@ -71,7 +71,12 @@ std::string shape_key(const Request &r) {
     add(&r.pb.el, sizeof(double) * 7);
     add(&r.pb.mr_n, sizeof(int32_t) * 2);
     add(&r.pb.rmin, sizeof(double));
-    add(&r.mg, sizeof(r.mg));
+    // field by field: the struct's padding bytes are not part of the key
+    const tosp_mg_params &m = r.mg;
+    for (int32_t v : {m.ngrids, m.cycle, m.smoother, m.smoothiter1, m.smoothiter2, m.maxiterMG, m.nmaxchol,
+                      m.flexible, m.maxstall, m.warp_stencil_max, m.small_cycle_max, m.cg_product})
+        add(&v, sizeof(v));
+    for (double v : {m.omega, m.tolMG, m.replace_drop}) add(&v, sizeof(v));
     add(&r.precision, sizeof(r.precision));
     uint64_t hsh = 1469598103934665603ull;
     auto mix = [&](const std::vector<int64_t> &v) {
@@ -89,10 +94,16 @@ std::string shape_key(const Request &r) {
     return k;
 }
 
-// Multigrid parameters of a served request: as submitted.  A request with
+// Multigrid parameters of a served request: as submitted, except cg_product
+// (batched iterations keep the FP64 product every iteration; the residual
+// replacements of cg_product 1 are per-solve host decisions).  A request with
 // mg.small_cycle_max > 0 runs its small levels as the persistent cycle, which
 // the batch runner launches once per visit for all same-shape requests.
-tosp_mg_params serving_mg(const tosp_mg_params &mg) { return mg; }
+tosp_mg_params serving_mg(const tosp_mg_params &mg) {
+    tosp_mg_params m = mg;
+    m.cg_product = 0;
+    return m;
+}
 
 int64_t estimate_bytes(const Request &r) {
     const int64_t nx = r.pb.nelx + 1, ny = r.pb.nely + 1, nz = r.pb.nelz + 1;

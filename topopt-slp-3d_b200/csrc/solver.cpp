@@ -61,10 +61,12 @@ struct tosp_handle {
     std::vector<double> ktab_c;     // MR 2: FP64 Walsh-Hadamard coefficients passed with each launch
     uint16_t *d_tcimg = nullptr;    // mixed: tensor-core B operand image of the blocks (null: CUDA-core kernel)
     int *d_tcerr = nullptr;         // set by the tensor-core operator when an MMA wait times out
+    uint16_t *d_tcimg32 = nullptr;  // cg_product 1: B image of the CG's product (three-piece blocks)
     // densities
     double *d_rho = nullptr, *d_w64 = nullptr;
     double *d_wq = nullptr;         // mixed: BF16-rounded factors in FP64 (V-cycle hierarchy)
     __nv_bfloat16 *d_wbf = nullptr;
+    float *d_w32 = nullptr;         // cg_product 1: FP32 factors of the CG's tensor-core product
     uint8_t *d_free_elem = nullptr;
     // filter
     FilterTap *d_taps = nullptr;
@@ -99,6 +101,9 @@ struct tosp_handle {
     bool graph_failed = false;
     // CG (FP64, full-length vectors with zeros on fixed dofs)
     double *cx = nullptr, *cr = nullptr, *cd = nullptr, *cq = nullptr, *cs = nullptr, *cf = nullptr, *cso = nullptr;
+    // cg_product 1: the direction in FP32 and its tensor-core product
+    bool cg32 = false;
+    float *cd32 = nullptr, *cq32 = nullptr;
     double *d_partials = nullptr, *d_scal = nullptr, *h_scal = nullptr;
     // staging
     double *d_stage_a = nullptr, *d_stage_b = nullptr;
@@ -264,6 +269,14 @@ int fine_apply(tosp_handle *h, const T *x, T *y) {
 }
 
 int fine_apply64(tosp_handle *h, const double *x, double *y) { return fine_apply<double>(h, x, y); }
+
+// cg_product 1: the CG's product y = K x on the tensor cores with FP32 factors.
+int fine_apply_cg32(tosp_handle *h, const float *x, float *y) {
+    CK(cudaMemsetAsync(y, 0, sizeof(float) * h->fg.g.ndof, h->stream));
+    launch_fine_apply_tc_w32(x, y, h->d_w32, h->lev[0].fm, h->d_tcimg32, h->fg, h->n, h->d_tcerr, h->stream);
+    CKL();
+    return TOSP_OK;
+}
 
 // Damped Jacobi sweeps (I/Smooth.m:14-23).  first_done: the first sweep from
 // a zero guess was already written into lev[l].x (fused into the CG update);
@@ -699,6 +712,15 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
         h->err = "precision must be TOSP_PREC_FP64 or TOSP_PREC_MIXED";
         return TOSP_ERR_BAD_ARG;
     }
+    if (mg->cg_product < 0 || mg->cg_product > 1 || mg->replace_drop < 0.0 || mg->replace_drop >= 1.0) {
+        h->err = "cg_product must be 0 or 1 and replace_drop in [0, 1)";
+        return TOSP_ERR_BAD_ARG;
+    }
+    if (mg->cg_product == 1 && (precision != TOSP_PREC_MIXED || !fine_tc_supported(pb->mr_n, pb->nely) ||
+                                !fine_tc_w32_supported(pb->mr_n))) {
+        h->err = "cg_product 1 needs TOSP_PREC_MIXED and the tensor-core operator (n * nely even)";
+        return TOSP_ERR_UNSUPPORTED;
+    }
     if (!pb->freedofs || pb->nfree <= 0) {
         h->err = "freedofs missing";
         return TOSP_ERR_BAD_ARG;
@@ -714,6 +736,8 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
     h->el = pb->el; h->eh = pb->eh; h->ew = pb->ew;
     h->opfilter = pb->opfilter; h->rmin = pb->rmin;
     h->mg = *mg;
+    if (h->mg.replace_drop == 0.0) h->mg.replace_drop = 0.1;
+    h->cg32 = mg->cg_product == 1;
     std::string msg;
     int ng = choose_levels(pb->nelx, pb->nely, pb->nelz, mg->ngrids, mg->nmaxchol, msg);
     if (ng < 0) {
@@ -774,6 +798,11 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
         CK(cudaMemcpy(h->d_tcimg, img.data(), sizeof(uint16_t) * img.size(), cudaMemcpyHostToDevice));
         TRY(dalloc(h, &h->d_tcerr, 1));
         CK(cudaMemset(h->d_tcerr, 0, sizeof(int)));
+        if (mg->cg_product == 1) {
+            fine_tc_image_w32(packed, h->n, img);
+            TRY(dalloc(h, &h->d_tcimg32, (int64_t)img.size()));
+            CK(cudaMemcpy(h->d_tcimg32, img.data(), sizeof(uint16_t) * img.size(), cudaMemcpyHostToDevice));
+        }
     }
 
     // levels
@@ -814,6 +843,7 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
         TRY(dalloc(h, &h->d_wbf, nd));
         TRY(dalloc(h, &h->d_wq, nd));
     }
+    if (h->cg32) TRY(dalloc(h, &h->d_w32, nd));
     TRY(dalloc(h, &h->d_free_elem, g0.nelem));
     {
         std::vector<uint8_t> fe(g0.nelem, pb->free_dens_g ? 0 : 1);
@@ -837,6 +867,10 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
     TRY(dalloc(h, &h->cs, g0.ndof));
     TRY(dalloc(h, &h->cf, g0.ndof));
     if (mg->flexible) TRY(dalloc(h, &h->cso, g0.ndof));
+    if (h->cg32) {
+        TRY(dalloc(h, &h->cd32, g0.ndof));
+        TRY(dalloc(h, &h->cq32, g0.ndof));
+    }
     TRY(dalloc(h, &h->d_partials, 2 * RED_BLOCKS + 1));   // + the reductions' arrival counter
     CK(cudaMemset(h->d_partials, 0, sizeof(double) * (2 * RED_BLOCKS + 1)));
     TRY(dalloc(h, &h->d_scal, 16));
@@ -1009,13 +1043,21 @@ int cg_iteration(tosp_handle *h, int mode, int k) {
         if (mode == 2) launch_dot2(h->cr, s, s_old, nd, h->d_partials, h->d_scal + 0, h->d_scal + 5, h->stream);
         else launch_dot(h->cr, s, nd, h->d_partials, h->d_scal + 0, h->stream);
     }
-    launch_pcg_direction(h->cd, s, nullptr, h->d_scal, nd, mode, h->cx, h->stream);
+    launch_pcg_direction(h->cd, s, nullptr, h->d_scal, nd, mode, h->cx, h->stream, h->cg32 ? h->cd32 : nullptr);
     CKL();
-    TRY(fine_apply64(h, h->cd, h->cq));
-    launch_dot(h->cd, h->cq, nd, h->d_partials, h->d_scal + 2, h->stream);
     const bool first = mixed && fused_first_sweep(h);
-    launch_pcg_update(h->cr, h->cq, h->d_scal, h->d_partials, nd, h->stream, mixed ? (float *)F.b : nullptr,
-                      first ? (const float *)F.invd : nullptr, first ? (float *)F.x : nullptr);
+    float *b0 = mixed ? (float *)F.b : nullptr;
+    const float *invd0 = first ? (const float *)F.invd : nullptr;
+    float *x0 = first ? (float *)F.x : nullptr;
+    if (h->cg32) {
+        TRY(fine_apply_cg32(h, h->cd32, h->cq32));
+        launch_dot(h->cd, (const float *)h->cq32, nd, h->d_partials, h->d_scal + 2, h->stream);
+        launch_pcg_update(h->cr, (const float *)h->cq32, h->d_scal, h->d_partials, nd, h->stream, b0, invd0, x0);
+    } else {
+        TRY(fine_apply64(h, h->cd, h->cq));
+        launch_dot(h->cd, h->cq, nd, h->d_partials, h->d_scal + 2, h->stream);
+        launch_pcg_update(h->cr, h->cq, h->d_scal, h->d_partials, nd, h->stream, b0, invd0, x0);
+    }
     CKL();
     CK(cudaMemcpyAsync(h->h_scal, h->d_scal, sizeof(double) * 8, cudaMemcpyDeviceToHost, h->stream));
     return TOSP_OK;
@@ -1067,6 +1109,8 @@ int solve_init(tosp_handle *h) {
     S.rc = TOSP_OK;
     S.best = S.nr;
     S.best_it = 1;
+    S.rmax = S.nr;
+    S.replaced = 0;
     S.done = !(S.nr > h->mg.tolMG && S.it <= h->mg.maxiterMG);
     return TOSP_OK;
 }
@@ -1131,8 +1175,39 @@ int solve_finish(tosp_handle *h, int32_t *it_out, double *relres_out) {
     if (relres_out) *relres_out = S.nr;
     h->stats.it = S.it;
     h->stats.relres = S.nr;
+    h->stats.replacements = S.replaced;
     TRY(check_tc(h));
     return S.rc;
+}
+
+// cg_product 1, after solve_account: once the recurrence residual has fallen
+// by replace_drop below the largest one since the last replacement, claims
+// convergence, or the loop ends otherwise, the iterate update of this
+// iteration is applied and r is replaced by the FP64 residual f - K x (FP64
+// operator).  The search direction is kept; the loop then continues from the
+// true residual, so convergence is only accepted on it.
+int replace_residual(tosp_handle *h) {
+    SolveState &S = h->st;
+    if (!h->cg32 || S.rc == TOSP_ERR_BREAKDOWN) return TOSP_OK;
+    if (S.nr > S.rmax) S.rmax = S.nr;
+    if (!S.done && !(S.nr < h->mg.replace_drop * S.rmax)) return TOSP_OK;
+    Level &F = h->lev[0];
+    const int64_t nd = F.g.ndof;
+    launch_pcg_finish(h->cx, h->cd, h->d_scal, nd, h->stream);
+    CKL();
+    // the update is applied: the next direction update and the final one add nothing
+    CK(cudaMemsetAsync(h->d_scal + 6, 0, sizeof(double), h->stream));
+    TRY(fine_apply64(h, h->cx, h->cq));
+    const bool first = fused_first_sweep(h);
+    launch_replace_residual(h->cf, h->cq, h->cr, h->d_scal, h->d_partials, nd, h->stream, (float *)F.b,
+                            first ? (const float *)F.invd : nullptr, first ? (float *)F.x : nullptr);
+    CKL();
+    TRY(read_scalars(h));
+    S.nr = std::sqrt(h->h_scal[3]) / S.nf;
+    S.rmax = S.nr;
+    ++S.replaced;
+    if (S.rc == TOSP_OK) S.done = !(S.nr > h->mg.tolMG && S.it <= h->mg.maxiterMG);
+    return TOSP_OK;
 }
 
 int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
@@ -1141,6 +1216,7 @@ int solve_impl(tosp_handle *h, int32_t *it_out, double *relres_out) {
         TRY(solve_launch_iteration(h));
         TRY(sync(h));
         solve_account(h);
+        TRY(replace_residual(h));
     }
     return solve_finish(h, it_out, relres_out);
 }
@@ -1395,6 +1471,8 @@ void tosp_default_mg_params(tosp_mg_params *mg) {
     mg->maxstall = 0;
     mg->warp_stencil_max = 0;
     mg->small_cycle_max = 0;
+    mg->cg_product = 0;
+    mg->replace_drop = 0.1;
 }
 
 int tosp_create(const tosp_problem *prob, const tosp_mg_params *mg, int32_t precision, tosp_handle **out) {
@@ -1459,7 +1537,7 @@ int tosp_setup_gmg(tosp_handle *h, const double *xfil, int64_t ndens) {
     TRY(check_len(h, ndens, h->dens.nelem, "densities"));
     CK(cudaEventRecord(h->ev0, h->stream));
     TRY(load_vec(h, h->d_rho, xfil, ndens));
-    launch_simp(h->d_rho, h->d_w64, h->d_wbf, h->d_wq, ndens, h->p, h->emin, h->E, h->stream);
+    launch_simp(h->d_rho, h->d_w64, h->d_wbf, h->d_wq, h->d_w32, ndens, h->p, h->emin, h->E, h->stream);
     CKL();
     h->setup_done = false;
     if (h->mg_ok) {
@@ -1504,6 +1582,28 @@ int tosp_kelem_prod_mixed(tosp_handle *h, const double *x, double *y, int64_t nf
     CKL();
     TRY(fine_apply<float>(h, (const float *)F.x, (float *)F.t));
     launch_convert<float, double>((const float *)F.t, h->cq, nd, h->stream);
+    CKL();
+    TRY(full_to_free(h, h->cq, y, "y"));
+    TRY(sync(h));
+    return check_tc(h);
+}
+
+int tosp_kelem_prod_cg32(tosp_handle *h, const double *x, double *y, int64_t nfree) {
+    TraceRange trace_("KelemProdCG32");
+    if (!h || !x || !y) return TOSP_ERR_BAD_ARG;
+    cudaSetDevice(h->device);
+    if (!h->cg32) {
+        h->err = "the CG's tensor-core product exists only on handles created with cg_product 1";
+        return TOSP_ERR_STATE;
+    }
+    TRY(check_len(h, nfree, h->nfree, "x"));
+    TRY(need_setup(h));
+    const int64_t nd = h->lev[0].g.ndof;
+    TRY(free_to_full(h, x, h->cd, "x"));
+    launch_convert<double, float>(h->cd, h->cd32, nd, h->stream);
+    CKL();
+    TRY(fine_apply_cg32(h, h->cd32, h->cq32));
+    launch_convert<float, double>(h->cq32, h->cq, nd, h->stream);
     CKL();
     TRY(full_to_free(h, h->cq, y, "y"));
     TRY(sync(h));
@@ -1647,8 +1747,13 @@ int tosp_time_operator(tosp_handle *h, int32_t precision, int32_t reps, double *
     if (!h || !ms_per_launch || reps < 1) return TOSP_ERR_BAD_ARG;
     cudaSetDevice(h->device);
     TRY(need_setup(h));
+    if (precision < 0 || precision > 2) return TOSP_ERR_BAD_ARG;
     if (precision == TOSP_PREC_MIXED && h->precision != TOSP_PREC_MIXED) {
         h->err = "the FP32/BF16 operator exists only on TOSP_PREC_MIXED handles";
+        return TOSP_ERR_STATE;
+    }
+    if (precision == 2 && !h->cg32) {
+        h->err = "the CG's tensor-core product exists only on handles created with cg_product 1";
         return TOSP_ERR_STATE;
     }
     const Grid &g0 = h->lev[0].g;
@@ -1661,6 +1766,11 @@ int tosp_time_operator(tosp_handle *h, int32_t precision, int32_t reps, double *
             CK(cudaMemsetAsync(h->cq, 0, sizeof(double) * g0.ndof, h->stream));
             CK(cudaEventRecord(a, h->stream));
             launch_fine64(h, h->cd, h->cq);
+        } else if (precision == 2) {
+            CK(cudaMemsetAsync(h->cq32, 0, sizeof(float) * g0.ndof, h->stream));
+            CK(cudaEventRecord(a, h->stream));
+            launch_fine_apply_tc_w32(h->cd32, h->cq32, h->d_w32, h->lev[0].fm, h->d_tcimg32, h->fg, h->n, h->d_tcerr,
+                                     h->stream);
         } else {
             Level &F = h->lev[0];
             CK(cudaMemsetAsync(F.t, 0, sizeof(float) * g0.ndof, h->stream));

@@ -99,10 +99,10 @@ void filter_taps(double rmin, double el, double eh, double ew, int opfilter, std
 // ---------------------------------------------------------------------------
 // Kernel launchers.  All take the stream of the handle.
 // ---------------------------------------------------------------------------
-// SIMP factors w = emin + (E-emin) rho^p, in FP64 and (optionally) BF16 plus
-// the BF16 values widened to FP64.
-void launch_simp(const double *rho, double *w64, __nv_bfloat16 *wbf, double *wq, int64_t n, double p, double emin,
-                 double E, cudaStream_t st);
+// SIMP factors w = emin + (E-emin) rho^p, in FP64 and (each optional) BF16,
+// the BF16 values widened to FP64, and FP32.
+void launch_simp(const double *rho, double *w64, __nv_bfloat16 *wbf, double *wq, float *w32, int64_t n, double p,
+                 double emin, double E, cudaStream_t st);
 
 // Fine MR operator y = K(w) x (y must be zeroed by the caller; fixed dofs of
 // y stay zero).  kt: the n^3 blocks pair-major, see fine_nsp.
@@ -128,6 +128,12 @@ bool fine_tc_supported(int n, int nely);
 void fine_tc_image(const std::vector<double> &packed_rowmajor, int n, std::vector<uint16_t> &img);
 void launch_fine_apply_tc(const float *x, float *y, const __nv_bfloat16 *w, const uint8_t *fm, const void *bimg,
                           const FineGeom &fg, int n, int *err, cudaStream_t st);
+// The same product with FP32 SIMP factors and the blocks in three FP16 pieces
+// (the CG's product of cg_product 1), with its own B image.
+bool fine_tc_w32_supported(int n);
+void fine_tc_image_w32(const std::vector<double> &packed_rowmajor, int n, std::vector<uint16_t> &img);
+void launch_fine_apply_tc_w32(const float *x, float *y, const float *w, const uint8_t *fm, const void *bimg,
+                              const FineGeom &fg, int n, int *err, cudaStream_t st);
 
 // Sensitivities g0 (I/Grad.m:24-49), zero for elements not in freeDensG.
 void launch_grad(const double *u, const double *rho, const uint8_t *free_elem, const double *kepack,
@@ -249,12 +255,13 @@ void launch_convert(const TI *a, TO *b, int64_t n, cudaStream_t st);
 // Deterministic dot products: out[0] = sum a*b (fixed reduction tree).
 constexpr int RED_BLOCKS = 592;
 void launch_dot(const double *a, const double *b, int64_t n, double *partials, double *out, cudaStream_t st);
+void launch_dot(const double *a, const float *b, int64_t n, double *partials, double *out, cudaStream_t st);
 // a'b -> out0 and a'c -> out1 in one pass (partials: 2 * RED_BLOCKS).
 void launch_dot2(const double *a, const double *b, const double *c, int64_t n, double *partials, double *out0,
                  double *out1, cudaStream_t st);
 // PCG pieces (scalars in device memory, see solver.cpp for the slots).
 void launch_pcg_direction(double *d, const double *s, double *sold, const double *scal, int64_t n, int mode,
-                          double *x, cudaStream_t st);
+                          double *x, cudaStream_t st, float *d32 = nullptr);
 void launch_pcg_finish(double *x, const double *d, const double *scal, int64_t n, cudaStream_t st);
 // launch_jacobi_out with the CG's dots r's (-> out0) and r's_old (-> out1,
 // when so is given) of the new s in the same pass.
@@ -263,6 +270,12 @@ void launch_jacobi_out_dot(double *out, const T *x, const T *b, const T *t, cons
                            const double *so, double *partials, double *out0, double *out1, cudaStream_t st);
 void launch_pcg_update(double *r, const double *q, double *scal, double *partials, int64_t n, cudaStream_t st,
                        float *b0 = nullptr, const float *invd0 = nullptr, float *x0 = nullptr);
+void launch_pcg_update(double *r, const float *q, double *scal, double *partials, int64_t n, cudaStream_t st,
+                       float *b0 = nullptr, const float *invd0 = nullptr, float *x0 = nullptr);
+// r = f - t with r'r into scal[3] (residual replacement of cg_product 1), and
+// the next mixed cycle's input as in launch_pcg_update.
+void launch_replace_residual(const double *f, const double *t, double *r, double *scal, double *partials, int64_t n,
+                             cudaStream_t st, float *b0 = nullptr, const float *invd0 = nullptr, float *x0 = nullptr);
 void launch_set_scalar(double *dst, const double *src, cudaStream_t st);
 
 // Loop state of an MG-preconditioned CG solve (I/SolveMG.m:26-53).
@@ -273,6 +286,8 @@ struct SolveState {
     int best_it = 0;
     int rc = 0;             // TOSP_OK, TOSP_NOT_CONVERGED or TOSP_ERR_BREAKDOWN
     bool done = false;      // the loop condition no longer holds
+    double rmax = 0;        // cg_product 1: largest residual since the last replacement
+    int replaced = 0;       // cg_product 1: residual replacements so far
 };
 
 // Serving-loop batches (solver.cpp): a solve's steps, and one CG iteration of

@@ -51,7 +51,8 @@ class MgParams(C.Structure):
     _fields_ = [("ngrids", C.c_int32), ("cycle", C.c_int32), ("smoother", C.c_int32), ("omega", C.c_double),
                 ("smoothiter1", C.c_int32), ("smoothiter2", C.c_int32), ("tolMG", C.c_double),
                 ("maxiterMG", C.c_int32), ("nmaxchol", C.c_int32), ("flexible", C.c_int32),
-                ("maxstall", C.c_int32), ("warp_stencil_max", C.c_int32), ("small_cycle_max", C.c_int32)]
+                ("maxstall", C.c_int32), ("warp_stencil_max", C.c_int32), ("small_cycle_max", C.c_int32),
+                ("cg_product", C.c_int32), ("replace_drop", C.c_double)]
 
 
 class RequestStats(C.Structure):
@@ -60,7 +61,8 @@ class RequestStats(C.Structure):
 
 
 class SolveStats(C.Structure):
-    _fields_ = [("it", C.c_int32), ("relres", C.c_double), ("ms_setup", C.c_double), ("ms_solve", C.c_double)]
+    _fields_ = [("it", C.c_int32), ("relres", C.c_double), ("ms_setup", C.c_double), ("ms_solve", C.c_double),
+                ("replacements", C.c_int32)]
 
 
 def _load():
@@ -81,6 +83,7 @@ def _load():
         "tosp_setup_gmg": (C.c_int, [C.c_void_p, d, C.c_int64]),
         "tosp_kelem_prod": (C.c_int, [C.c_void_p, d, d, C.c_int64]),
         "tosp_kelem_prod_mixed": (C.c_int, [C.c_void_p, d, d, C.c_int64]),
+        "tosp_kelem_prod_cg32": (C.c_int, [C.c_void_p, d, d, C.c_int64]),
         "tosp_mg_cycle": (C.c_int, [C.c_void_p, d, d, C.c_int64]),
         "tosp_solve_mg": (C.c_int, [C.c_void_p, d, d, C.c_int64, P(C.c_int32), P(C.c_double)]),
         "tosp_grad": (C.c_int, [C.c_void_p, d, C.c_int64, d, d, C.c_int64]),
@@ -240,7 +243,8 @@ class Solver:
     def stats(self):
         st = SolveStats()
         self._check(_lib.tosp_last_stats(self.h, C.byref(st)))
-        return {"it": st.it, "relres": st.relres, "ms_setup": st.ms_setup, "ms_solve": st.ms_solve}
+        return {"it": st.it, "relres": st.relres, "ms_setup": st.ms_setup, "ms_solve": st.ms_solve,
+                "replacements": st.replacements}
 
     # -- reference entry points ------------------------------------------------
     def SetupGMG(self, xfil):
@@ -260,10 +264,18 @@ class Solver:
 
     def KelemProdMixed(self, x):
         """K(rho) x by the mixed V-cycle's finest operator (FP32 vectors, BF16
-        SIMP factors; tensor-core element matrices for MR factor 2)."""
+        SIMP factors; tensor-core sub-cell products when n * nely is even)."""
         x = np.ascontiguousarray(x, dtype=np.float64)
         y = np.empty_like(x)
         self._check(_lib.tosp_kelem_prod_mixed(self.h, _ptr(x), _ptr(y), x.size))
+        return y
+
+    def KelemProdCG32(self, x):
+        """K(rho) x by the CG's product of ``mg.cg_product = 1`` (tensor cores,
+        FP32 SIMP factors and vectors)."""
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        y = np.empty_like(x)
+        self._check(_lib.tosp_kelem_prod_cg32(self.h, _ptr(x), _ptr(y), x.size))
         return y
 
     def MGCycle(self, r):
