@@ -526,12 +526,14 @@ def profile_kernels(args):
     spec = WORKLOADS[args.workload]
     pb, n, xfil, spec = build_workload(args.workload, filter_fn=lambda x: x)
     mg = tosp.default_mg(ngrids=args.ngrids or spec["ngrids"], cycle=0, omega=spec["omega"], tolMG=1e-8,
-                         maxiterMG=1000, flexible=1)
+                         maxiterMG=1000, flexible=1, cg_product=args.cg_product)
     s = tosp.Solver(pb, mg, precision=tosp.PREC_MIXED, mr_n=n, p=3.0, emin=1e-9, opfilter=1, rmin=spec["rmin"])
     s.SetupGMG(xfil)
     r = np.random.default_rng(0).standard_normal(pb.freedofs.size)
     s.KelemProd(r)       # one FP64 product (the outer CG's operator)
     s.MGCycle(r)         # one V-cycle: two launches of the V-cycle's finest operator
+    if args.cg_product:
+        s.KelemProdCG32(r)   # one launch of the CG's tensor-core product
     if args.profile_solve:
         u, it, rr, rc = s.SolveMG(np.zeros(pb.f.size), pb.f)   # one full mixed solve
         print("solve iterations", it)

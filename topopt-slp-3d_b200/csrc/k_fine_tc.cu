@@ -379,7 +379,14 @@ __device__ __forceinline__ void stage_brick(int64_t brick, float *xs, WT *wslab,
 }
 
 // A tiles of this thread's element (row tid) from the staged nodal values;
-// returns 2^(E - 140), the inverse of the element's scale factor.
+// returns 2^(E - 140), the inverse of the element's scale factor.  SHIFT:
+// the element's mean translation (one value per component) is subtracted
+// first.  The blocks map a rigid translation to zero (in exact arithmetic), so
+// the product is unchanged, while the FP16 pieces, the truncation of the
+// blocks and the FP32 accumulation then err relative to the element's
+// deformation instead of its displacement, which for smooth fields is the
+// much smaller part.
+template <bool SHIFT>
 __device__ __forceinline__ float build_a(const float *xs, unsigned char *abuf, int ln0, int tid) {
     float u[24];
 #pragma unroll
@@ -389,6 +396,17 @@ __device__ __forceinline__ float build_a(const float *xs, unsigned char *abuf, i
         u[3 * a] = v.x;
         u[3 * a + 1] = v.y;
         u[3 * a + 2] = v.z;
+    }
+    if constexpr (SHIFT) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float t = 0.f;
+#pragma unroll
+            for (int a = 0; a < 8; ++a) t += u[3 * a + c];
+            t *= 0.125f;
+#pragma unroll
+            for (int a = 0; a < 8; ++a) u[3 * a + c] -= t;
+        }
     }
     float m = 0.f;
 #pragma unroll
@@ -491,7 +509,7 @@ k_fine_apply_tc(const float *__restrict__ x, float *__restrict__ y, const WT *__
         cp_async_commit();
         cp_async_wait_0();
         group_sync(grp);
-        fsc = build_a(xs, abuf, ln0, tid);
+        fsc = build_a<K::K3>(xs, abuf, ln0, tid);
         fence_async_smem();
         group_sync(grp);
         if (tid == 0) {
@@ -575,7 +593,7 @@ k_fine_apply_tc(const float *__restrict__ x, float *__restrict__ y, const WT *__
         cp_async_wait_0();
         group_sync(grp);
         if (next < fg.nbricks) {
-            fsc = build_a(xs, abuf, ln0, tid);
+            fsc = build_a<K::K3>(xs, abuf, ln0, tid);
             fence_async_smem();
         }
         group_sync(grp);
