@@ -101,14 +101,25 @@ typedef struct tosp_mg_params {
     int32_t cg_product;    /* product K d of the CG recurrence (I/SolveMG.m:37-38):
                               0: FP64 operator every iteration (default, the reference's PCG);
                               1 (TOSP_PREC_MIXED with the tensor-core operator, n * nely even):
-                              the tensor-core operator with FP32 SIMP factors (about 22
-                              significant bits), every CG vector, dot and update still FP64;
+                              the tensor-core operator with FP32 SIMP factors and the blocks
+                              in three FP16 pieces (about 1e-7 of |K||d|), every CG vector,
+                              dot and update still FP64;
                               the recurrence residual is replaced by the FP64 residual
                               f - K u (FP64 operator) whenever its norm has fallen by the
                               factor replace_drop since the last replacement, and before
                               convergence is accepted, so the tolerance holds for the true
                               residual.  Ignored by the serving loop.                          */
     double  replace_drop;  /* replacement factor of cg_product 1, in (0, 1); 0: 0.1            */
+    int32_t opchol;        /* mg.opchol: 0 (default) add grids while the coarsest system exceeds
+                              nmaxchol and solve it directly; 1 PCG on the coarsest grid
+                              (I/VCycle.m:28-35).  With 0, a coarsest system above nmaxchol
+                              on a mesh that cannot take another grid switches to 1, as
+                              I/StartStrSLP.m:122-132 does.                                  */
+    int32_t opcond;        /* mg.opcond, the coarsest PCG's preconditioner in the reference
+                              (0 diag, 1 ichol); the GPU PCG always uses the diagonal
+                              (Jacobi) preconditioner and stops on the same tolerance        */
+    double  tolPCG;        /* pcgp.tolPCG: the coarsest PCG's relative residual tolerance     */
+    int32_t maxiterPCG;    /* pcgp.maxiterPCG: its iteration cap                              */
 } tosp_mg_params;
 
 /* Statistics of the last tosp_solve_mg call. */

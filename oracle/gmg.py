@@ -80,15 +80,19 @@ def gmg_levels(nelx, nely, nelz, ngrids, nmaxchol=60000, opchol=0):
 class Hierarchy:
     """The cell arrays ``A, P, M`` and the coarse factor of I/SetupGMG.m."""
 
-    def __init__(self, A, P, Mdiag, chol, freedofs, omega):
+    def __init__(self, A, P, Mdiag, chol, freedofs, omega, pcg=None):
         self.A, self.P, self.Mdiag, self.chol = A, P, Mdiag, chol
         self.freedofs, self.omega = freedofs, omega
+        self.pcg = pcg   # (tolPCG, maxiterPCG) with opchol = 1, else None
 
 
-def setup_gmg(K, nelx, nely, nelz, freedofs, ngrids, omega):
-    """I/SetupGMG.m:16-77 with ``smoother = 0`` (Jacobi) and ``opchol = 0``.
+def setup_gmg(K, nelx, nely, nelz, freedofs, ngrids, omega, opchol=0, tolPCG=1e-8, maxiterPCG=10000):
+    """I/SetupGMG.m:16-77 with ``smoother = 0`` (Jacobi).
 
-    ``M{i} = (1/omega) diag(A{i})`` is kept as its diagonal.
+    ``M{i} = (1/omega) diag(A{i})`` is kept as its diagonal.  ``opchol = 1``
+    solves the coarsest grid by PCG with the diagonal preconditioner
+    (I/SetupGMG.m:52-57 with ``opcond = 0``, I/VCycle.m:28-35) instead of the
+    Cholesky factor.
     """
     nel = [(nelx // 2 ** i, nely // 2 ** i, nelz // 2 ** i) for i in range(ngrids)]
     fd = [np.asarray(freedofs)]
@@ -102,6 +106,8 @@ def setup_gmg(K, nelx, nely, nelz, freedofs, ngrids, omega):
     for i in range(1, ngrids):
         A.append((P[i - 1].T @ A[i - 1] @ P[i - 1]).tocsr())
     Mdiag = [A[i].diagonal() / omega for i in range(ngrids - 1)]
+    if opchol == 1:
+        return Hierarchy(A, P, Mdiag, None, fd, omega, pcg=(tolPCG, maxiterPCG))
     chol = sla.cho_factor(A[-1].toarray(), lower=False)
     return Hierarchy(A, P, Mdiag, chol, fd, omega)
 
@@ -114,8 +120,37 @@ def smooth(A, Mdiag, b, x0, niter):
     return x
 
 
+def pcg_diag(A, b, tol, maxit):
+    """MATLAB's ``pcg(A, b, tol, maxit, diag(diag(A)))`` from a zero iterate:
+    preconditioned CG, stopped once ||r|| <= tol ||b|| or after maxit
+    iterations (the last iterate is returned)."""
+    d = A.diagonal()
+    x = np.zeros(b.size)
+    nb = np.linalg.norm(b)
+    if nb == 0.0:
+        return x
+    r = b.copy()
+    p = r / d
+    rho = r @ p
+    for _ in range(maxit):
+        q = A @ p
+        alpha = rho / (p @ q)
+        x = x + alpha * p
+        r = r - alpha * q
+        if np.linalg.norm(r) <= tol * nb:
+            break
+        z = r / d
+        rho_new = r @ z
+        p = z + (rho_new / rho) * p
+        rho = rho_new
+    return x
+
+
 def coarse_solve(H, rH):
-    """``R\\(R'\\rH(perm))`` of I/VCycle.m:40 (dense Cholesky substitute)."""
+    """``R\\(R'\\rH(perm))`` of I/VCycle.m:40 (dense Cholesky substitute), or
+    with ``opchol = 1`` the coarsest PCG of I/VCycle.m:28-35."""
+    if H.pcg is not None:
+        return pcg_diag(H.A[-1], rH, H.pcg[0], H.pcg[1])
     return sla.cho_solve(H.chol, rH)
 
 

@@ -319,3 +319,52 @@ def test_coarsest_above_dense_limit_adds_a_grid(tosp_mod):
     s.SetupGMG(np.full(pb.nelem, 0.4))
     u, it, rr, rc = s.SolveMG(np.zeros(pb.f.size), pb.f)
     assert rc == 0 and rr <= 1e-8
+
+
+@pytest.mark.parametrize("prec", [0, 1])
+@pytest.mark.parametrize("cycle", [0, 1, 2])
+def test_coarsest_pcg_matches_direct_solve(tosp_mod, prec, cycle):
+    """mg.opchol = 1: PCG on the coarsest grid (I/VCycle.m:28-35) to tolPCG =
+    1e-8 instead of the direct solve.  The cycle output differs from the
+    direct solve's by the PCG tolerance, so the solve takes the same
+    iterations (within one), reaches the tolerance in the true residual and
+    the compliance agrees to 1e-9."""
+    pb = P.cantilever(32, 16, 16)
+    dens = make(pb, 2, seed=21)
+    ks = fem.elem_stiff_gqmr(pb.el, pb.eh, pb.ew, pb.nu, 2)
+    K = fem.global_stiff_matrix(pb.nelx, pb.nely, pb.nelz, ks, dens, P_SIMP, EMIN, pb.freedofs)
+    res = {}
+    for opchol in (0, 1):
+        s = solver(tosp_mod, pb, 2, prec=prec, cycle=cycle, omega=0.5, flexible=1, opchol=opchol)
+        assert s.info()["ngrids"] == 3
+        s.SetupGMG(dens)
+        u, it, rr, rc = s.SolveMG(np.zeros(pb.f.size), pb.f)
+        s.close()
+        assert rc == 0
+        assert np.linalg.norm(pb.f - K @ u) <= 1.0001e-8 * np.linalg.norm(pb.f)
+        res[opchol] = (it, pb.f @ u)
+    assert abs(res[1][0] - res[0][0]) <= 1, res
+    assert abs(res[1][1] - res[0][1]) <= 1e-9 * abs(res[0][1])
+
+
+def test_level_rule_switches_to_coarsest_pcg(tosp_mod):
+    """The reference's level rule (I/StartStrSLP.m:122-132): the coarsest
+    system of 20x10x10 with 2 grids (1 188 dofs) exceeds nmaxchol = 500 and
+    the mesh cannot take a third grid (10 is not a multiple of 4), so the
+    coarsest grid is solved by PCG.  The solve matches the oracle's 2-grid
+    solve with the same coarsest PCG (diagonal preconditioner, tolPCG 1e-8):
+    iterations within one, compliance to 1e-9, true residual <= 1e-8."""
+    pb = P.cantilever(20, 10, 10)
+    dens = make(pb, 1, seed=4)
+    ks = fem.elem_stiff_gqmr(pb.el, pb.eh, pb.ew, pb.nu, 1)
+    K = fem.global_stiff_matrix(pb.nelx, pb.nely, pb.nelz, ks, dens, P_SIMP, EMIN, pb.freedofs)
+    H = gmg.setup_gmg(K, pb.nelx, pb.nely, pb.nelz, pb.freedofs, 2, 0.5, opchol=1)
+    uo, ito = gmg.solve_mg(H, np.zeros(pb.f.size), pb.f, 0, 1, 1, 1e-8, 500)
+    s = solver(tosp_mod, pb, 1, ngrids=2, nmaxchol=500, omega=0.5)
+    assert s.info()["ngrids"] == 2
+    s.SetupGMG(dens)
+    u, it, rr, rc = s.SolveMG(np.zeros(pb.f.size), pb.f)
+    s.close()
+    assert rc == 0 and abs(it - ito) <= 1, (it, ito)
+    assert np.linalg.norm(pb.f - K @ u) <= 1.0001e-8 * np.linalg.norm(pb.f)
+    assert abs(pb.f @ u - pb.f @ uo) <= 1e-9 * abs(pb.f @ uo)

@@ -122,3 +122,25 @@ def test_grad_finite_difference():
         h = 1e-6
         fd = (compliance(dens + h * I[i])[0] - compliance(dens - h * I[i])[0]) / (2 * h)
         assert abs(fd - g0[i]) <= 1e-5 * abs(g0[i]) + 1e-12
+
+
+def test_coarsest_pcg_branch_matches_direct_solve():
+    """The oracle's opchol = 1 branch (I/VCycle.m:28-35: pcg with the diagonal
+    preconditioner to tolPCG = 1e-8) gives the direct solve's cycle to within
+    the PCG tolerance, and tighter as the tolerance shrinks."""
+    import numpy as np
+    from oracle import fem, gmg
+    from tosp import problems as P
+    pb = P.cantilever(12, 6, 6)
+    dens = np.random.default_rng(3).uniform(0.001, 1, pb.nelem)
+    ks = fem.elem_stiff_gqmr(pb.el, pb.eh, pb.ew, pb.nu, 1)
+    K = fem.global_stiff_matrix(pb.nelx, pb.nely, pb.nelz, ks, dens, 3.0, 1e-9, pb.freedofs)
+    r = np.random.default_rng(5).standard_normal(pb.freedofs.size)
+    Hd = gmg.setup_gmg(K, pb.nelx, pb.nely, pb.nelz, pb.freedofs, 2, 0.5)
+    zd = gmg.precondition(Hd, r, 0, 1, 1)
+    errs = []
+    for tol in (1e-6, 1e-10):
+        Hp = gmg.setup_gmg(K, pb.nelx, pb.nely, pb.nelz, pb.freedofs, 2, 0.5, opchol=1, tolPCG=tol)
+        zp = gmg.precondition(Hp, r, 0, 1, 1)
+        errs.append(np.abs(zp - zd).max() / np.abs(zd).max())
+    assert errs[1] <= 1e-7 and errs[1] < errs[0]

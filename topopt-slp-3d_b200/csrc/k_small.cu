@@ -18,6 +18,7 @@
 // and every block leaves the step loop.  The poll limit and one block that
 // skips its first arrival can be set from the host (tosp_inject_wait_fault),
 // so tests make the wait run out without faulting or hanging the GPU.
+#include "grid_sync.cuh"
 #include "tosp_internal.h"
 
 namespace tosp {
@@ -32,46 +33,6 @@ __device__ __forceinline__ void small_node_xyz(int64_t I, int ny, int nx, int &x
     y = i - q * ny;
     z = q / nx;
     x = q - z * nx;
-}
-
-__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
-    unsigned v;
-    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-    return v;
-}
-
-// Grid-wide barrier over the co-resident blocks of a cooperative launch.
-// limit: polls before the wait gives up; skip: this block does not arrive
-// (a fault injected by tests: the other blocks' waits then run out).
-__device__ __forceinline__ bool grid_barrier(GridBarrier *bar, unsigned nblocks, uint32_t limit, bool skip) {
-    __shared__ int s_ok;
-    __syncthreads();
-    if (threadIdx.x == 0 && skip) {
-        s_ok = 1;
-    } else if (threadIdx.x == 0) {
-        int ok = 1;
-        const unsigned g = ld_acquire(&bar->gen);
-        __threadfence();
-        if (atomicAdd(&bar->count, 1u) == nblocks - 1) {
-            atomicExch(&bar->count, 0u);
-            __threadfence();
-            atomicAdd(&bar->gen, 1u);
-        } else {
-            uint32_t it = 0;
-            while (ld_acquire(&bar->gen) == g) {
-                if (++it >= limit) {
-                    atomicExch(&bar->err, 1);
-                    ok = 0;
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-        s_ok = ok;
-    }
-    __syncthreads();
-    return s_ok != 0;
 }
 
 template <typename T>

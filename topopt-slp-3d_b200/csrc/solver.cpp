@@ -79,6 +79,11 @@ struct tosp_handle {
     double *d_diag64 = nullptr;     // diag of the finest operator
     double *d_Adense = nullptr, *d_sweepC = nullptr, *d_pinv = nullptr;   // coarsest: A, then A^{-1}
     int64_t ncoarse = 0, npad = 0;
+    // coarsest grid by PCG (mg.opchol = 1 or the level rule's switch): FP64
+    // node-major stencil, 1 / diag and the kernel's work buffers
+    bool coarse_pcg = false;
+    double *d_cst = nullptr, *d_cinvd = nullptr;
+    CoarsePcgWork cpw;
     int *d_info = nullptr;
     bool setup_done = false;
     // persistent small-level cycle: first level it covers (-1: off), its grid
@@ -211,35 +216,32 @@ int sync(tosp_handle *h) {
 // (npad^2 doubles, 4.8 GB here) is applied as one GEMV per cycle.
 constexpr int DENSE_MAX = 24576;
 
-// The reference adds grids while the coarsest system exceeds nmaxchol
-// (opchol = 0).  The same rule runs here against min(nmaxchol, DENSE_MAX): a
-// coarsest system between DENSE_MAX and nmaxchol, which the reference would
-// factor with sparse Cholesky, gets one more grid instead.
-int choose_levels(int nelx, int nely, int nelz, int ngrids, int nmaxchol, std::string &msg) {
+// The reference's level rule (I/StartStrSLP.m:122-132): with opchol = 0,
+// grids are added while the coarsest system exceeds nmaxchol, and a mesh that
+// cannot take another grid switches to PCG on the coarsest grid (pcg = true).
+// The direct solve here is an explicit dense inverse of at most DENSE_MAX
+// dofs, so a coarsest system between DENSE_MAX and nmaxchol, which the
+// reference would factor with sparse Cholesky, gets one more grid when the
+// mesh allows it and PCG otherwise.  opchol = 1 keeps ngrids and uses PCG.
+int choose_levels(int nelx, int nely, int nelz, int ngrids, int nmaxchol, int opchol, bool &pcg, std::string &msg) {
     const int cap = nmaxchol < DENSE_MAX ? nmaxchol : DENSE_MAX;
     auto divisible = [&](int k) {
         const int m = 1 << (k - 1);
         return nelx % m == 0 && nely % m == 0 && nelz % m == 0;
     };
+    pcg = opchol == 1;
     int ng = ngrids < 2 ? 2 : ngrids;
     while (ng >= 2 && !divisible(ng)) --ng;
     if (ng < 2) {
         msg = "geometric multigrid needs even element counts (the reference falls back to AMG, not provided)";
         return -1;
     }
-    for (;;) {
+    while (!pcg) {
         const double m = (double)(1 << (ng - 1));
         const double nc = (nelx / m + 1) * (nely / m + 1) * (nelz / m + 1) * 3;
         if (nc <= cap) break;
         if (divisible(ng + 1)) ++ng;
-        else {
-            msg = nc <= nmaxchol
-                      ? "coarsest system of " + std::to_string((long long)nc) + " dofs exceeds the dense direct "
-                        "solve's " + std::to_string(DENSE_MAX) + " and no further level is possible"
-                      : "coarsest system larger than nmaxchol and no further level possible "
-                        "(the reference switches to PCG on the coarsest grid, not provided)";
-            return -1;
-        }
+        else pcg = true;
     }
     return ng;
 }
@@ -329,6 +331,12 @@ int residual(tosp_handle *h, int l) {
 template <typename T>
 int coarse_solve(tosp_handle *h) {
     Level &C = h->lev[h->ngrids - 1];
+    if (h->coarse_pcg) {
+        launch_coarse_pcg<T>(h->d_cst, h->d_cinvd, (const T *)C.b, (T *)C.x, C.g, h->cpw, h->mg.tolPCG,
+                             h->mg.maxiterPCG, h->stream);
+        CKL();
+        return TOSP_OK;
+    }
     launch_dense_solve<T>(h->d_Adense, (const T *)C.b, (T *)C.x, C.g.ndof, h->npad, h->stream);
     CKL();
     return TOSP_OK;
@@ -452,7 +460,7 @@ int build_small(tosp_handle *h) {
     h->small_built = true;
     h->small_l = -1;
     const int Lc = h->ngrids - 1;
-    if (!h->mg_ok || h->mg.cycle == 2 || h->mg.small_cycle_max <= 0 || Lc < 2) return TOSP_OK;
+    if (!h->mg_ok || h->mg.cycle == 2 || h->mg.small_cycle_max <= 0 || Lc < 2 || h->coarse_pcg) return TOSP_OK;
     const int64_t smax = h->mg.small_cycle_max;
     int ls = -1;
     for (int l = 1; l < Lc; ++l)
@@ -738,8 +746,13 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
     h->mg = *mg;
     if (h->mg.replace_drop == 0.0) h->mg.replace_drop = 0.1;
     h->cg32 = mg->cg_product == 1;
+    if (mg->opchol < 0 || mg->opchol > 1 || !(mg->tolPCG > 0) || mg->maxiterPCG < 1) {
+        h->err = "opchol must be 0 or 1, tolPCG > 0 and maxiterPCG >= 1";
+        return TOSP_ERR_BAD_ARG;
+    }
     std::string msg;
-    int ng = choose_levels(pb->nelx, pb->nely, pb->nelz, mg->ngrids, mg->nmaxchol, msg);
+    bool cpcg = false;
+    int ng = choose_levels(pb->nelx, pb->nely, pb->nelz, mg->ngrids, mg->nmaxchol, mg->opchol, cpcg, msg);
     if (ng < 0) {
         // the operator, Grad and the filter still work; SolveMG/cycles report why not
         h->mg_ok = false;
@@ -761,7 +774,8 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
     fg.nbricks = (int64_t)fg.nbx * fg.nby * fg.nbz;
     h->dens = make_grid(pb->nelx * h->n, pb->nely * h->n, pb->nelz * h->n);
     h->ncoarse = h->mg_ok ? h->lev[ng - 1].g.ndof : 0;
-    h->npad = (h->ncoarse + 31) / 32 * 32;
+    h->coarse_pcg = h->mg_ok && cpcg;
+    h->npad = h->coarse_pcg ? 0 : (h->ncoarse + 31) / 32 * 32;
     if (h->npad > DENSE_MAX) {
         h->err = "coarsest system too large for the dense direct solve: " + std::to_string(h->ncoarse) +
                  " dofs; use more grids";
@@ -829,7 +843,21 @@ int create_impl(tosp_handle *h, const tosp_problem *pb, const tosp_mg_params *mg
         }
     }
     TRY(dalloc(h, &h->d_diag64, g0.ndof));
-    if (h->mg_ok) {
+    if (h->mg_ok && h->coarse_pcg) {
+        const Grid &gc = h->lev[ng - 1].g;
+        CoarsePcgWork &w = h->cpw;
+        TRY(dalloc(h, &h->d_cst, gc.nnodes * STENCIL_VALS));
+        TRY(dalloc(h, &h->d_cinvd, gc.ndof));
+        TRY(dalloc(h, &w.x, gc.ndof));
+        TRY(dalloc(h, &w.r, gc.ndof));
+        TRY(dalloc(h, &w.p, gc.ndof));
+        TRY(dalloc(h, &w.q, gc.ndof));
+        w.max_blocks = coarse_pcg_max_blocks();
+        TRY(dalloc(h, &w.part, 3 * (int64_t)w.max_blocks));
+        TRY(dalloc(h, &w.bar, 1));
+        CK(cudaMemset(w.bar, 0, sizeof(GridBarrier)));
+        TRY(dalloc(h, &w.iters, 1));
+    } else if (h->mg_ok) {
         TRY(dalloc(h, &h->d_Adense, h->npad * h->npad));
         TRY(dalloc(h, &h->d_sweepC, h->npad * 32));
         TRY(dalloc(h, &h->d_pinv, 32 * 32));
@@ -946,6 +974,14 @@ int setup_levels(tosp_handle *h) {
         CKL();
     }
     Level &C = h->lev[ng - 1];
+    if (h->coarse_pcg) {
+        // the coarsest operator as an FP64 stencil and 1 / diag for the PCG
+        CK(cudaMemsetAsync(h->d_info, 0, sizeof(int), h->stream));
+        launch_assemble_stencil<double>(C.Ae, C.fm, C.g, h->d_cst, h->d_cinvd, 1.0, true, h->stream);
+        CKL();
+        if (!h->small_built) TRY(build_small<T>(h));
+        return sync(h);
+    }
     launch_dense_assemble(C.Ae, C.fm, C.g, h->d_Adense, h->npad, h->stream);
     CKL();
     dense_sweep_inverse(h->d_Adense, h->d_sweepC, h->d_pinv, h->npad, h->d_info, h->stream);
@@ -980,6 +1016,15 @@ int need_mg(tosp_handle *h) {
 // Reads (and clears) the tensor-core operator's timeout flag; call after a
 // stream synchronisation.
 int check_tc(tosp_handle *h) {
+    if (h->cpw.bar) {
+        GridBarrier b{};
+        CK(cudaMemcpy(&b, h->cpw.bar, sizeof b, cudaMemcpyDeviceToHost));
+        if (b.err) {
+            CK(cudaMemset(h->cpw.bar, 0, sizeof b));
+            h->err = "coarsest-grid PCG: grid barrier wait timed out";
+            return TOSP_ERR_TIMEOUT;
+        }
+    }
     if (h->d_bar) {
         GridBarrier b{};
         CK(cudaMemcpy(&b, h->d_bar, sizeof b, cudaMemcpyDeviceToHost));
@@ -1473,6 +1518,10 @@ void tosp_default_mg_params(tosp_mg_params *mg) {
     mg->small_cycle_max = 0;
     mg->cg_product = 0;
     mg->replace_drop = 0.1;
+    mg->opchol = 0;
+    mg->opcond = 1;
+    mg->tolPCG = 1e-8;
+    mg->maxiterPCG = 10000;
 }
 
 int tosp_create(const tosp_problem *prob, const tosp_mg_params *mg, int32_t precision, tosp_handle **out) {

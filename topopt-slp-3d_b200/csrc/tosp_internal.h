@@ -225,6 +225,21 @@ struct GridBarrier {
     int skip;         // k > 0: block k - 1 skips its first arrival (fault injection for tests)
     int pad;
 };
+// Work buffers of the coarsest-grid PCG (mg.opchol = 1, k_coarse_pcg.cu):
+// FP64 vectors of the coarsest level, 3 * max_blocks partial sums, the grid
+// barrier and the iteration count of the last solve.
+struct CoarsePcgWork {
+    double *x = nullptr, *r = nullptr, *p = nullptr, *q = nullptr, *part = nullptr;
+    GridBarrier *bar = nullptr;
+    int *iters = nullptr;
+    int max_blocks = 0;
+};
+// y = pcg(A_c, b) on the coarsest grid: A_c as the FP64 node-major stencil,
+// invd = 1 / diag(A_c) (0 on fixed dofs), stop at ||r|| <= tol ||b|| or maxit.
+template <typename T>
+void launch_coarse_pcg(const double *st, const double *invd, const T *b, T *x, const Grid &g, CoarsePcgWork &w,
+                       double tol, int maxit, cudaStream_t stream);
+int coarse_pcg_max_blocks();
 // One member of a batched small-level cycle: its step list (SmallStep of the
 // cycle precision), and the blocks of the launch that run it.
 struct SmallBatchEntry {

@@ -52,7 +52,8 @@ class MgParams(C.Structure):
                 ("smoothiter1", C.c_int32), ("smoothiter2", C.c_int32), ("tolMG", C.c_double),
                 ("maxiterMG", C.c_int32), ("nmaxchol", C.c_int32), ("flexible", C.c_int32),
                 ("maxstall", C.c_int32), ("warp_stencil_max", C.c_int32), ("small_cycle_max", C.c_int32),
-                ("cg_product", C.c_int32), ("replace_drop", C.c_double)]
+                ("cg_product", C.c_int32), ("replace_drop", C.c_double),
+                ("opchol", C.c_int32), ("opcond", C.c_int32), ("tolPCG", C.c_double), ("maxiterPCG", C.c_int32)]
 
 
 class RequestStats(C.Structure):
