@@ -357,7 +357,7 @@ def run_serving(args):
         pb, n, x, ng = item
         # cycle and omega unspecified for the stream: the reference defaults
         mg = tosp.default_mg(ngrids=ng, cycle=1, omega=W.REF_OMEGA, tolMG=1e-8, maxiterMG=1000, flexible=1,
-                             maxstall=60, small_cycle_max=args.small_levels)
+                             maxstall=60, small_cycle_max=args.small_levels, cg_product=args.cg_product)
         return srv.submit(pb, x, mg=mg, precision=tosp.PREC_MIXED, mr_n=n, p=3.0, emin=1e-9, opfilter=1,
                           rmin=1.0 if n > 1 else 1.5)
 
@@ -369,7 +369,7 @@ def run_serving(args):
         if k not in seen:
             pb, n, x, ng = it
             mg = tosp.default_mg(ngrids=ng, cycle=1, omega=W.REF_OMEGA, tolMG=1e-8, maxiterMG=1000, flexible=1,
-                                 maxstall=60, small_cycle_max=args.small_levels)
+                                 maxstall=60, small_cycle_max=args.small_levels, cg_product=args.cg_product)
             if args.prepare > 0:
                 srv.prepare(pb, count=args.prepare, mg=mg, precision=tosp.PREC_MIXED, mr_n=n,
                             rmin=1.0 if n > 1 else 1.5)
@@ -415,6 +415,7 @@ def run_serving(args):
             "data": "synthetic", "dtype": "f64 outer CG / f32+bf16 V-cycle",
             "config": {"workload": "serving stream seed 7", "requests": len(items), "slots": args.slots,
                        "hbm_budget_gb": args.budget_gb, "small_levels": args.small_levels,
+                       "cg_product": args.cg_product,
                        "mesh_nx": list(W.SERVING_NX), "mr_n": [1, 2],
                        "cycle": "W", "omega": W.REF_OMEGA,
                        "bc": list(W.SERVING_BC)},

@@ -108,7 +108,7 @@ typedef struct tosp_mg_params {
                               f - K u (FP64 operator) whenever its norm has fallen by the
                               factor replace_drop since the last replacement, and before
                               convergence is accepted, so the tolerance holds for the true
-                              residual.  Ignored by the serving loop.                          */
+                              residual.  Served FP64 requests ignore it.                       */
     double  replace_drop;  /* replacement factor of cg_product 1, in (0, 1); 0: 0.1            */
     int32_t opchol;        /* mg.opchol: 0 (default) add grids while the coarsest system exceeds
                               nmaxchol and solve it directly; 1 PCG on the coarsest grid

@@ -95,20 +95,22 @@ def test_admission_by_budget_and_cancel(tosp_mod):
 
 
 @pytest.mark.parametrize("small", [0, 65536])
-@pytest.mark.parametrize("precision", [0, 1])
-def test_batched_requests_match_standalone_solves(tosp_mod, precision, small):
+@pytest.mark.parametrize("precision,cgp", [(0, 0), (1, 0), (1, 1)])
+def test_batched_requests_match_standalone_solves(tosp_mod, precision, cgp, small):
     """Requests of one shape in flight together run as one batch, one CG
     iteration per tick; with mg.small_cycle_max > 0 every visit to the small
-    levels is one persistent launch for all of them.  Supports, loads and
-    densities differ between members; each result equals the standalone solve
-    of its request (same parameters) to the solve tolerance."""
+    levels is one persistent launch for all of them; with mg.cg_product = 1
+    the runner replaces each member's residual after its tick.  Supports,
+    loads and densities differ between members; each result equals the
+    standalone solve of its request (same parameters) to the solve
+    tolerance."""
     pool = W.FieldPool(seed=5)
     items = []
     for k, bc in enumerate(("cantilever", "bridge", "torsion", "cantilever", "bridge", "torsion")):
         pb = W.serving_problem(32, bc)
         items.append((pb, pool.field(32, 1, k % 3, 0.45 + 0.02 * k)))
     mg = tosp_mod.default_mg(ngrids=3, cycle=1, omega=0.5, tolMG=1e-8, maxiterMG=1000, flexible=1,
-                             small_cycle_max=small)
+                             small_cycle_max=small, cg_product=cgp)
     srv = tosp_mod.Server(max_slots=6, hbm_budget_bytes=8 << 30)
     srv.prepare(items[0][0], count=6, mg=mg, precision=precision)
     ids = [srv.submit(pb, x, mg=mg, precision=precision, mr_n=1, p=3.0, emin=1e-9, rmin=1.5) for pb, x in items]

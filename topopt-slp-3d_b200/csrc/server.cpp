@@ -94,14 +94,15 @@ std::string shape_key(const Request &r) {
     return k;
 }
 
-// Multigrid parameters of a served request: as submitted, except cg_product
-// (batched iterations keep the FP64 product every iteration; the residual
-// replacements of cg_product 1 are per-solve host decisions).  A request with
-// mg.small_cycle_max > 0 runs its small levels as the persistent cycle, which
-// the batch runner launches once per visit for all same-shape requests.
-tosp_mg_params serving_mg(const tosp_mg_params &mg) {
+// Multigrid parameters of a served request: as submitted, except that only
+// mixed-precision requests keep mg.cg_product (the tensor-core CG product
+// with residual replacement; the batch runner replaces residuals per member
+// after each tick).  A request with mg.small_cycle_max > 0 runs its small
+// levels as the persistent cycle, which the batch runner launches once per
+// visit for all same-shape requests.
+tosp_mg_params serving_mg(const tosp_mg_params &mg, int precision) {
     tosp_mg_params m = mg;
-    m.cg_product = 0;
+    if (precision != TOSP_PREC_MIXED) m.cg_product = 0;
     return m;
 }
 
@@ -380,6 +381,7 @@ void worker_main(tosp_server *s) {
                 r->fallbacks = 1;
                 r->precision = TOSP_PREC_FP64;
                 r->mg.maxstall = 0;
+                r->mg.cg_product = 0;
                 r->u0.clear();
                 bool finite = !r->u.empty();
                 for (double v : r->u) finite = finite && std::isfinite(v);
@@ -468,8 +470,10 @@ void batch_main(tosp_server *s, Batch *b) {
                     r->solve_failed = true;
                     r->status = TOSP_ERR_TIMEOUT;
                     r->err = "batched small-level cycle: grid barrier wait timed out";
-                } else {
-                    tosp::solve_step_account(r->h);
+                } else if (tosp::solve_step_account(r->h) != TOSP_OK) {
+                    r->solve_failed = true;
+                    r->status = TOSP_ERR_CUDA;
+                    r->err = tosp_last_error(r->h);
                 }
             }
             s->batched_iterations += (int64_t)b->mem.size();
@@ -540,7 +544,7 @@ int tosp_server_prepare(tosp_server *s, const tosp_problem *pb, const tosp_mg_pa
     r.pb.freedofs = nullptr;
     r.pb.fixed_dens = nullptr;
     r.pb.free_dens_g = nullptr;
-    r.mg = serving_mg(*mg);
+    r.mg = serving_mg(*mg, precision);
     r.precision = precision;
     r.key = shape_key(r);
     r.est_bytes = estimate_bytes(r);
@@ -584,7 +588,7 @@ int tosp_server_submit(tosp_server *s, const tosp_problem *pb, const tosp_mg_par
     r->pb.freedofs = nullptr;
     r->pb.fixed_dens = nullptr;
     r->pb.free_dens_g = nullptr;
-    r->mg = serving_mg(*mg);
+    r->mg = serving_mg(*mg, precision);
     r->precision = precision;
     r->xfil.assign(xfil, xfil + ndens);
     r->f.assign(f, f + nfree);

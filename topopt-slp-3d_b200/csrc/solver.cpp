@@ -1314,13 +1314,16 @@ int tosp::solve_start(tosp_handle *h, const double *x, const double *f) {
     return TOSP_OK;
 }
 
-void tosp::solve_step_account(tosp_handle *h) { solve_account(h); }
+int tosp::solve_step_account(tosp_handle *h) {
+    solve_account(h);
+    return replace_residual(h);
+}
 
 int tosp::solve_step(tosp_handle *h) {
     TRY(solve_launch_iteration(h));
     TRY(sync(h));
     solve_account(h);
-    return TOSP_OK;
+    return replace_residual(h);
 }
 
 const SolveState &tosp::solve_state(const tosp_handle *h) { return h->st; }

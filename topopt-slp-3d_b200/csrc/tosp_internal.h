@@ -308,7 +308,8 @@ struct SolveState {
 // Serving-loop batches (solver.cpp): a solve's steps, and one CG iteration of
 // several handles of one shape captured as a single graph.
 int solve_start(tosp_handle *h, const double *x, const double *f);   // loads, r, norms, first iteration
-void solve_step_account(tosp_handle *h);                              // after a batch iteration's sync
+int solve_step_account(tosp_handle *h);                               // after a batch iteration's sync
+                                                                      // (and the residual replacement)
 int solve_step(tosp_handle *h);                                       // one iteration on the handle's stream
 const SolveState &solve_state(const tosp_handle *h);
 int solve_stop(tosp_handle *h, double *x, int32_t *it, double *relres);  // final update, x to the host
