@@ -255,7 +255,8 @@ def run_slp(args):
     iters = args.slp_iters or iters
     lp = args.lp or lp
     mg = tosp.default_mg(ngrids=ngr, cycle=cycle, omega=omega, smoothiter1=1, smoothiter2=1, tolMG=1e-8,
-                         maxiterMG=2000, flexible=1 if prec == tosp.PREC_MIXED else 0)
+                         maxiterMG=2000, flexible=1 if prec == tosp.PREC_MIXED else 0,
+                         cg_product=args.cg_product if prec == tosp.PREC_MIXED else 0)
     if prec == tosp.PREC_MIXED:
         # high-contrast designs defeat the FP32 V-cycle: stalled mixed solves
         # are finished in FP64, which then serves the rest of the loop
@@ -279,7 +280,8 @@ def run_slp(args):
             "unit": "s/iteration", "higher_is_better": False, "n_gpus": 1, "data": "synthetic",
             "dtype": "f64" if prec == tosp.PREC_FP64 else "f64 outer CG / f32+bf16 V-cycle",
             "config": {"workload": args.slp, "mesh": [pb.nelx, pb.nely, pb.nelz], "mr_n": n, "volfrac": volfrac,
-                       "rmin": rmin, "lp": lp, "ngrids": ngr, "cycle": "VW"[cycle], "omega": omega},
+                       "rmin": rmin, "lp": lp, "ngrids": ngr, "cycle": "VW"[cycle], "omega": omega,
+                       "cg_product": int(mg.cg_product)},
             "slp": {"accepted": res.iters, "rejected": res.rejected, "opstop": res.opstop, "F_final": res.F,
                     "F_first": res.history[0]["F"] if res.history else None,
                     "pcg_iterations_total": int(sum(res.pcgit)), "pcg_iterations": [int(i) for i in res.pcgit],

@@ -357,6 +357,7 @@ class FallbackSolver:
         mg64 = MgParams.from_buffer_copy(mg)
         mg64.maxstall = 0
         mg64.flexible = 0
+        mg64.cg_product = 0      # the FP64 handle's CG product is FP64
         self._args = dict(mr_n=mr_n, p=p, emin=emin, opfilter=opfilter, rmin=rmin, **kw)
         self.pb, self._mg64, self.sticky = pb, mg64, sticky
         self.mixed = Solver(pb, mgm, precision=PREC_MIXED, **self._args)
