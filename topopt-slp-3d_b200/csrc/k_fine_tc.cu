@@ -57,11 +57,12 @@
 // y of 8n BF16 values copied in 4-byte pieces), which needs n * nely even; the
 // host uses the CUDA-core kernel otherwise.
 //
-// The same kernel with FP32 factors (one cell per 4-byte piece) and the blocks
-// in three FP16 pieces (two more MMA steps, hi + mid + lo against u_hi) is the
-// product of the FP64 CG recurrence when the caller asks for it (cg_product 1).
-// Its larger B image is shared by four bricks per CTA at one CTA per SM (one
-// brick for n = 3), which keeps 16 warps per SM for n = 1, 2.
+// The same kernel with FP32 factors (one cell per 4-byte piece), the element's
+// mean translation subtracted from u_e and, for n = 1, 2, the blocks in three
+// FP16 pieces (eight MMA steps) is the product of the FP64 CG recurrence when
+// the caller asks for it (cg_product 1).  Its larger B image is shared by four
+// bricks per CTA at one CTA per SM, which keeps 16 warps per SM; for n = 3 it
+// keeps the two-piece image at two bricks per CTA.
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
@@ -100,10 +101,13 @@ struct Tc {
     static constexpr int COLS = 2 * CH;                   // tensor-memory columns per CTA
     static constexpr int B_TILE = NPAD / 8 * TC_GROUP;    // bytes of one B step
     // blocks in two FP16 pieces (hi + mid, five MMA steps) for the V-cycle's
-    // BF16-factor kernel, three (hi + mid + lo, eight steps) for the CG's
-    // FP32-factor kernel
+    // BF16-factor kernel; the CG's FP32-factor kernel takes three (hi + mid +
+    // lo, eight steps) for n = 1, 2 and two for n = 3, whose three-piece image
+    // (166 KB) would leave room for one brick per SM (measured on the MR-3
+    // bridge: two pieces at two bricks per CTA, 0.157 ms per launch and a
+    // 14 % faster V-cycle solve for the same 124 iterations, against 0.287 ms)
     static constexpr bool K3 = sizeof(WT) == 4;
-    static constexpr int B_STEPS = K3 ? 8 : 5;
+    static constexpr int B_STEPS = K3 && N != 3 ? 8 : 5;
     static constexpr int B_BYTES = B_STEPS * B_TILE;
     static constexpr int WY = BY * N, WX = BX * N, WZ = BZ * N;   // factor slab (density cells)
     static constexpr int CPP = 4 / (int)sizeof(WT);       // cells per 4-byte piece
@@ -112,7 +116,7 @@ struct Tc {
     // bricks processed side by side by one CTA, sharing the B image: four
     // warps each, their own A tiles, staging, outputs, barriers and
     // tensor-memory columns
-    static constexpr int NB = K3 ? (N == 3 ? 1 : 4) : (N == 3 ? 3 : 2);
+    static constexpr int NB = K3 ? (N == 3 ? 2 : 4) : (N == 3 ? 3 : 2);
     static constexpr int THREADS = NB * BRICK_ELEMS;
     static constexpr int TMEM_COLS = NB * COLS <= 64 ? 64 : (NB * COLS <= 128 ? 128 : (NB * COLS <= 256 ? 256 : 512));
     // layout: B image, slot table, then one region per brick
@@ -631,8 +635,9 @@ k_fine_apply_tc(const float *__restrict__ x, float *__restrict__ y, const WT *__
 // to the largest; that truncation, and the dropped u_lo * mid product, change
 // the operator by about 2^-22 |KE| |u_e|, which slows a CG whose recurrence
 // uses it (110 -> 173 iterations on the 192 x 96 x 96 MR-2 workload; the
-// V-cycle tolerates it), so the CG's kernel takes three pieces and five
-// products (hi*hi, lo*hi, hi*mid, lo*mid, hi*lo).
+// V-cycle tolerates it), so the CG's kernel for n = 1, 2 takes three pieces
+// and five products (hi*hi, lo*hi, hi*mid, lo*mid, hi*lo); for n = 3 the
+// two-piece image with the translation removed costs fewer solve seconds.
 static uint16_t f16_bits(float v) {
     const __half h = __float2half_rn(v);
     uint16_t b;
@@ -670,7 +675,7 @@ static void tc_image(const std::vector<double> &packed_rowmajor, std::vector<uin
             else put(1, r, j - 16, hi);
             if (j < 8) put(1, r, j + 8, hi);
             else put(2, r, j - 8, hi);
-            if (!K::K3) {
+            if (K::B_STEPS == 5) {
                 if (j < 16) put(3, r, j, mid);
                 else put(4, r, j - 16, mid);
             } else {
