@@ -69,7 +69,7 @@ def test_cg32_operator_parity(tosp_mod, dims, n):
 
 @pytest.mark.parametrize("dims,n,seed", [((16, 8, 8), 2, 0), ((16, 8, 8), 2, 13), ((24, 12, 12), 1, 3),
                                          ((8, 6, 4), 3, 2)])
-@pytest.mark.parametrize("cycle", [0, 1])
+@pytest.mark.parametrize("cycle", [0, 1, 2])
 def test_cg32_solve(tosp_mod, dims, n, seed, cycle):
     pb = P.cantilever(*dims)
     dens = make(pb, n, seed=seed)
@@ -117,3 +117,26 @@ def test_cg32_refusals(tosp_mod):
         s.KelemProdCG32(np.ones(pb.freedofs.size))
     assert e.value.code == -6
     s.close()
+
+
+def test_cg32_cap_and_warm_start(tosp_mod):
+    """At the iteration cap the solve ends with TOSP_NOT_CONVERGED and reports
+    the true residual of its iterate (a replacement runs at the end); a warm
+    start from that iterate then converges with the true residual <= tolMG."""
+    pb = P.cantilever(16, 8, 8)
+    dens = make(pb, 2, seed=3)
+    ks = fem.elem_stiff_gqmr(pb.el, pb.eh, pb.ew, pb.nu, 2)
+    K = fem.global_stiff_matrix(pb.nelx, pb.nely, pb.nelz, ks, dens, P_SIMP, EMIN, pb.freedofs)
+    nf = np.linalg.norm(pb.f)
+    s = solver(tosp_mod, pb, 2, omega=0.5, cg_product=1, maxiterMG=5)
+    s.SetupGMG(dens)
+    u, it, relres, rc = s.SolveMG(np.zeros(pb.f.size), pb.f)
+    s.close()
+    assert rc == 1 and it == 6
+    rtrue = np.linalg.norm(pb.f - K @ u) / nf
+    assert abs(relres - rtrue) <= 1e-6 * rtrue, (relres, rtrue)
+    s = solver(tosp_mod, pb, 2, omega=0.5, cg_product=1)
+    s.SetupGMG(dens)
+    u2, it2, relres2, rc2 = s.SolveMG(u, pb.f)
+    s.close()
+    assert rc2 == 0 and np.linalg.norm(pb.f - K @ u2) <= 1.0001e-8 * nf
