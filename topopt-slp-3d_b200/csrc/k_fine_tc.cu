@@ -222,6 +222,12 @@ __device__ __forceinline__ void cp_async4(void *dst, const void *src, int nbytes
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(nbytes)
                  : "memory");
 }
+// 16-byte asynchronous global -> shared copy (both addresses 16-byte
+// aligned); nbytes = 0 zero-fills.
+__device__ __forceinline__ void cp_async16(void *dst, const void *src, int nbytes) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(smem_u32(dst)), "l"(src), "r"(nbytes)
+                 : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_0() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
@@ -372,6 +378,24 @@ __device__ __forceinline__ void stage_brick(int64_t brick, float *xs, WT *wslab,
     // mesh and 4-byte aligned
     const int nelz_d = g.nelz * N;
     const int xd0 = ex0 * N, yd0 = ey0 * N, zd0 = ez0 * N;
+    // 16-byte pieces when the density mesh's rows along y are a whole number
+    // of pieces: every row then starts 16-byte aligned (the brick's first
+    // cell yd0 = 8 N bby is a multiple of a piece) and a piece lies wholly
+    // inside or wholly outside the mesh
+    constexpr int C16 = 16 / (int)sizeof(WT);             // cells per 16-byte piece
+    static_assert((K::WY * (int)sizeof(WT)) % 16 == 0 && (BY * N) % C16 == 0, "16-byte slab pieces");
+    if (fg.nely_d % C16 == 0) {
+        constexpr int P16 = K::WY / C16;                  // pieces per slab row
+        for (int u = tid; u < K::WZ * K::WX * P16; u += BRICK_ELEMS) {
+            const int row = u / P16, k = u - row * P16;
+            const int rz = row / K::WX, rx = row - rz * K::WX;
+            const int zd = zd0 + rz, xd = xd0 + rx, yd = yd0 + C16 * k;
+            const bool in = zd < nelz_d && xd < fg.nelx_d && yd < fg.nely_d;
+            const WT *src = in ? w + ((int64_t)zd * fg.nelx_d + xd) * fg.nely_d + yd : w;
+            cp_async16(wslab + row * K::WY + C16 * k, src, in ? 16 : 0);
+        }
+        return;
+    }
     for (int u = tid; u < K::WZ * K::WX * K::UPR; u += BRICK_ELEMS) {
         const int row = u / K::UPR, k = u - row * K::UPR;
         const int rz = row / K::WX, rx = row - rz * K::WX;
