@@ -61,6 +61,30 @@ __device__ __forceinline__ unsigned *red_counter(double *partials) {
     return reinterpret_cast<unsigned *>(partials + 2 * RED_BLOCKS);
 }
 
+// Grid-stride loop of the reduction kernels over [0, n), taken VB strides at a
+// time: load(k, i) reads element i into slot k for the VB elements of a batch,
+// then use(k, i) consumes them in index order.  The reduction grid is a few
+// blocks per SM, so a thread walks dozens of elements; with one element's
+// loads in flight the loop waits one DRAM latency per element, with VB it
+// waits one per batch.  A thread visits its elements in the same order as the
+// plain grid-stride loop, so its running sums are bitwise the same.
+constexpr int VB = 4;
+template <class Load, class Use>
+__device__ __forceinline__ void grid_batched(int64_t n, Load load, Use use) {
+    const int64_t T = (int64_t)gridDim.x * blockDim.x;
+    int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    for (; i + (VB - 1) * T < n; i += VB * T) {
+#pragma unroll
+        for (int k = 0; k < VB; ++k) load(k, i + k * T);
+#pragma unroll
+        for (int k = 0; k < VB; ++k) use(k, i + k * T);
+    }
+    for (; i < n; i += T) {
+        load(0, i);
+        use(0, i);
+    }
+}
+
 // Call after thread 0 wrote this block's partial(s); true in every thread of
 // the last block, which then sees all partials.
 __device__ __forceinline__ bool last_block(unsigned *counter) {
@@ -81,11 +105,14 @@ __device__ __forceinline__ double sum_partials(const double *partials, int np, d
 }
 
 template <typename TB>
-__global__ void k_dot_partial(const double *a, const TB *b, int64_t n, double *partials, double *out) {
+__global__ void __launch_bounds__(256, 4) k_dot_partial(const double *a, const TB *b, int64_t n, double *partials, double *out) {
     __shared__ double sh[32];
     double s = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
-        s += a[i] * (double)b[i];
+    double av[VB];
+    TB bv[VB];
+    grid_batched(
+        n, [&](int k, int64_t i) { av[k] = a[i]; bv[k] = b[i]; },
+        [&](int k, int64_t) { s += av[k] * (double)bv[k]; });
     s = block_sum(s, sh);
     if (threadIdx.x == 0) partials[blockIdx.x] = s;
     if (last_block(red_counter(partials))) {
@@ -102,15 +129,17 @@ void launch_dot(const double *a, const float *b, int64_t n, double *partials, do
 }
 
 // a'b and a'c in one pass over a (partials: 2 * RED_BLOCKS).
-__global__ void k_dot2_partial(const double *a, const double *b, const double *c, int64_t n, double *partials,
+__global__ void __launch_bounds__(256, 4) k_dot2_partial(const double *a, const double *b, const double *c, int64_t n, double *partials,
                                double *out0, double *out1) {
     __shared__ double sh[32];
     double s = 0.0, t = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double ai = a[i];
-        s += ai * b[i];
-        t += ai * c[i];
-    }
+    double av[VB], bv[VB], cv[VB];
+    grid_batched(
+        n, [&](int k, int64_t i) { av[k] = a[i]; bv[k] = b[i]; cv[k] = c[i]; },
+        [&](int k, int64_t) {
+            s += av[k] * bv[k];
+            t += av[k] * cv[k];
+        });
     s = block_sum(s, sh);
     t = block_sum(t, sh);
     if (threadIdx.x == 0) {
@@ -138,17 +167,28 @@ void launch_dot2(const double *a, const double *b, const double *c, int64_t n, d
 // loop order and reduction tree as k_dot2_partial / k_dot_partial, so the
 // dots are bitwise those of the separate kernels.
 template <typename T>
-__global__ void k_jacobi_out_dot(double *out, const T *x, const T *b, const T *t, const T *invd, int64_t n,
+__global__ void __launch_bounds__(256, 4) k_jacobi_out_dot(double *out, const T *x, const T *b, const T *t, const T *invd, int64_t n,
                                  const double *r, const double *so, double *partials, double *out0, double *out1) {
     __shared__ double sh[32];
     double s0 = 0.0, s1 = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double si = (double)(x[i] + invd[i] * (b[i] - t[i]));
-        out[i] = si;
-        const double ri = r[i];
-        s0 += ri * si;
-        if (so) s1 += ri * so[i];
-    }
+    T xv[VB], bv[VB], tv[VB], dv[VB];
+    double rv[VB], ov[VB];
+    grid_batched(
+        n,
+        [&](int k, int64_t i) {
+            xv[k] = x[i];
+            bv[k] = b[i];
+            tv[k] = t[i];
+            dv[k] = invd[i];
+            rv[k] = r[i];
+            if (so) ov[k] = so[i];
+        },
+        [&](int k, int64_t i) {
+            const double si = (double)(xv[k] + dv[k] * (bv[k] - tv[k]));
+            out[i] = si;
+            s0 += rv[k] * si;
+            if (so) s1 += rv[k] * ov[k];
+        });
     s0 = block_sum(s0, sh);
     if (so) s1 = block_sum(s1, sh);
     if (threadIdx.x == 0) {
@@ -225,21 +265,31 @@ void launch_pcg_finish(double *x, const double *d, const double *scal, int64_t n
 // x0 is given, its first Jacobi iterate x0 = invd0 b0 (the sweep from a zero
 // guess).
 template <typename TQ>
-__global__ void k_pcg_update(double *r, const TQ *q, double *scal, int64_t n, double *partials, float *b0,
+__global__ void __launch_bounds__(256, 4) k_pcg_update(double *r, const TQ *q, double *scal, int64_t n, double *partials, float *b0,
                              const float *invd0, float *x0) {
     __shared__ double sh[32];
     const double alpha = scal[0] / scal[2];
     double s = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double ri = r[i] - alpha * (double)q[i];
-        r[i] = ri;
-        s += ri * ri;
-        if (b0) {
-            const float bi = (float)ri;
-            b0[i] = bi;
-            if (x0) x0[i] = invd0[i] * bi;
-        }
-    }
+    double rv[VB];
+    TQ qv[VB];
+    float dv[VB];
+    grid_batched(
+        n,
+        [&](int k, int64_t i) {
+            rv[k] = r[i];
+            qv[k] = q[i];
+            if (b0 && x0) dv[k] = invd0[i];
+        },
+        [&](int k, int64_t i) {
+            const double ri = rv[k] - alpha * (double)qv[k];
+            r[i] = ri;
+            s += ri * ri;
+            if (b0) {
+                const float bi = (float)ri;
+                b0[i] = bi;
+                if (x0) x0[i] = dv[k] * bi;
+            }
+        });
     s = block_sum(s, sh);
     if (threadIdx.x == 0) partials[blockIdx.x] = s;
     if (last_block(red_counter(partials))) {
@@ -264,20 +314,29 @@ void launch_pcg_update(double *r, const float *q, double *scal, double *partials
 // Residual replacement: r = f - t (t = K x by the FP64 operator), r'r into
 // slot 3 (last block) and, for the mixed V-cycle (b0 given), the next cycle's
 // FP32 right-hand side and first Jacobi iterate as in k_pcg_update.
-__global__ void k_replace_residual(const double *f, const double *t, double *r, double *scal, int64_t n,
+__global__ void __launch_bounds__(256, 4) k_replace_residual(const double *f, const double *t, double *r, double *scal, int64_t n,
                                    double *partials, float *b0, const float *invd0, float *x0) {
     __shared__ double sh[32];
     double s = 0.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const double ri = f[i] - t[i];
-        r[i] = ri;
-        s += ri * ri;
-        if (b0) {
-            const float bi = (float)ri;
-            b0[i] = bi;
-            if (x0) x0[i] = invd0[i] * bi;
-        }
-    }
+    double fv[VB], tv[VB];
+    float dv[VB];
+    grid_batched(
+        n,
+        [&](int k, int64_t i) {
+            fv[k] = f[i];
+            tv[k] = t[i];
+            if (b0 && x0) dv[k] = invd0[i];
+        },
+        [&](int k, int64_t i) {
+            const double ri = fv[k] - tv[k];
+            r[i] = ri;
+            s += ri * ri;
+            if (b0) {
+                const float bi = (float)ri;
+                b0[i] = bi;
+                if (x0) x0[i] = dv[k] * bi;
+            }
+        });
     s = block_sum(s, sh);
     if (threadIdx.x == 0) partials[blockIdx.x] = s;
     if (last_block(red_counter(partials))) {
