@@ -177,33 +177,43 @@ int dense_sweep_inverse(double *A, double *C, double *Pinv, int64_t npad, int *d
 
 // x = X b (X symmetric, npad x npad; only the first n entries are used).
 template <typename T>
-__global__ void k_dense_gemv(const double *__restrict__ X, const T *__restrict__ b, T *__restrict__ x, int64_t n,
-                             int64_t npad) {
-    const int lane = threadIdx.x & 31;
-    const int64_t warp = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
-    const int64_t nwarps = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t row = warp; row < n; row += nwarps) {
-        const double *xr = X + row * npad;
-        // four independent partial sums keep four loads per lane in flight
-        double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-        int64_t j = lane;
-        for (; j + 96 < n; j += 128) {
-            s0 += xr[j] * (double)b[j];
-            s1 += xr[j + 32] * (double)b[j + 32];
-            s2 += xr[j + 64] * (double)b[j + 64];
-            s3 += xr[j + 96] * (double)b[j + 96];
+__global__ void __launch_bounds__(256)
+k_dense_gemv(const double *__restrict__ X, const T *__restrict__ b, T *__restrict__ x, int64_t n, int64_t npad) {
+    // Four warps per row (two rows per block), four partial sums per lane:
+    // the coarsest system has only a few thousand rows, and with one warp
+    // per row the loads in flight were too few to cover the memory latency.
+    __shared__ double part[8];
+    const int lane = threadIdx.x & 127;   // lane within the row's four warps
+    const int grp = threadIdx.x >> 7;     // row of the block (0, 1)
+    const int w = threadIdx.x >> 5;       // warp of the block
+    for (int64_t row0 = 2 * (int64_t)blockIdx.x; row0 < n; row0 += 2 * (int64_t)gridDim.x) {   // block-uniform
+        const int64_t row = row0 + grp;
+        double s = 0.0;
+        if (row < n) {
+            const double *xr = X + row * npad;
+            double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+            int64_t j = lane;
+            for (; j + 384 < n; j += 512) {
+                s0 += xr[j] * (double)b[j];
+                s1 += xr[j + 128] * (double)b[j + 128];
+                s2 += xr[j + 256] * (double)b[j + 256];
+                s3 += xr[j + 384] * (double)b[j + 384];
+            }
+            for (; j < n; j += 128) s0 += xr[j] * (double)b[j];
+            s = (s0 + s1) + (s2 + s3);
         }
-        for (; j < n; j += 32) s0 += xr[j] * (double)b[j];
-        double s = (s0 + s1) + (s2 + s3);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
-        if (lane == 0) x[row] = (T)s;
+        if ((threadIdx.x & 31) == 0) part[w] = s;
+        __syncthreads();
+        if (lane == 0 && row < n) x[row] = (T)((part[4 * grp] + part[4 * grp + 1]) + (part[4 * grp + 2] + part[4 * grp + 3]));
+        __syncthreads();
     }
 }
 
 template <typename T>
 void launch_dense_solve(const double *X, const T *b, T *x, int64_t n, int64_t npad, cudaStream_t st) {
-    int64_t blocks = (n * 32 + 255) / 256;
+    int64_t blocks = (n + 1) / 2;
     if (blocks > 2048) blocks = 2048;
     if (blocks < 1) blocks = 1;
     k_dense_gemv<T><<<(unsigned)blocks, 256, 0, st>>>(X, b, x, n, npad); count_launch();

@@ -67,9 +67,10 @@ __device__ __forceinline__ unsigned *red_counter(double *partials) {
 // blocks per SM, so a thread walks dozens of elements; with one element's
 // loads in flight the loop waits one DRAM latency per element, with VB it
 // waits one per batch.  A thread visits its elements in the same order as the
-// plain grid-stride loop, so its running sums are bitwise the same.
+// plain grid-stride loop, so its running sums are bitwise the same.  The
+// plain dot (two loads per element) takes batches of eight.
 constexpr int VB = 4;
-template <class Load, class Use>
+template <int VB = tosp::VB, class Load, class Use>
 __device__ __forceinline__ void grid_batched(int64_t n, Load load, Use use) {
     const int64_t T = (int64_t)gridDim.x * blockDim.x;
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
@@ -108,9 +109,10 @@ template <typename TB>
 __global__ void __launch_bounds__(256, 4) k_dot_partial(const double *a, const TB *b, int64_t n, double *partials, double *out) {
     __shared__ double sh[32];
     double s = 0.0;
-    double av[VB];
-    TB bv[VB];
-    grid_batched(
+    constexpr int VB8 = 2 * VB;
+    double av[VB8];
+    TB bv[VB8];
+    grid_batched<VB8>(
         n, [&](int k, int64_t i) { av[k] = a[i]; bv[k] = b[i]; },
         [&](int k, int64_t) { s += av[k] * (double)bv[k]; });
     s = block_sum(s, sh);
