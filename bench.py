@@ -10,8 +10,9 @@ the whole-job rate, timed with CUDA events and maximised over ranks.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tosp|reference]
 
-`--impl reference` times the reference algorithm on the host cores (the C/OpenMP
-restatement of the matrix-free SolveMGWOK path in oracle/) on a bounded sample.
+`--impl reference` times the reference's default algorithm on the host cores
+(the C/OpenMP restatement of the assembled GlobalStiffMatrix / SetupGMG /
+SolveMG / Grad path in oracle/): one complete solve, split over the timed steps.
 """
 import argparse
 import json
@@ -664,8 +665,7 @@ def main():
         rc = lib.tosp_solve_mg(s.h, u_d.data_ptr(), f_d.data_ptr(), u_d.numel(), C.byref(it), C.byref(rr))
         if rc != 0:
             raise tosp.TospError(rc, lib.tosp_last_error(s.h).decode())
-        ufull_d.zero_()
-        ufull_d[fidx_d] = u_d
+        ufull_d.index_copy_(0, fidx_d, u_d)    # U(freedofs) = u; fixed entries stay zero
         rc = lib.tosp_grad(s.h, ufull_d.data_ptr(), ufull_d.numel(), g_d.data_ptr(), None, g_d.numel())
         if rc != 0:
             raise tosp.TospError(rc, lib.tosp_last_error(s.h).decode())
@@ -724,8 +724,8 @@ def main():
         u_h.zero_()
         it, rr = C.c_int32(), C.c_double()
         lib.tosp_solve_mg(s.h, u_h.data_ptr(), f_h.data_ptr(), u_h.numel(), C.byref(it), C.byref(rr))
-        uf_h.zero_()
-        uf_h[fidx_h] = u_h
+        # U(freedofs) = u; the fixed entries of uf_h stay zero (never written)
+        uf_h.index_copy_(0, fidx_h, u_h)
         lib.tosp_grad(s.h, uf_h.data_ptr(), uf_h.numel(), g_h.data_ptr(), None, g_h.numel())
         return it.value
 
