@@ -61,24 +61,24 @@ __device__ __forceinline__ unsigned *red_counter(double *partials) {
     return reinterpret_cast<unsigned *>(partials + 2 * RED_BLOCKS);
 }
 
-// Grid-stride loop of the reduction kernels over [0, n), taken VB strides at a
-// time: load(k, i) reads element i into slot k for the VB elements of a batch,
-// then use(k, i) consumes them in index order.  The reduction grid is a few
-// blocks per SM, so a thread walks dozens of elements; with one element's
-// loads in flight the loop waits one DRAM latency per element, with VB it
-// waits one per batch.  A thread visits its elements in the same order as the
+// Grid-stride loop of the reduction kernels over [0, n), taken B strides at a
+// time (VB = 4 by default): load(k, i) reads element i into slot k for the B
+// elements of a batch, then use(k, i) consumes them in index order.  The
+// reduction grid is a few blocks per SM, so a thread walks dozens of
+// elements; with one element's loads in flight the loop waits one DRAM
+// latency per element, with B it waits one per batch.  A thread visits its elements in the same order as the
 // plain grid-stride loop, so its running sums are bitwise the same.  The
 // plain dot (two loads per element) takes batches of eight.
 constexpr int VB = 4;
-template <int VB = tosp::VB, class Load, class Use>
+template <int B = VB, class Load, class Use>
 __device__ __forceinline__ void grid_batched(int64_t n, Load load, Use use) {
     const int64_t T = (int64_t)gridDim.x * blockDim.x;
     int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    for (; i + (VB - 1) * T < n; i += VB * T) {
+    for (; i + (B - 1) * T < n; i += B * T) {
 #pragma unroll
-        for (int k = 0; k < VB; ++k) load(k, i + k * T);
+        for (int k = 0; k < B; ++k) load(k, i + k * T);
 #pragma unroll
-        for (int k = 0; k < VB; ++k) use(k, i + k * T);
+        for (int k = 0; k < B; ++k) use(k, i + k * T);
     }
     for (; i < n; i += T) {
         load(0, i);
